@@ -1,0 +1,295 @@
+"""Benchmark of the B200-native Boussinesq RBC step (one JSON line on rank 0).
+
+Workload (the config the headline metric is quoted on that fits one GPU): plain FP64
+step, 256 x 256 grid, Lx = Ly = 32, Nz = 8 Galerkin modes, Pr = 0.9, Ra = 5000,
+dt = 5e-4, 65,536 passive tracers, seeded synthetic initial state (theta N(0, 1e-3^2)
+on |k| <= 8 of the lowest mode, tracers uniform). A "step" is one IMEX step plus one
+tracer advance. Timing: W untimed warm-up steps, then K steps bracketed by a barrier and
+a synchronize, CUDA events on the solver's stream, max over ranks. N > 1 runs N
+independent replicas (weak scaling; no collective on the data path).
+
+--impl reference times the reference method's CPU implementation (the FP64 oracle
+port, all host cores) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Sim-time/s per GPU: mixed/batched/surrogate vs plain FP64 at ≤1e-3 Nu error"
+WORK = dict(nx=256, ny=256, nz=8, lx=32.0, ly=32.0, ra=5000.0, pr=0.9, dt=5e-4)
+NTRACERS = 65536
+SEED = 2
+
+
+def bytes_alg(nx, ny, L, ntr):
+    """Algorithmic bytes of one plain FP64 step (step + tracers)."""
+    S = (nx // 2 + 1) * ny
+    P = nx * ny
+    step = L * (12 * S * 16 + 44 * P * 8) + 40 * L * L * S
+    tr = 5 * L * P * 8 + 816 * ntr
+    return step, tr
+
+
+def stage_bytes(nx, ny, L, ckeep, nkept, ntr):
+    """Algorithmic bytes per launch of each kernel (read + write of its compulsory data)."""
+    P = nx * ny
+    C = 16  # complex double
+    kept = nkept  # kept wavenumbers (c < ckeep, rows of the 2/3 rule)
+    col = ckeep * ny
+    return {
+        "synth_columns": 3 * L * kept * C + 8 * L * col * C,
+        "rows_c2r": 8 * L * col * C + 8 * L * P * 8,
+        "tracers": 5 * L * P * 8 + 48 * ntr,
+        "contract": 8 * L * P * 8 + 13 * L * P * 8,
+        "rows_r2c": 13 * L * P * 8 + 13 * L * col * C,
+        "columns_combine": 13 * L * col * C + 3 * L * col * C,
+        # N, state and history read, state and history written, operator tables
+        "update": kept * L * C * (3 + 3 + 3 + 3 + 3) + kept * 5 * L * L * 8,
+    }
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch from a committed ncu summary (profiles/traffic.json)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(kernel)
+    return None if v is None else v.get("dram_bytes_per_launch")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device):
+        self.proc = None
+        self.out = os.path.join("/tmp", f"rbc_clocks_{os.getpid()}.csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.out, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.out) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.out)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(steps_hint):
+    """Oracle port on the host cores: bounded sample of the same workload."""
+    import oracle
+    threads = os.cpu_count() or 1
+    o = oracle.Oracle(WORK["nx"], WORK["ny"], WORK["nz"], WORK["lx"], WORK["ly"], WORK["ra"], WORK["pr"],
+                      WORK["dt"], threads=threads)
+    o.init_theta(SEED, 1e-3, 8.0)
+    o.tracers_set(oracle.tracer_positions(SEED, NTRACERS, WORK["lx"], WORK["ly"]))
+    t = time.perf_counter()
+    o.step(1)
+    first = time.perf_counter() - t
+    n = max(2, min(steps_hint, int(20.0 / max(first, 1e-3))))
+    t = time.perf_counter()
+    o.step(n)
+    el = time.perf_counter() - t
+    return {"value": n * WORK["dt"] / el, "unit": "sim-time/s", "cores": threads, "kind": "port",
+            "sample": f"{n} oracle steps (after 1 warm-up) of the 256x256x8 + 65536-tracer workload, "
+                      f"{el / n:.3f} s/step", "steps_per_s": n / el}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import oracle  # noqa: F401  (checker library; the reference method's CPU port)
+    cb = cpu_baseline(args.steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "sim-time/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / cb["steps_per_s"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "plain FP64 RBC step 256x256x8, Lx=Ly=32, Ra=5000, Pr=0.9, dt=5e-4, "
+                                   "+65536 tracers", "impl": "oracle port of the reference method"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "sim-time/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import numpy as np
+    import sdc_b200
+
+    s = sdc_b200.Solver(**WORK, form=args.form, n_tracers=NTRACERS, device=local)
+    stream = torch.cuda.current_stream()
+    s.set_stream(stream.cuda_stream)
+    s.init_fields(SEED, 1e-3, 8.0)
+    s.tracers_seed(SEED)
+    s.step(args.warmup)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident throughput
+    clk = ClockSampler(local)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step_async(args.steps)
+    e1.record(stream)
+    s.synchronize()
+    launches = s.kernel_launches
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * WORK["dt"] / (ms_max / 1000.0)
+
+    # ---- per-kernel timing (roofline of the dominant kernel)
+    stages = s.stage_times(max(5, min(50, args.steps // 10)))
+    nx, ny, L = WORK["nx"], WORK["ny"], WORK["nz"]
+    mox = nx // 2 + 1
+    ck = 0
+    while ck < mox and not (mox - ck <= (1.0 / 3.0) * mox):
+        ck += 1
+    nrow = sum(1 for r in range(ny) if not (abs(0.5 * ny - r) <= (1.0 / 3.0) * 0.5 * ny))
+    sb = stage_bytes(nx, ny, L, ck, ck * nrow, NTRACERS)
+    per_step = {k: v[0] * v[1] for k, v in stages.items()}
+    dom = max(per_step, key=per_step.get)
+    peak, peak_kind = measured_peaks()
+    ach = sb[dom] / (stages[dom][0] * 1e-3) / 1e9
+    roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": ach / peak, "traffic": profile_traffic(dom), "peak_source": peak_kind,
+            "alg_bytes_per_launch": sb[dom], "ms_per_launch": stages[dom][0],
+            "stages_ms": {k: round(v[0], 5) for k, v in stages.items()}}
+    step_b, tr_b = bytes_alg(nx, ny, L, NTRACERS)
+
+    # ---- end to end through the C ABI with host buffers
+    host_state = s.get_state()
+    host_tr = s.tracers_get()
+    barrier()
+    t0 = time.perf_counter()
+    s.set_state(*host_state)
+    s.tracers_set(host_tr)
+    for _ in range(args.steps):
+        s.step(1)
+        s.diagnostics()
+    out_state = s.get_state()
+    out_tr = s.tracers_get()
+    el = time.perf_counter() - t0
+    te = torch.tensor([el], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    el = float(te.item())
+    state_bytes = sum(a.nbytes for a in host_state)
+    tr_bytes = host_tr.nbytes
+    e2e = {"value": world * args.steps * WORK["dt"] / el, "unit": "sim-time/s",
+           "h2d_bytes_per_step": (state_bytes + tr_bytes) / args.steps,
+           "d2h_bytes_per_step": 32 + (state_bytes + tr_bytes) / args.steps,
+           "includes": "set_state + tracers_set, K x (rbc_step(1) + rbc_diagnostics), get_state + tracers_get"}
+    d = s.diagnostics()
+    assert np.isfinite(d["ke"]) and np.all(np.isfinite(out_tr)) and all(np.all(np.isfinite(a)) for a in out_state)
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(8)
+        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "sim-time/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "steps_per_s": 1000.0 * args.steps / ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64", "data": "synthetic",
+                "config": {"workload": f"plain {args.form.upper()} RBC step 256x256x8, Lx=Ly=32, Ra=5000, "
+                                       f"Pr=0.9, dt=5e-4, +65536 tracers (RK4, 128 z levels)",
+                           "form": args.form, "parallelism": f"replicas x{world}",
+                           "l2": "working set > 126 MB L2 (state, history, scratch ~300 MB); no flush",
+                           "alg_bytes_per_step": step_b + tr_b},
+                "roofline": roof, "gpu_launches": launches,
+                "hbm_gbs_step_alg": (step_b + tr_b) / (ms_max / args.steps * 1e-3) / 1e9,
+                "clocks": clocks, "e2e": e2e, "cpu_baseline": cb,
+                "diag": {"nu_wall": d["nu_wall"], "ke": d["ke"], "step": d["step"]}}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

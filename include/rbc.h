@@ -1,0 +1,166 @@
+/* rbc.h -- C ABI of the B200-native Boussinesq Rayleigh-Benard step (libsdc_b200.so).
+ *
+ * Drop-in boundary for the solver path of jceyy/sdc gpu_flow/code: field init, the IMEX
+ * step, the nonlinear operator, tracer advance and diagnostics. Plain pointers and sizes
+ * only. Spectral fields use the reference layout of matrix_device
+ * (gpu_flow/code/matrix/matrix_device.h:13-66): complex numbers as interleaved
+ * (re, im) doubles, index c + (Nx/2+1) * (r + Ny * k) for kx index c, ky index r
+ * (ky = r for r <= Ny/2, r - Ny above) and vertical mode k. F and G hold L complex
+ * values (imaginary parts are zero after every step, as in the reference).
+ *
+ * Every function returns an rbc_status; none exits the process (the reference calls
+ * exit() through EXIT_ERROR, gpu_flow/code/cuda_defines.h:50-51). rbc_last_error()
+ * gives the message of the last failure on a handle. A handle may be used from one
+ * host thread at a time; all device work runs on the handle's CUDA stream, and no
+ * device memory is allocated after rbc_create().
+ */
+#ifndef SDC_B200_RBC_H
+#define SDC_B200_RBC_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBC_ABI_VERSION 1
+
+typedef struct rbc_handle rbc_handle;
+
+typedef enum {
+    RBC_OK = 0,
+    RBC_ERR_INVALID_ARG = 1,
+    RBC_ERR_CUDA = 2,
+    RBC_ERR_NAN = 3,          /* a non-finite value appeared in the state */
+    RBC_ERR_TIMEOUT = 4,
+    RBC_ERR_IO = 5,
+    RBC_ERR_UNSUPPORTED = 6,
+    RBC_ERR_OUT_OF_MEMORY = 7
+} rbc_status;
+
+typedef enum {
+    RBC_FORM_FP64 = 0,        /* plain step: everything in FP64 */
+    RBC_FORM_MIXED = 1        /* FP32 synthesis, products, contraction and FFTs;
+                                 FP64 implicit solve, mean flow and diagnostics */
+} rbc_form;
+
+/* Construction parameters. Replaces main.cu's -nmodes M N L, -clength Lx Ly, -ra,
+ * -pr, -dt, -device (gpu_flow/code/main.cu:64-112) and the operator constructors
+ * Coeff<double>(L), linear_implicit_operator::init_operator, inverse_B_matrix::init_operator,
+ * nonlinear_operator_rayleigh_noslip::init_operator, implicit_explicit_step::init_timestepping
+ * (main.cu:431-454). */
+typedef struct {
+    int nx;          /* physical grid points in x (Nx = 2^a 3^b, 8..1024) */
+    int ny;          /* physical grid points in y (same rule) */
+    int nz;          /* vertical Galerkin modes L */
+    double lx, ly;   /* box lengths in units of the layer depth */
+    double ra, pr;   /* Rayleigh and Prandtl numbers */
+    double dt;       /* time step */
+    int form;        /* rbc_form */
+    int n_tracers;   /* passive tracers (0: none) */
+    int device;      /* CUDA device ordinal */
+    int diag_capacity; /* per-step diagnostics ring entries (0: 4096) */
+} rbc_params;
+
+/* Diagnostics of the state after a step (no reference counterpart; see DESIGN). */
+typedef struct {
+    double nu_wall;  /* 1 - d<theta>_xy/dz at z = -1/2 */
+    double nu_vol;   /* 1 + <w theta>_V */
+    double ke;       /* 1/2 <u^2 + v^2 + w^2>_V */
+    long long step;  /* steps taken since construction */
+} rbc_diag;
+
+/* Five host buffers in the reference layout (see top of file). */
+typedef struct {
+    double* theta; double* f; double* g; double* F; double* G;
+} rbc_state;
+
+/* --- construction -------------------------------------------------------------- */
+rbc_status rbc_create(const rbc_params* p, rbc_handle** out);
+void rbc_destroy(rbc_handle* h);
+const char* rbc_last_error(const rbc_handle* h);
+const char* rbc_status_string(rbc_status s);
+/* Sets the CUDA stream (cudaStream_t) for all later device work; NULL restores the
+ * handle's own stream. */
+rbc_status rbc_set_stream(rbc_handle* h, void* stream);
+
+/* --- fields -------------------------------------------------------------------- */
+/* Seeded initial condition: theta of the lowest vertical mode gets N(0, amplitude^2)
+ * real and imaginary parts on all (c, r) with c^2 + ky^2 <= kmax^2 (SplitMix64 +
+ * Box-Muller, visited r-major then c), then the Hermitian fix of make_real_signal
+ * (gpu_flow/code/util/util.cu:213-224); f = g = F = G = 0. Replaces
+ * matrix_device_init::init_random (gpu_flow/code/util/init.cu:9-20) and main.cu:300-396.
+ * The next step is an Euler step. */
+rbc_status rbc_init_fields(rbc_handle* h, unsigned long long seed, double amplitude, double kmax);
+/* Upload / download the state (host buffers, reference layout). rbc_set_state applies
+ * the 2/3 dealiasing of the reference's first dealias_data call and resets the AB2
+ * history, as a restart from dump files does (main.cu:290-385,
+ * implicit_explicit_stepping.cu:43-52). */
+rbc_status rbc_set_state(rbc_handle* h, const double* theta, const double* f, const double* g,
+                         const double* F, const double* G);
+rbc_status rbc_get_state(rbc_handle* h, double* theta, double* f, double* g, double* F, double* G);
+
+/* --- step ---------------------------------------------------------------------- */
+/* nsteps iterations of the reference loop body (main.cu:612-637): step_time
+ * (implicit_explicit_stepping.cu:32-97), make_real_signal, and the tracer advance when
+ * tracers exist. Waits for completion; RBC_ERR_NAN if a non-finite value appeared. */
+rbc_status rbc_step(rbc_handle* h, int nsteps);
+/* Same, enqueued on the handle's stream without waiting. */
+rbc_status rbc_step_async(rbc_handle* h, int nsteps);
+rbc_status rbc_synchronize(rbc_handle* h);
+
+/* --- nonlinear operator -------------------------------------------------------- */
+/* The reference's nonlinear_operator_rayleigh_noslip::calculate_operator(theta, f, g, F, G)
+ * (gpu_flow/code/operator/nonlinear_operator_rayleigh_noslip.cu:83-1394) on host buffers:
+ * reads `in`, writes the five operator results to `out` (caller-owned; the reference
+ * returned a new matrix_folder*[5]). The input is dealiased first, as step_time does
+ * before calling it. Does not change the solver state. */
+rbc_status rbc_nonlinear(rbc_handle* h, const rbc_state* in, rbc_state* out);
+
+/* --- tracers ------------------------------------------------------------------- */
+/* Positions as three blocks x[n], y[n], z[n] (z in (-1/2, 1/2)); replaces
+ * particle_tracer::init_positions and get_particle_positions
+ * (gpu_flow/code/particle/particle_tracer.h:65-87). n must equal params.n_tracers. */
+rbc_status rbc_tracers_set(rbc_handle* h, const double* xyz, int n);
+rbc_status rbc_tracers_get(rbc_handle* h, double* xyz, int n);
+/* Uniform seeded positions in [0,Lx) x [0,Ly) x (-1/2,1/2) (SplitMix64). */
+rbc_status rbc_tracers_seed(rbc_handle* h, unsigned long long seed);
+/* One tracer step with the current velocity field (particle_tracer::step_particles,
+ * particle_tracer.cu:141-212: RK4, trilinear interpolation on 128 z levels, periodic x/y,
+ * reflection at z = +-(1/2 - 1e-3)); rbc_step calls it after every fluid step. */
+rbc_status rbc_tracers_advance(rbc_handle* h);
+
+/* --- diagnostics --------------------------------------------------------------- */
+/* Diagnostics of the latest step (or of the initial state before any step). */
+rbc_status rbc_diagnostics(rbc_handle* h, rbc_diag* out);
+/* The last min(n, steps, capacity) per-step entries, oldest first; *count receives the
+ * number written. */
+rbc_status rbc_diag_history(rbc_handle* h, rbc_diag* out, int n, int* count);
+/* Radial shell spectrum of theta(x, y, z): sum of |theta_hat|^2 over the half spectrum
+ * in nbins shells of width |q_max| / nbins, as energy_spectrum_2d::reduce_spectrum
+ * (gpu_flow/code/postProcessing/energy_spectrum_2d.cu:85-129). */
+rbc_status rbc_spectrum(rbc_handle* h, double z, double* bins, int nbins);
+
+/* --- inspection (tests, tools) ------------------------------------------------- */
+/* Physical fields of the current state: 8 blocks [L][Ny][Nx] in the order
+ * d_x f, d_y f, q^2 f, d_y g + F, -d_x g + G, theta, d_x theta, d_y theta
+ * (the synthesis of nonlinear_operator_rayleigh_noslip.cu:112-233). */
+rbc_status rbc_synthesis(rbc_handle* h, double* out);
+/* Galerkin table by the reference getter name ("Iac", "Ia1" L*L; "Ibbb", "Ibb1", "Ib11",
+ * "I111", "Iabc", "Iac1", "Iaab", "Iaa1", "Iab2", "Ia12" L^3; "lambda" L), index order of
+ * gpu_flow/code/util/coeff.cu:1151-1222. Returns the count written in *count. */
+rbc_status rbc_table(rbc_handle* h, const char* name, double* out, int* count);
+/* Same tables without a handle or a GPU (host computation only). */
+rbc_status rbc_galerkin_table(int nz, const char* name, double* out, int* count);
+/* Stage timing (CUDA events on the handle's stream around every kernel): runs nsteps
+ * steps and returns the mean milliseconds per launch of each kernel kind in
+ * ms[RBC_NSTAGE] and the launches per step in counts[RBC_NSTAGE], in the order
+ * synth_columns, rows_c2r, tracers, contract, rows_r2c, columns_combine, update.
+ * Replaces the reference's -DTIMER host Timer (gpu_flow/code/util/util.cu:230-281). */
+#define RBC_NSTAGE 7
+rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts);
+/* Device kernel launches issued by the last rbc_step call (for launch accounting). */
+long long rbc_kernel_launches(const rbc_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDC_B200_RBC_H */

@@ -1,0 +1,206 @@
+"""ctypes wrapper around the CPU FP64 oracle (oracle/rbc_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py, as the checker. The sdc_b200 package never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptr(a):
+    assert a.dtype in (np.float64, np.complex128) and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "_build", "liboracle.so")
+        if not os.path.exists(path):
+            _build.build()
+        L = ctypes.CDLL(path)
+        L.oracle_create.restype = ctypes.c_void_p
+        L.oracle_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 5 + [ctypes.c_int]
+        for name in ("oracle_destroy", "oracle_step", "oracle_set_threads", "oracle_tracers_advance"):
+            getattr(L, name).restype = None
+        L.oracle_destroy.argtypes = [ctypes.c_void_p]
+        L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_tracers_advance.argtypes = [ctypes.c_void_p]
+        for name in ("oracle_set_state", "oracle_get_state", "oracle_nonlinear"):
+            getattr(L, name).restype = None
+            getattr(L, name).argtypes = [ctypes.c_void_p] + [_dp] * 5
+        L.oracle_synthesis.argtypes = [ctypes.c_void_p, _dp]
+        L.oracle_synthesis.restype = None
+        L.oracle_tracers_set.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int]
+        L.oracle_tracers_set.restype = None
+        L.oracle_tracers_get.argtypes = [ctypes.c_void_p, _dp]
+        L.oracle_tracers_get.restype = None
+        L.oracle_velocity_grid.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.oracle_velocity_grid.restype = None
+        L.oracle_diagnostics.argtypes = [ctypes.c_void_p, _dp]
+        L.oracle_diagnostics.restype = None
+        L.oracle_nu_wall.argtypes = [ctypes.c_void_p]
+        L.oracle_nu_wall.restype = ctypes.c_double
+        L.oracle_spectrum.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp, ctypes.c_int]
+        L.oracle_spectrum.restype = None
+        L.oracle_table.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp]
+        L.oracle_table.restype = ctypes.c_int
+        L.oracle_operator_table.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.oracle_operator_table.restype = None
+        L.oracle_fft.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
+        L.oracle_fft.restype = None
+        L.oracle_rfft2.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.oracle_rfft2.restype = None
+        L.oracle_irfft2.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.oracle_irfft2.restype = None
+        L.oracle_lu_invert.argtypes = [ctypes.c_int, _dp, _dp]
+        L.oracle_lu_invert.restype = ctypes.c_int
+        L.oracle_init_theta.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, ctypes.c_double]
+        L.oracle_init_theta.restype = None
+        L.oracle_tracer_positions.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp]
+        L.oracle_tracer_positions.restype = None
+        _LIB = L
+    return _LIB
+
+
+def table(L, name):
+    n = L if name == "lambda" else (L * L if name in ("Iac", "Ia1") else L ** 3)
+    out = np.zeros(n)
+    m = lib().oracle_table(L, name.encode(), _ptr(out))
+    if m < 0:
+        raise KeyError(name)
+    return out[:m]
+
+
+def fft(x, sign=-1):
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.zeros_like(x)
+    lib().oracle_fft(x.size, _ptr(x), _ptr(out), sign)
+    return out
+
+
+def rfft2(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    ny, nx = a.shape
+    out = np.zeros((ny, nx // 2 + 1), np.complex128)
+    lib().oracle_rfft2(nx, ny, _ptr(a), _ptr(out))
+    return out
+
+
+def irfft2(a, nx):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    ny = a.shape[0]
+    out = np.zeros((ny, nx))
+    lib().oracle_irfft2(nx, ny, _ptr(a), _ptr(out))
+    return out
+
+
+def lu_invert(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    out = np.zeros_like(a)
+    if lib().oracle_lu_invert(a.shape[0], _ptr(a), _ptr(out)) != 0:
+        raise np.linalg.LinAlgError("singular")
+    return out
+
+
+def tracer_positions(seed, n, lx, ly):
+    out = np.zeros(3 * n)
+    lib().oracle_tracer_positions(seed, n, lx, ly, _ptr(out))
+    return out
+
+
+class Oracle:
+    """FP64 CPU restatement of the reference step (see rbc_oracle.cpp header)."""
+
+    def __init__(self, nx, ny, L, lx, ly, ra, pr, dt, threads=None):
+        if threads is None:
+            threads = os.cpu_count() or 1
+        self.nx, self.ny, self.L = nx, ny, L
+        self.mox = nx // 2 + 1
+        self.h = lib().oracle_create(nx, ny, L, lx, ly, ra, pr, dt, threads)
+        if not self.h:
+            raise ValueError("invalid oracle parameters")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_destroy(self.h)
+            self.h = None
+
+    def set_threads(self, n):
+        lib().oracle_set_threads(self.h, n)
+
+    def _bufs(self):
+        shp = (self.L, self.ny, self.mox)
+        return [np.zeros(shp, np.complex128) for _ in range(3)] + [np.zeros(self.L, np.complex128) for _ in range(2)]
+
+    def set_state(self, th, f, g, F, G):
+        arrs = [np.ascontiguousarray(a, dtype=np.complex128) for a in (th, f, g, F, G)]
+        lib().oracle_set_state(self.h, *[_ptr(a) for a in arrs])
+
+    def get_state(self):
+        b = self._bufs()
+        lib().oracle_get_state(self.h, *[_ptr(a) for a in b])
+        return b
+
+    def step(self, n=1):
+        lib().oracle_step(self.h, n)
+
+    def nonlinear(self):
+        b = self._bufs()
+        lib().oracle_nonlinear(self.h, *[_ptr(a) for a in b])
+        return b
+
+    def synthesis(self):
+        out = np.zeros((8, self.L, self.ny, self.nx))
+        lib().oracle_synthesis(self.h, _ptr(out))
+        return out
+
+    def init_theta(self, seed, amp, kmax):
+        lib().oracle_init_theta(self.h, seed, amp, kmax)
+
+    def tracers_set(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self.ntr = xyz.size // 3
+        lib().oracle_tracers_set(self.h, _ptr(xyz), self.ntr)
+
+    def tracers_get(self):
+        out = np.zeros(3 * self.ntr)
+        lib().oracle_tracers_get(self.h, _ptr(out))
+        return out
+
+    def tracers_advance(self):
+        lib().oracle_tracers_advance(self.h)
+
+    def velocity_grid(self):
+        shp = (128, self.ny, self.nx)
+        u = [np.zeros(shp) for _ in range(3)]
+        lib().oracle_velocity_grid(self.h, *[_ptr(a) for a in u])
+        return u
+
+    def diagnostics(self):
+        d = np.zeros(3)
+        lib().oracle_diagnostics(self.h, _ptr(d))
+        return {"nu_wall": d[0], "nu_vol": d[1], "ke": d[2]}
+
+    def nu_wall(self):
+        return lib().oracle_nu_wall(self.h)
+
+    def spectrum(self, nbins, z=0.0):
+        out = np.zeros(nbins)
+        lib().oracle_spectrum(self.h, z, _ptr(out), nbins)
+        return out
+
+    def operator_table(self, which):
+        out = np.zeros((self.L * self.L, self.ny, self.mox))
+        lib().oracle_operator_table(self.h, which, _ptr(out))
+        return out

@@ -1,0 +1,230 @@
+"""sdc_b200 -- B200-native (sm_100a) Boussinesq Rayleigh-Benard step.
+
+Python access to libsdc_b200.so through its C ABI (include/rbc.h). The library is the
+only compute path: if it is missing this package raises on import of `Solver` use, it
+never falls back to another implementation.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libsdc_b200.so")
+_LIB = None
+
+RBC_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite value", 4: "timeout",
+          5: "I/O error", 6: "unsupported", 7: "out of device memory"}
+FORMS = {"fp64": 0, "mixed": 1}
+
+
+class RBCError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("ra", ctypes.c_double),
+                ("pr", ctypes.c_double), ("dt", ctypes.c_double), ("form", ctypes.c_int),
+                ("n_tracers", ctypes.c_int), ("device", ctypes.c_int), ("diag_capacity", ctypes.c_int)]
+
+
+class _Diag(ctypes.Structure):
+    _fields_ = [("nu_wall", ctypes.c_double), ("nu_vol", ctypes.c_double), ("ke", ctypes.c_double),
+                ("step", ctypes.c_longlong)]
+
+
+class _State(ctypes.Structure):
+    _fields_ = [("theta", ctypes.c_void_p), ("f", ctypes.c_void_p), ("g", ctypes.c_void_p),
+                ("F", ctypes.c_void_p), ("G", ctypes.c_void_p)]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "rbc_set_stream",
+           "rbc_init_fields", "rbc_set_state", "rbc_get_state", "rbc_step", "rbc_step_async",
+           "rbc_synchronize", "rbc_nonlinear", "rbc_tracers_set", "rbc_tracers_get", "rbc_tracers_seed",
+           "rbc_tracers_advance", "rbc_diagnostics", "rbc_diag_history", "rbc_spectrum", "rbc_synthesis",
+           "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_kernel_launches"]
+
+
+def lib():
+    """Loads libsdc_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} not built: run python -c 'import __graft_entry__ as g; g.build()'")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.rbc_create.argtypes = [ctypes.POINTER(_Params), ctypes.POINTER(vp)]
+    L.rbc_destroy.argtypes = [vp]
+    L.rbc_destroy.restype = None
+    L.rbc_last_error.argtypes = [vp]
+    L.rbc_last_error.restype = ctypes.c_char_p
+    L.rbc_status_string.argtypes = [ctypes.c_int]
+    L.rbc_status_string.restype = ctypes.c_char_p
+    L.rbc_set_stream.argtypes = [vp, vp]
+    L.rbc_init_fields.argtypes = [vp, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_double]
+    L.rbc_set_state.argtypes = [vp] + [_dp] * 5
+    L.rbc_get_state.argtypes = [vp] + [_dp] * 5
+    L.rbc_step.argtypes = [vp, ctypes.c_int]
+    L.rbc_step_async.argtypes = [vp, ctypes.c_int]
+    L.rbc_synchronize.argtypes = [vp]
+    L.rbc_nonlinear.argtypes = [vp, ctypes.POINTER(_State), ctypes.POINTER(_State)]
+    L.rbc_tracers_set.argtypes = [vp, _dp, ctypes.c_int]
+    L.rbc_tracers_get.argtypes = [vp, _dp, ctypes.c_int]
+    L.rbc_tracers_seed.argtypes = [vp, ctypes.c_ulonglong]
+    L.rbc_tracers_advance.argtypes = [vp]
+    L.rbc_diagnostics.argtypes = [vp, ctypes.POINTER(_Diag)]
+    L.rbc_diag_history.argtypes = [vp, ctypes.POINTER(_Diag), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.rbc_spectrum.argtypes = [vp, ctypes.c_double, _dp, ctypes.c_int]
+    L.rbc_synthesis.argtypes = [vp, _dp]
+    L.rbc_table.argtypes = [vp, ctypes.c_char_p, _dp, ctypes.POINTER(ctypes.c_int)]
+    L.rbc_galerkin_table.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp, ctypes.POINTER(ctypes.c_int)]
+    L.rbc_stage_times.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]
+    L.rbc_kernel_launches.argtypes = [vp]
+    L.rbc_kernel_launches.restype = ctypes.c_longlong
+    _LIB = L
+    return L
+
+
+def galerkin_table(nz, name):
+    """Galerkin table of the library (host computation; no GPU needed)."""
+    out = np.zeros(max(nz ** 3, 1))
+    cnt = ctypes.c_int(0)
+    st = lib().rbc_galerkin_table(nz, name.encode(), out.ctypes.data_as(_dp), ctypes.byref(cnt))
+    if st != RBC_OK:
+        raise RBCError(st, f"rbc_galerkin_table({nz}, {name})")
+    return out[:cnt.value]
+
+
+def _p(a):
+    assert a.flags["C_CONTIGUOUS"] and a.dtype in (np.float64, np.complex128)
+    return a.ctypes.data_as(_dp)
+
+
+class Solver:
+    """One RBC run on one GPU (mirrors the reference's operator set, see include/rbc.h)."""
+
+    def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0):
+        self.nx, self.ny, self.L = nx, ny, nz
+        self.mox = nx // 2 + 1
+        self.n_tracers = n_tracers
+        self.params = dict(nx=nx, ny=ny, nz=nz, lx=lx, ly=ly, ra=ra, pr=pr, dt=dt, form=form)
+        p = _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity)
+        h = ctypes.c_void_p()
+        st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
+        if st != RBC_OK:
+            raise RBCError(st, "rbc_create failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().rbc_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, st):
+        if st != RBC_OK:
+            raise RBCError(st, lib().rbc_last_error(self.h).decode())
+
+    def _bufs(self):
+        shp = (self.L, self.ny, self.mox)
+        return [np.zeros(shp, np.complex128) for _ in range(3)] + [np.zeros(self.L, np.complex128) for _ in range(2)]
+
+    # fields
+    def init_fields(self, seed, amplitude=1e-3, kmax=4.0):
+        self._check(lib().rbc_init_fields(self.h, seed, amplitude, kmax))
+
+    def set_state(self, theta, f, g, F, G):
+        a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (theta, f, g, F, G)]
+        self._check(lib().rbc_set_state(self.h, *[_p(x) for x in a]))
+
+    def get_state(self):
+        b = self._bufs()
+        self._check(lib().rbc_get_state(self.h, *[_p(x) for x in b]))
+        return b
+
+    # step
+    def step(self, n=1):
+        self._check(lib().rbc_step(self.h, n))
+
+    def step_async(self, n=1):
+        self._check(lib().rbc_step_async(self.h, n))
+
+    def synchronize(self):
+        self._check(lib().rbc_synchronize(self.h))
+
+    def set_stream(self, stream_ptr):
+        self._check(lib().rbc_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    @property
+    def kernel_launches(self):
+        return lib().rbc_kernel_launches(self.h)
+
+    STAGES = ("synth_columns", "rows_c2r", "tracers", "contract", "rows_r2c", "columns_combine", "update")
+
+    def stage_times(self, nsteps):
+        """Runs nsteps steps with CUDA events around each kernel; mean ms per launch."""
+        ms = np.zeros(7)
+        cnt = (ctypes.c_int * 7)()
+        self._check(lib().rbc_stage_times(self.h, nsteps, _p(ms), cnt))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.STAGES)}
+
+    # operator
+    def nonlinear(self, theta, f, g, F, G):
+        a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (theta, f, g, F, G)]
+        out = self._bufs()
+        si = _State(*[x.ctypes.data for x in a])
+        so = _State(*[x.ctypes.data for x in out])
+        self._check(lib().rbc_nonlinear(self.h, ctypes.byref(si), ctypes.byref(so)))
+        return out
+
+    def synthesis(self):
+        out = np.zeros((8, self.L, self.ny, self.nx))
+        self._check(lib().rbc_synthesis(self.h, _p(out)))
+        return out
+
+    # tracers
+    def tracers_set(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self._check(lib().rbc_tracers_set(self.h, _p(xyz), xyz.size // 3))
+
+    def tracers_get(self):
+        out = np.zeros(3 * self.n_tracers)
+        self._check(lib().rbc_tracers_get(self.h, _p(out), self.n_tracers))
+        return out
+
+    def tracers_seed(self, seed):
+        self._check(lib().rbc_tracers_seed(self.h, seed))
+
+    def tracers_advance(self):
+        self._check(lib().rbc_tracers_advance(self.h))
+
+    # diagnostics
+    def diagnostics(self):
+        d = _Diag()
+        self._check(lib().rbc_diagnostics(self.h, ctypes.byref(d)))
+        return {"nu_wall": d.nu_wall, "nu_vol": d.nu_vol, "ke": d.ke, "step": d.step}
+
+    def diag_history(self, n):
+        arr = (_Diag * max(1, n))()
+        cnt = ctypes.c_int(0)
+        self._check(lib().rbc_diag_history(self.h, arr, n, ctypes.byref(cnt)))
+        return np.array([(d.nu_wall, d.nu_vol, d.ke, d.step) for d in arr[:cnt.value]]).reshape(-1, 4)
+
+    def spectrum(self, nbins, z=0.0):
+        out = np.zeros(nbins)
+        self._check(lib().rbc_spectrum(self.h, z, _p(out), nbins))
+        return out
+
+    def table(self, name):
+        L = self.L
+        out = np.zeros(L ** 3)
+        cnt = ctypes.c_int(0)
+        self._check(lib().rbc_table(self.h, name.encode(), _p(out), ctypes.byref(cnt)))
+        return out[:cnt.value]

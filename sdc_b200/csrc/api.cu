@@ -1,0 +1,998 @@
+// api.cu -- C ABI (include/rbc.h) of the B200-native RBC step: handle, device buffers,
+// launch sequence, layout conversion, spectrum. Kernels live in the *.cuh headers.
+#include "../../include/rbc.h"
+#include "common.cuh"
+#include "contract_kernel.cuh"
+#include "fft.cuh"
+#include "galerkin.h"
+#include "step_kernels.cuh"
+#include "tracer_kernel.cuh"
+#include "update_kernel.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace rbck;
+
+// ------------------------------------------------------------------ helpers
+namespace {
+
+struct CudaError {
+    cudaError_t e;
+    const char* what;
+};
+
+#define RBC_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) throw CudaError{e_, #call};                               \
+    } while (0)
+
+struct ArgError {
+    std::string msg;
+};
+
+template <typename T> T* dalloc(size_t n, std::vector<void*>& owned)
+{
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    RBC_CUDA(cudaMalloc(&p, n * sizeof(T)));
+    owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+bool fft_len_ok(int n)
+{
+    if (n < 8 || n > 1024 || (n & 1)) return false;
+    while (n % 2 == 0) n /= 2;
+    while (n % 3 == 0) n /= 3;
+    return n == 1;
+}
+
+} // namespace
+
+// ------------------------------------------------------------------ handle
+struct rbc_handle {
+    rbc_params prm{};
+    rbchost::GridInfo gi;
+    rbchost::Tables tab;
+    Geom G{};
+    int W = 4, NP = 8;
+    bool mixed = false;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    std::vector<void*> owned;
+    // state (FP64, CM) and AB2 history
+    double2 *th = nullptr, *f = nullptr, *g = nullptr, *FG = nullptr;
+    double2 *hist = nullptr, *hFG = nullptr;
+    bool have_hist = false;
+    // operators
+    int* cls = nullptr;
+    double *binv = nullptr, *imp = nullptr, *diag_tab = nullptr;
+    void* coef = nullptr; // R
+    double2 *twx = nullptr, *twy = nullptr;
+    rbcfft::Plan px{}, py{};
+    // scratch (R precision)
+    void *H = nullptr, *phys = nullptr, *grp = nullptr, *gh = nullptr, *N = nullptr;
+    double* NFG = nullptr;
+    // diagnostics
+    double *partial = nullptr, *th00 = nullptr, *ring = nullptr;
+    unsigned int* ticket = nullptr;
+    long long* step_counter = nullptr;
+    int* err = nullptr;
+    int ring_cap = 4096;
+    int upd_blocks = 0;
+    long long host_steps = 0;
+    // staging for layout conversion
+    double2* stage = nullptr;
+    // tracers
+    int ntr = 0;
+    double* trpos = nullptr;      // [3][ntr]
+    double* zbasis = nullptr;     // [128][3][L]
+    bool tracer_pending = false;  // a fluid step ran whose tracer advance is not done yet
+    long long launches = 0;
+    // stage timing: events recorded around each launch while `profiling`
+    bool profiling = false;
+    struct Mark { int stage; cudaEvent_t a, b; };
+    std::vector<Mark> marks;
+    std::string last_error;
+};
+
+static rbc_status fail(rbc_handle* h, rbc_status s, const std::string& m)
+{
+    if (h) h->last_error = m;
+    return s;
+}
+
+// Stage ids for rbc_stage_times.
+enum { ST_SYNTH = 0, ST_C2R, ST_TRACER, ST_CONTRACT, ST_R2C, ST_COMBINE, ST_UPDATE };
+struct StageScope {
+    rbc_handle* h;
+    int stage;
+    cudaEvent_t a = nullptr;
+    StageScope(rbc_handle* h_, int s) : h(h_), stage(s)
+    {
+        if (h->profiling) {
+            cudaEventCreate(&a);
+            cudaEventRecord(a, h->stream);
+        }
+    }
+    ~StageScope()
+    {
+        if (h->profiling) {
+            cudaEvent_t b;
+            cudaEventCreate(&b);
+            cudaEventRecord(b, h->stream);
+            h->marks.push_back({stage, a, b});
+        }
+    }
+};
+
+// ------------------------------------------------------------------ layout kernels
+// reference [L][Ny][mox] <-> CM [L][ckp][Ny]; set applies the 2/3 mask.
+__global__ void k_ref_to_cm(const double2* __restrict__ src, double2* __restrict__ dst, Geom G, int nmat)
+{
+    const size_t n = (size_t)nmat * G.ckp * G.ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e % G.ny);
+        const size_t t = e / G.ny;
+        const int c = (int)(t % G.ckp);
+        const int k = (int)(t / G.ckp);
+        double2 v = make_double2(0, 0);
+        if (c < G.ckeep && row_kept(r, G.ny)) v = src[((size_t)k * G.ny + r) * G.mox + c];
+        dst[e] = v;
+    }
+}
+__global__ void k_cm_to_ref(const double2* __restrict__ src, double2* __restrict__ dst, Geom G, int nmat)
+{
+    const size_t n = (size_t)nmat * G.ny * G.mox;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % G.mox);
+        const size_t t = e / G.mox;
+        const int r = (int)(t % G.ny);
+        const int k = (int)(t / G.ny);
+        double2 v = make_double2(0, 0);
+        if (c < G.ckp) v = src[((size_t)k * G.ckp + c) * G.ny + r];
+        dst[e] = v;
+    }
+}
+
+// Spectrum: one CTA per bin, deterministic block reduction over the half spectrum
+// (energy_spectrum_2d.cu:85-129 bins; theta(z) = sum_i S_i(z) theta_i per wavenumber).
+__global__ void k_spectrum(const double2* __restrict__ th, Geom G, double z, int nbins, double* __restrict__ bins)
+{
+    const int b = blockIdx.x;
+    const double mmx = 2.0 * kPi * (G.mox - 1) / G.lx, mmy = 2.0 * kPi * (G.ny / 2) / G.ly;
+    const double inc = sqrt(mmx * mmx + mmy * mmy) / ((double)nbins);
+    const double lo = b * inc, hi = (b + 1) * inc;
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < G.ckeep * G.ny; e += blockDim.x) {
+        const int c = e / G.ny, r = e - c * G.ny;
+        const double cx = 2.0 * kPi * c / G.lx;
+        const double cy = r <= G.ny / 2 ? 2.0 * kPi * r / G.ly : 2.0 * kPi * (G.ny - r) / G.ly;
+        const double a = sqrt(cx * cx + cy * cy);
+        if (lo <= a && hi > a) {
+            double2 v = make_double2(0, 0);
+            for (int i = 0; i < G.L; ++i) {
+                const double s = sin(kPi * (i + 1) * (z + 0.5));
+                const double2 t = th[((size_t)i * G.ckp + c) * G.ny + r];
+                v = make_double2(v.x + s * t.x, v.y + s * t.y);
+            }
+            acc += v.x * v.x + v.y * v.y;
+        }
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bins[b] = red[0];
+}
+
+// ------------------------------------------------------------------ dispatch
+template <typename R, int L> static void launch_contract(rbc_handle* h)
+{
+    const int smem = (int)(rbcprog::NUNIT * L * L * rbcprog::half_len(L) * sizeof(R));
+    static bool attr = false;
+    if (!attr) {
+        RBC_CUDA(cudaFuncSetAttribute(k_contract<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr = true;
+    }
+    int nsm = 148;
+    int dev = 0;
+    RBC_CUDA(cudaGetDevice(&dev));
+    RBC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    int per = 0;
+    RBC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_contract<R, L>, 128, smem));
+    if (per < 1) per = 1;
+    const int need = (h->G.P + 127) / 128;
+    const int grid = need < nsm * per ? need : nsm * per;
+    StageScope sc(h, ST_CONTRACT);
+    k_contract<R, L><<<grid, 128, smem, h->stream>>>((const R*)h->phys, (R*)h->grp, (const R*)h->coef, h->G.P);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
+template <typename R, int L> static void launch_update(rbc_handle* h)
+{
+    UpdateArgs A;
+    A.G = h->G;
+    A.cls = h->cls;
+    A.binv = h->binv;
+    A.imp = h->imp;
+    A.diag_tab = h->diag_tab;
+    A.N = h->N;
+    A.NFG = h->NFG;
+    A.th = h->th;
+    A.f = h->f;
+    A.g = h->g;
+    A.FG = h->FG;
+    A.hist = h->hist;
+    A.hFG = h->hFG;
+    A.first = h->have_hist ? 0 : 1;
+    A.partial = h->partial;
+    A.ticket = h->ticket;
+    A.th00 = h->th00;
+    A.ring = h->ring;
+    A.ring_cap = h->ring_cap;
+    A.step_counter = h->step_counter;
+    A.err = h->err;
+    StageScope sc(h, ST_UPDATE);
+    k_update<R, L><<<h->upd_blocks, kThreads, 0, h->stream>>>(A);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
+#define RBC_DISPATCH_L(FN, R, Lv, h)                                                    \
+    switch (Lv) {                                                                         \
+    case 2: FN<R, 2>(h); break;                                                           \
+    case 3: FN<R, 3>(h); break;                                                           \
+    case 4: FN<R, 4>(h); break;                                                           \
+    case 5: FN<R, 5>(h); break;                                                           \
+    case 6: FN<R, 6>(h); break;                                                           \
+    case 8: FN<R, 8>(h); break;                                                           \
+    default: throw ArgError{"unsupported number of vertical modes"};                      \
+    }
+
+static bool L_supported(int L, bool mixed)
+{
+    (void)mixed;
+    return L == 2 || L == 3 || L == 4 || L == 5 || L == 6 || L == 8;
+}
+
+template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
+{
+    return sizeof(typename cplx_t<R>::type) * (size_t)h->G.ny * (1 + (size_t)nfield * h->W);
+}
+template <typename R> static size_t smem_combine(const rbc_handle* h)
+{
+    return smem_cols<R>(h, 1) + 3 * sizeof(double2) * (size_t)h->W * h->G.ny;
+}
+template <typename R> static size_t smem_rows(const rbc_handle* h)
+{
+    return sizeof(typename cplx_t<R>::type) * (size_t)h->G.nx * (1 + (size_t)h->NP);
+}
+
+// Synthesis: K1 (columns) + K2 (rows) into h->phys from the state in (th, f, g, FG).
+template <typename R>
+static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, const double2* g, const double2* FG)
+{
+    typedef typename cplx_t<R>::type C;
+    const Geom& G = h->G;
+    dim3 g1(G.ckw / h->W, G.L);
+    {
+    StageScope sc(h, ST_SYNTH);
+    k_synth_columns<R><<<g1, kThreads, smem_cols<R>(h, 8), h->stream>>>(G, h->W, h->py, h->twy, th, f, g, FG, (C*)h->H);
+    RBC_CUDA(cudaGetLastError());
+    }
+    const int rows = 8 * G.L * G.ny;
+    StageScope sc(h, ST_C2R);
+    k_rows_c2r<R><<<rows / (2 * h->NP), kThreads, smem_rows<R>(h), h->stream>>>(G, h->NP, h->px, h->twx, (const C*)h->H, (R*)h->phys);
+    RBC_CUDA(cudaGetLastError());
+    h->launches += 2;
+}
+
+// Nonlinear operator from phys into N / NFG: K3 + K4 + K5 over the columns of G.
+template <typename R> static void run_analysis(rbc_handle* h, const Geom& G)
+{
+    typedef typename cplx_t<R>::type C;
+    RBC_DISPATCH_L(launch_contract, R, G.L, h);
+    const int rows = 13 * G.L * G.ny;
+    {
+    StageScope sc(h, ST_R2C);
+    k_rows_r2c<R><<<rows / (2 * h->NP), kThreads, smem_rows<R>(h), h->stream>>>(G, h->NP, h->px, h->twx, (const R*)h->grp, (C*)h->gh);
+    RBC_CUDA(cudaGetLastError());
+    }
+    dim3 g5(G.ckw / h->W, G.L);
+    StageScope sc(h, ST_COMBINE);
+    k_columns_combine<R><<<g5, kThreads, smem_combine<R>(h), h->stream>>>(G, h->W, h->py, h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
+    RBC_CUDA(cudaGetLastError());
+    h->launches += 2;
+}
+
+
+// ------------------------------------------------------------------ tracers
+// 128 z levels of particle_tracer.cu:151-154 and the basis values of
+// calculate_velocity_operator.cu:458-488 (get_z_coeff_at), host FP64.
+static void tracer_setup(rbc_handle* h)
+{
+    h->ntr = h->prm.n_tracers;
+    if (h->ntr == 0) return;
+    const int L = h->G.L;
+    const double zmax = 0.5f - 1e-3;
+    std::vector<double> zb((size_t)kZNum * 3 * L);
+    for (int l = 0; l < kZNum; ++l) {
+        double z = -zmax + l * (zmax - -zmax) / (kZNum - 1);
+        if (z < -0.5) z = -0.5;
+        else if (z > 0.5) z = 0.5;
+        for (int i = 0; i < L; ++i) {
+            const int m = i + 1;
+            const double lam = h->tab.lambda[i], lz = lam * z;
+            double C, D;
+            if (m % 2 == 1) {
+                const double ich = 1.0 / std::cosh(lam * 0.5), ic = 1.0 / std::cos(lam * 0.5);
+                C = std::cosh(lz) * ich - std::cos(lz) * ic;
+                D = lam * (std::sinh(lz) * ich + std::sin(lz) * ic);
+            } else {
+                const double ish = 1.0 / std::sinh(lam * 0.5), is = 1.0 / std::sin(lam * 0.5);
+                C = std::sinh(lz) * ish - std::sin(lz) * is;
+                D = lam * (std::cosh(lz) * ish - std::cos(lz) * is);
+            }
+            zb[((size_t)l * 3 + 0) * L + i] = C;
+            zb[((size_t)l * 3 + 1) * L + i] = std::sin(kPi * m * (z + 0.5));
+            zb[((size_t)l * 3 + 2) * L + i] = D;
+        }
+    }
+    h->zbasis = dalloc<double>(zb.size(), h->owned);
+    RBC_CUDA(cudaMemcpy(h->zbasis, zb.data(), zb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->trpos = dalloc<double>(3 * (size_t)h->ntr, h->owned);
+    RBC_CUDA(cudaMemset(h->trpos, 0, 3 * (size_t)h->ntr * sizeof(double)));
+}
+
+template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
+{
+    TracerArgs A;
+    A.phys = h->phys;
+    A.zbasis = h->zbasis;
+    A.pos = h->trpos;
+    A.n = h->ntr;
+    A.nx = h->G.nx;
+    A.ny = h->G.ny;
+    A.L = L;
+    A.lx = h->G.lx;
+    A.ly = h->G.ly;
+    A.dt = h->G.dt;
+    A.zmax = 0.5f - 1e-3;
+    StageScope sc(h, ST_TRACER);
+    k_tracers<R, L><<<(h->ntr + 127) / 128, 128, 0, h->stream>>>(A);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
+// Tracer advance with the velocity of the synthesis currently in h->phys.
+template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h)
+{
+    if (h->ntr == 0) return;
+    RBC_DISPATCH_L(launch_tracer_L, R, h->G.L, h);
+}
+
+// One iteration of the reference loop (main.cu:612-637). The tracer advance of a step
+// needs the velocity of the state after it, which is exactly the synthesis the next
+// step starts with; it is therefore run there (or by flush_tracers).
+template <typename R> static void run_step(rbc_handle* h)
+{
+    run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
+    if (h->tracer_pending) launch_tracer_from_synthesis<R>(h);
+    h->tracer_pending = false;
+    run_analysis<R>(h, h->G);
+    RBC_DISPATCH_L(launch_update, R, h->G.L, h);
+    h->have_hist = true;
+    h->tracer_pending = h->ntr > 0;
+    ++h->host_steps;
+}
+
+template <typename R> static void flush_tracers_t(rbc_handle* h)
+{
+    if (!h->tracer_pending) return;
+    run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
+    launch_tracer_from_synthesis<R>(h);
+    h->tracer_pending = false;
+}
+static void flush_tracers(rbc_handle* h)
+{
+    if (h->mixed) flush_tracers_t<float>(h);
+    else flush_tracers_t<double>(h);
+}
+
+template <typename R> static void set_attributes(rbc_handle* h)
+{
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols<R>(h, 8)));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_combine<R>(h)));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows<R>(h)));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows<R>(h)));
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* rbc_status_string(rbc_status s)
+{
+    switch (s) {
+    case RBC_OK: return "ok";
+    case RBC_ERR_INVALID_ARG: return "invalid argument";
+    case RBC_ERR_CUDA: return "CUDA error";
+    case RBC_ERR_NAN: return "non-finite value in the state";
+    case RBC_ERR_TIMEOUT: return "timeout";
+    case RBC_ERR_IO: return "I/O error";
+    case RBC_ERR_UNSUPPORTED: return "unsupported";
+    case RBC_ERR_OUT_OF_MEMORY: return "out of device memory";
+    }
+    return "unknown status";
+}
+
+const char* rbc_last_error(const rbc_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+static void free_all(rbc_handle* h)
+{
+    for (void* p : h->owned) cudaFree(p);
+    h->owned.clear();
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    h->own_stream = nullptr;
+}
+
+void rbc_destroy(rbc_handle* h)
+{
+    if (!h) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(h->prm.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    cudaSetDevice(cur);
+    delete h;
+}
+
+static void twiddles(int n, std::vector<double2>& tw)
+{
+    tw.resize(n);
+    for (int t = 0; t < n; ++t) {
+        const long double a = -2.0L * 3.14159265358979323846264338327950288L * t / n;
+        tw[t] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+}
+
+rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
+{
+    if (!p || !out) return RBC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!fft_len_ok(p->nx) || !fft_len_ok(p->ny)) return RBC_ERR_INVALID_ARG;
+    if (!(p->lx > 0 && p->ly > 0 && p->pr > 0 && p->dt > 0) || p->n_tracers < 0) return RBC_ERR_INVALID_ARG;
+    if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED) return RBC_ERR_INVALID_ARG;
+    if (!L_supported(p->nz, p->form == RBC_FORM_MIXED)) return RBC_ERR_UNSUPPORTED;
+    rbc_handle* h = new rbc_handle;
+    h->prm = *p;
+    h->mixed = p->form == RBC_FORM_MIXED;
+    if (p->diag_capacity > 0) h->ring_cap = p->diag_capacity;
+    try {
+        RBC_CUDA(cudaSetDevice(p->device));
+        rbchost::grid_info(p->nx, p->ny, p->nz, p->lx, p->ly, p->ra, p->pr, p->dt, h->gi);
+        rbchost::build_tables(p->nz, h->tab);
+        const size_t csz = h->mixed ? sizeof(float2) : sizeof(double2);
+        // column block: 8 synthesis columns per (W, Ny) tile within ~200 KB of shared memory
+        int W = 8;
+        while (W > 1 && ((size_t)8 * W * p->ny + p->ny) * csz > 200 * 1024) W /= 2;
+        while (W > 1 && W * p->ny > 8 * kThreads) W /= 2;
+        h->W = W;
+        int NP = 8;
+        while (NP > 1 && ((p->ny / 2) % NP != 0)) NP /= 2;
+        h->NP = NP;
+        Geom& G = h->G;
+        G.nx = p->nx;
+        G.ny = p->ny;
+        G.mox = p->nx / 2 + 1;
+        G.L = p->nz;
+        G.ckeep = h->gi.ckeep;
+        G.ckw = ((G.ckeep + W - 1) / W) * W;
+        G.ckp = ((G.mox + W - 1) / W) * W;
+        G.P = p->nx * p->ny;
+        G.lx = p->lx;
+        G.ly = p->ly;
+        G.pr = p->pr;
+        G.dt = p->dt;
+        h->px = rbcfft::make_plan(p->nx);
+        h->py = rbcfft::make_plan(p->ny);
+        RBC_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        h->stream = h->own_stream;
+        const int L = G.L;
+        const size_t plane = (size_t)G.ckp * G.ny;
+        h->th = dalloc<double2>(plane * L, h->owned);
+        h->f = dalloc<double2>(plane * L, h->owned);
+        h->g = dalloc<double2>(plane * L, h->owned);
+        h->FG = dalloc<double2>(2 * L, h->owned);
+        h->hist = dalloc<double2>(3 * plane * L, h->owned);
+        h->hFG = dalloc<double2>(2 * L, h->owned);
+        // operators
+        rbchost::OperatorTables op;
+        rbchost::build_operator_tables(h->gi, h->tab, op);
+        std::vector<int> cls_cm(plane, -1);
+        for (int c = 0; c < G.ckeep; ++c)
+            for (int r = 0; r < G.ny; ++r) cls_cm[(size_t)c * G.ny + r] = op.cls[(size_t)r * G.mox + c];
+        h->cls = dalloc<int>(plane, h->owned);
+        h->binv = dalloc<double>(op.binv.size(), h->owned);
+        h->imp = dalloc<double>(op.imp.size(), h->owned);
+        RBC_CUDA(cudaMemcpy(h->cls, cls_cm.data(), plane * sizeof(int), cudaMemcpyHostToDevice));
+        RBC_CUDA(cudaMemcpy(h->binv, op.binv.data(), op.binv.size() * sizeof(double), cudaMemcpyHostToDevice));
+        RBC_CUDA(cudaMemcpy(h->imp, op.imp.data(), op.imp.size() * sizeof(double), cudaMemcpyHostToDevice));
+        std::vector<double> dtab;
+        dtab.insert(dtab.end(), h->tab.CpCp.begin(), h->tab.CpCp.end());
+        dtab.insert(dtab.end(), h->tab.CC.begin(), h->tab.CC.end());
+        dtab.insert(dtab.end(), h->tab.CS.begin(), h->tab.CS.end());
+        h->diag_tab = dalloc<double>(dtab.size(), h->owned);
+        RBC_CUDA(cudaMemcpy(h->diag_tab, dtab.data(), dtab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        std::vector<double> coef;
+        rbchost::pack_contraction(h->tab, coef);
+        if (h->mixed) {
+            std::vector<float> cf(coef.begin(), coef.end());
+            h->coef = dalloc<float>(cf.size(), h->owned);
+            RBC_CUDA(cudaMemcpy(h->coef, cf.data(), cf.size() * sizeof(float), cudaMemcpyHostToDevice));
+        } else {
+            h->coef = dalloc<double>(coef.size(), h->owned);
+            RBC_CUDA(cudaMemcpy(h->coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        std::vector<double2> tw;
+        twiddles(G.nx, tw);
+        h->twx = dalloc<double2>(G.nx, h->owned);
+        RBC_CUDA(cudaMemcpy(h->twx, tw.data(), G.nx * sizeof(double2), cudaMemcpyHostToDevice));
+        twiddles(G.ny, tw);
+        h->twy = dalloc<double2>(G.ny, h->owned);
+        RBC_CUDA(cudaMemcpy(h->twy, tw.data(), G.ny * sizeof(double2), cudaMemcpyHostToDevice));
+        // scratch
+        const size_t rsz = h->mixed ? sizeof(float) : sizeof(double);
+        h->H = dalloc<unsigned char>(8 * plane * L * csz, h->owned);
+        h->phys = dalloc<unsigned char>((size_t)8 * L * G.P * rsz, h->owned);
+        h->grp = dalloc<unsigned char>((size_t)13 * L * G.P * rsz, h->owned);
+        h->gh = dalloc<unsigned char>(13 * plane * L * csz, h->owned);
+        h->N = dalloc<unsigned char>(3 * plane * L * csz, h->owned);
+        h->NFG = dalloc<double>(2 * L, h->owned);
+        h->upd_blocks = (G.ckeep * G.ny + kThreads - 1) / kThreads;
+        h->partial = dalloc<double>(2 * (size_t)h->upd_blocks, h->owned);
+        h->th00 = dalloc<double>(L, h->owned);
+        h->ring = dalloc<double>(4 * (size_t)h->ring_cap, h->owned);
+        h->ticket = dalloc<unsigned int>(1, h->owned);
+        h->step_counter = dalloc<long long>(1, h->owned);
+        h->err = dalloc<int>(1, h->owned);
+        h->stage = dalloc<double2>((size_t)G.ny * G.mox * L, h->owned);
+        RBC_CUDA(cudaMemset(h->ticket, 0, sizeof(unsigned int)));
+        RBC_CUDA(cudaMemset(h->step_counter, 0, sizeof(long long)));
+        RBC_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+        RBC_CUDA(cudaMemset(h->ring, 0, 4 * (size_t)h->ring_cap * sizeof(double)));
+        RBC_CUDA(cudaMemset(h->th, 0, plane * L * sizeof(double2)));
+        RBC_CUDA(cudaMemset(h->f, 0, plane * L * sizeof(double2)));
+        RBC_CUDA(cudaMemset(h->g, 0, plane * L * sizeof(double2)));
+        RBC_CUDA(cudaMemset(h->FG, 0, 2 * L * sizeof(double2)));
+        RBC_CUDA(cudaMemset(h->hist, 0, 3 * plane * L * sizeof(double2)));
+        RBC_CUDA(cudaMemset(h->hFG, 0, 2 * L * sizeof(double2)));
+        RBC_CUDA(cudaMemset(h->H, 0, 8 * plane * L * csz));
+        RBC_CUDA(cudaMemset(h->gh, 0, 13 * plane * L * csz));
+        RBC_CUDA(cudaMemset(h->N, 0, 3 * plane * L * csz));
+        if (h->mixed) set_attributes<float>(h);
+        else set_attributes<double>(h);
+        tracer_setup(h);
+        RBC_CUDA(cudaDeviceSynchronize());
+    } catch (const CudaError& e) {
+        std::string m = std::string("rbc_create: ") + e.what + ": " + cudaGetErrorString(e.e);
+        std::fprintf(stderr, "%s\n", m.c_str());
+        const bool oom = e.e == cudaErrorMemoryAllocation;
+        free_all(h);
+        delete h;
+        return oom ? RBC_ERR_OUT_OF_MEMORY : RBC_ERR_CUDA;
+    } catch (const ArgError& e) {
+        free_all(h);
+        delete h;
+        return RBC_ERR_UNSUPPORTED;
+    }
+    *out = h;
+    return RBC_OK;
+}
+
+rbc_status rbc_set_stream(rbc_handle* h, void* stream)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return RBC_OK;
+}
+
+#define RBC_GUARD(h)                                                                        \
+    if (!h) return RBC_ERR_INVALID_ARG;                                                     \
+    try {                                                                                   \
+        RBC_CUDA(cudaSetDevice(h->prm.device));
+#define RBC_GUARD_END(h)                                                                    \
+    }                                                                                       \
+    catch (const CudaError& e) {                                                            \
+        return fail(h, e.e == cudaErrorMemoryAllocation ? RBC_ERR_OUT_OF_MEMORY : RBC_ERR_CUDA, \
+                    std::string(e.what) + ": " + cudaGetErrorString(e.e));                   \
+    }                                                                                       \
+    catch (const ArgError& e) {                                                             \
+        return fail(h, RBC_ERR_UNSUPPORTED, e.msg);                                         \
+    }
+
+static void upload_field(rbc_handle* h, const double* src, double2* dst, int nmat)
+{
+    const size_t n = (size_t)h->G.ny * h->G.mox * nmat;
+    RBC_CUDA(cudaMemcpyAsync(h->stage, src, n * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    k_ref_to_cm<<<512, 256, 0, h->stream>>>(h->stage, dst, h->G, nmat);
+    RBC_CUDA(cudaGetLastError());
+}
+static void download_field(rbc_handle* h, const double2* src, double* dst, int nmat)
+{
+    const size_t n = (size_t)h->G.ny * h->G.mox * nmat;
+    k_cm_to_ref<<<512, 256, 0, h->stream>>>(src, h->stage, h->G, nmat);
+    RBC_CUDA(cudaGetLastError());
+    RBC_CUDA(cudaMemcpyAsync(dst, h->stage, n * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+rbc_status rbc_set_state(rbc_handle* h, const double* th, const double* f, const double* g, const double* F, const double* G)
+{
+    if (!th || !f || !g || !F || !G) return fail(h, RBC_ERR_INVALID_ARG, "null state buffer");
+    RBC_GUARD(h)
+    flush_tracers(h);
+    const int L = h->G.L;
+    upload_field(h, th, h->th, L);
+    upload_field(h, f, h->f, L);
+    upload_field(h, g, h->g, L);
+    std::vector<double2> fg(2 * L);
+    std::memcpy(fg.data(), F, L * sizeof(double2));
+    std::memcpy(fg.data() + L, G, L * sizeof(double2));
+    RBC_CUDA(cudaMemcpyAsync(h->FG, fg.data(), 2 * L * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    h->have_hist = false;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_get_state(rbc_handle* h, double* th, double* f, double* g, double* F, double* G)
+{
+    if (!th || !f || !g || !F || !G) return fail(h, RBC_ERR_INVALID_ARG, "null state buffer");
+    RBC_GUARD(h)
+    const int L = h->G.L;
+    download_field(h, h->th, th, L);
+    download_field(h, h->f, f, L);
+    download_field(h, h->g, g, L);
+    std::vector<double2> fg(2 * L);
+    RBC_CUDA(cudaMemcpyAsync(fg.data(), h->FG, 2 * L * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    std::memcpy(F, fg.data(), L * sizeof(double2));
+    std::memcpy(G, fg.data() + L, L * sizeof(double2));
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_init_fields(rbc_handle* h, unsigned long long seed, double amplitude, double kmax)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    const int L = h->G.L;
+    const size_t n = (size_t)h->G.ny * h->G.mox * L;
+    std::vector<double> th(2 * n), zero(2 * n, 0.0), fg(2 * L, 0.0);
+    rbchost::seeded_theta(h->gi, seed, amplitude, kmax, th.data());
+    return rbc_set_state(h, th.data(), zero.data(), zero.data(), fg.data(), fg.data());
+}
+
+static rbc_status check_err(rbc_handle* h)
+{
+    int e = 0;
+    RBC_CUDA(cudaMemcpyAsync(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    if (e & RBC_DEVERR_NAN) return fail(h, RBC_ERR_NAN, "non-finite value in the state");
+    if (e) return fail(h, RBC_ERR_CUDA, "device error word set");
+    return RBC_OK;
+}
+
+rbc_status rbc_step_async(rbc_handle* h, int nsteps)
+{
+    if (nsteps < 0) return fail(h, RBC_ERR_INVALID_ARG, "negative step count");
+    RBC_GUARD(h)
+    h->launches = 0;
+    for (int s = 0; s < nsteps; ++s) {
+        if (h->mixed) run_step<float>(h);
+        else run_step<double>(h);
+    }
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_synchronize(rbc_handle* h)
+{
+    RBC_GUARD(h)
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    return check_err(h);
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_step(rbc_handle* h, int nsteps)
+{
+    rbc_status s = rbc_step_async(h, nsteps);
+    if (s != RBC_OK) return s;
+    return rbc_synchronize(h);
+}
+
+long long rbc_kernel_launches(const rbc_handle* h) { return h ? h->launches : 0; }
+
+rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts)
+{
+    if (!ms || !counts || nsteps <= 0) return fail(h, RBC_ERR_INVALID_ARG, "bad arguments");
+    RBC_GUARD(h)
+    h->marks.clear();
+    h->profiling = true;
+    for (int s = 0; s < nsteps; ++s) {
+        if (h->mixed) run_step<float>(h);
+        else run_step<double>(h);
+    }
+    flush_tracers(h);
+    h->profiling = false;
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    double tot[RBC_NSTAGE] = {0};
+    int cnt[RBC_NSTAGE] = {0};
+    for (auto& m : h->marks) {
+        float t = 0;
+        cudaEventElapsedTime(&t, m.a, m.b);
+        tot[m.stage] += t;
+        cnt[m.stage] += 1;
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    h->marks.clear();
+    for (int i = 0; i < RBC_NSTAGE; ++i) {
+        ms[i] = cnt[i] ? tot[i] / cnt[i] : 0.0;
+        counts[i] = cnt[i] / nsteps;
+    }
+    return check_err(h);
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_nonlinear(rbc_handle* h, const rbc_state* in, rbc_state* out)
+{
+    if (!in || !out || !in->theta || !in->f || !in->g || !in->F || !in->G || !out->theta || !out->f ||
+        !out->g || !out->F || !out->G)
+        return fail(h, RBC_ERR_INVALID_ARG, "null state buffer");
+    RBC_GUARD(h)
+    const Geom& G = h->G;
+    const int L = G.L;
+    const size_t plane = (size_t)G.ckp * G.ny;
+    // the operator input goes into the history buffer's planes? No: use dedicated scratch
+    // carved from gh (13 L planes of complex R >= 3 L planes of double2 + 2 L).
+    static_assert(sizeof(double2) >= 8, "");
+    double2* tmp = reinterpret_cast<double2*>(h->gh);
+    const size_t need = (3 * plane * L + 2 * L) * sizeof(double2);
+    const size_t have = 13 * plane * L * (h->mixed ? sizeof(float2) : sizeof(double2));
+    if (need > have) throw ArgError{"scratch too small for rbc_nonlinear"};
+    double2* ti = tmp;
+    double2* fi = tmp + plane * L;
+    double2* gi = tmp + 2 * plane * L;
+    double2* FGi = tmp + 3 * plane * L;
+    upload_field(h, in->theta, ti, L);
+    upload_field(h, in->f, fi, L);
+    upload_field(h, in->g, gi, L);
+    std::vector<double2> fg(2 * L);
+    std::memcpy(fg.data(), in->F, L * sizeof(double2));
+    std::memcpy(fg.data() + L, in->G, L * sizeof(double2));
+    RBC_CUDA(cudaMemcpyAsync(FGi, fg.data(), 2 * L * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    if (h->mixed) run_synthesis<float>(h, ti, fi, gi, FGi);
+    else run_synthesis<double>(h, ti, fi, gi, FGi);
+    Geom Gf = G; // every column: the reference operator returns all modes
+    Gf.ckeep = G.mox;
+    Gf.ckw = G.ckp;
+    if (h->mixed) run_analysis<float>(h, Gf);
+    else run_analysis<double>(h, Gf);
+    // N (R precision, CM) -> double2 CM in the stage-adjacent scratch, then reference layout
+    std::vector<double> nfg(2 * L);
+    RBC_CUDA(cudaMemcpyAsync(nfg.data(), h->NFG, 2 * L * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double2> nh(3 * plane * L);
+    if (h->mixed) {
+        std::vector<float2> nf(3 * plane * L);
+        RBC_CUDA(cudaMemcpyAsync(nf.data(), h->N, nf.size() * sizeof(float2), cudaMemcpyDeviceToHost, h->stream));
+        RBC_CUDA(cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < nf.size(); ++i) nh[i] = make_double2(nf[i].x, nf[i].y);
+    } else {
+        RBC_CUDA(cudaMemcpyAsync(nh.data(), h->N, nh.size() * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+        RBC_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    double* outs[3] = {out->theta, out->f, out->g};
+    for (int a = 0; a < 3; ++a) {
+        double2* o = reinterpret_cast<double2*>(outs[a]);
+        std::memset(o, 0, (size_t)L * G.ny * G.mox * sizeof(double2));
+        for (int k = 0; k < L; ++k)
+            for (int c = 0; c < G.mox; ++c)
+                for (int r = 0; r < G.ny; ++r)
+                    o[((size_t)k * G.ny + r) * G.mox + c] = nh[((size_t)(a * L + k) * G.ckp + c) * G.ny + r];
+    }
+    for (int k = 0; k < L; ++k) {
+        out->F[2 * k] = nfg[k];
+        out->F[2 * k + 1] = 0.0;
+        out->G[2 * k] = nfg[L + k];
+        out->G[2 * k + 1] = 0.0;
+    }
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_synthesis(rbc_handle* h, double* out)
+{
+    if (!out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
+    RBC_GUARD(h)
+    const Geom& G = h->G;
+    if (h->mixed) run_synthesis<float>(h, h->th, h->f, h->g, h->FG);
+    else run_synthesis<double>(h, h->th, h->f, h->g, h->FG);
+    const size_t n = (size_t)8 * G.L * G.P;
+    if (h->mixed) {
+        std::vector<float> v(n);
+        RBC_CUDA(cudaMemcpyAsync(v.data(), h->phys, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        RBC_CUDA(cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < n; ++i) out[i] = v[i];
+    } else {
+        RBC_CUDA(cudaMemcpyAsync(out, h->phys, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        RBC_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_diagnostics(rbc_handle* h, rbc_diag* out)
+{
+    int n = 0;
+    if (!out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
+    rbc_status s = rbc_diag_history(h, out, 1, &n);
+    if (s != RBC_OK) return s;
+    if (n == 0) {
+        // no step yet: Nu_wall of the current state only
+        RBC_GUARD(h)
+        std::vector<double2> t((size_t)h->G.L * h->G.ckp * h->G.ny);
+        RBC_CUDA(cudaMemcpyAsync(t.data(), h->th, t.size() * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+        RBC_CUDA(cudaStreamSynchronize(h->stream));
+        double nu = 1.0;
+        for (int k = 0; k < h->G.L; ++k) nu -= (k + 1) * kPi * t[(size_t)k * h->G.ckp * h->G.ny].x;
+        out->nu_wall = nu;
+        out->nu_vol = NAN;
+        out->ke = NAN;
+        out->step = 0;
+        return RBC_OK;
+        RBC_GUARD_END(h)
+    }
+    return RBC_OK;
+}
+
+rbc_status rbc_diag_history(rbc_handle* h, rbc_diag* out, int n, int* count)
+{
+    if (!out || !count || n < 0) return fail(h, RBC_ERR_INVALID_ARG, "bad arguments");
+    RBC_GUARD(h)
+    long long steps = 0;
+    RBC_CUDA(cudaMemcpyAsync(&steps, h->step_counter, sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double> ring(4 * (size_t)h->ring_cap);
+    RBC_CUDA(cudaMemcpyAsync(ring.data(), h->ring, ring.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    long long avail = steps < h->ring_cap ? steps : h->ring_cap;
+    if (avail > n) avail = n;
+    for (long long i = 0; i < avail; ++i) {
+        const long long s = steps - avail + 1 + i; // 1-based step number
+        const double* slot = &ring[4 * (size_t)((s - 1) % h->ring_cap)];
+        out[i].nu_wall = slot[0];
+        out[i].nu_vol = slot[1];
+        out[i].ke = slot[2];
+        out[i].step = (long long)slot[3];
+    }
+    *count = (int)avail;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_spectrum(rbc_handle* h, double z, double* bins, int nbins)
+{
+    if (!bins || nbins <= 0) return fail(h, RBC_ERR_INVALID_ARG, "bad spectrum arguments");
+    RBC_GUARD(h)
+    double* d = reinterpret_cast<double*>(h->N); // scratch: nbins doubles
+    const size_t cap = 3 * (size_t)h->G.ckp * h->G.ny * h->G.L * (h->mixed ? sizeof(float2) : sizeof(double2));
+    if ((size_t)nbins * sizeof(double) > cap) throw ArgError{"too many spectrum bins"};
+    k_spectrum<<<nbins, 256, 0, h->stream>>>(h->th, h->G, z, nbins, d);
+    RBC_CUDA(cudaGetLastError());
+    RBC_CUDA(cudaMemcpyAsync(bins, d, nbins * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+static rbc_status table_by_name(const rbchost::Tables& T, const char* name, double* out, int* count)
+{
+    const int L = T.L;
+    const std::vector<double>* v = nullptr;
+    if (!std::strcmp(name, "Iac")) v = &T.Iac;
+    else if (!std::strcmp(name, "Ia1")) v = &T.Ia1;
+    else if (!std::strcmp(name, "Ibb1")) v = &T.Ibb1;
+    else if (!std::strcmp(name, "Ib11")) v = &T.Ib11;
+    else if (!std::strcmp(name, "I111")) v = &T.I111;
+    else if (!std::strcmp(name, "Iabc")) v = &T.Iabc;
+    else if (!std::strcmp(name, "Iac1")) v = &T.Iac1;
+    else if (!std::strcmp(name, "Iaab")) v = &T.Iaab;
+    else if (!std::strcmp(name, "Iaa1")) v = &T.Iaa1;
+    else if (!std::strcmp(name, "Iab2")) v = &T.Iab2;
+    else if (!std::strcmp(name, "Ia12")) v = &T.Ia12;
+    else if (!std::strcmp(name, "lambda")) v = &T.lambda;
+    else if (!std::strcmp(name, "Ibbb")) {
+        for (int k = 0; k < L; ++k)
+            for (int j = 0; j < L; ++j)
+                for (int i = 0; i < L; ++i) out[i + j * L + k * L * L] = T.ibbb(i, j, k);
+        *count = L * L * L;
+        return RBC_OK;
+    }
+    if (!v) return RBC_ERR_INVALID_ARG;
+    std::memcpy(out, v->data(), v->size() * sizeof(double));
+    *count = (int)v->size();
+    return RBC_OK;
+}
+
+rbc_status rbc_table(rbc_handle* h, const char* name, double* out, int* count)
+{
+    if (!h || !name || !out || !count) return RBC_ERR_INVALID_ARG;
+    const rbc_status s = table_by_name(h->tab, name, out, count);
+    if (s != RBC_OK) return fail(h, s, std::string("unknown table ") + name);
+    return RBC_OK;
+}
+
+rbc_status rbc_galerkin_table(int nz, const char* name, double* out, int* count)
+{
+    if (nz < 1 || nz > 16 || !name || !out || !count) return RBC_ERR_INVALID_ARG;
+    rbchost::Tables T;
+    rbchost::build_tables(nz, T);
+    return table_by_name(T, name, out, count);
+}
+
+rbc_status rbc_tracers_set(rbc_handle* h, const double* xyz, int n)
+{
+    if (!xyz) return fail(h, RBC_ERR_INVALID_ARG, "null positions");
+    if (!h || n != h->ntr) return fail(h, RBC_ERR_INVALID_ARG, "tracer count differs from params.n_tracers");
+    RBC_GUARD(h)
+    h->tracer_pending = false;
+    RBC_CUDA(cudaMemcpyAsync(h->trpos, xyz, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_tracers_get(rbc_handle* h, double* xyz, int n)
+{
+    if (!xyz) return fail(h, RBC_ERR_INVALID_ARG, "null positions");
+    if (!h || n != h->ntr) return fail(h, RBC_ERR_INVALID_ARG, "tracer count differs from params.n_tracers");
+    RBC_GUARD(h)
+    flush_tracers(h);
+    RBC_CUDA(cudaMemcpyAsync(xyz, h->trpos, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_tracers_seed(rbc_handle* h, unsigned long long seed)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    std::vector<double> xyz(3 * (size_t)h->ntr);
+    rbchost::seeded_positions(seed, h->ntr, h->prm.lx, h->prm.ly, xyz.data());
+    return rbc_tracers_set(h, xyz.data(), h->ntr);
+}
+
+rbc_status rbc_tracers_advance(rbc_handle* h)
+{
+    RBC_GUARD(h)
+    if (h->ntr == 0) return RBC_OK;
+    flush_tracers(h);
+    if (h->mixed) run_synthesis<float>(h, h->th, h->f, h->g, h->FG);
+    else run_synthesis<double>(h, h->th, h->f, h->g, h->FG);
+    if (h->mixed) launch_tracer_from_synthesis<float>(h);
+    else launch_tracer_from_synthesis<double>(h);
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+} // extern "C"

@@ -1,0 +1,417 @@
+// galerkin.cpp -- Galerkin integrals, per-wavenumber operators and seeded inputs.
+//
+// The integrals follow the definitions of gpu_flow/code/util/coeff.h:22-47 (basis
+// C_k, S_k on z in (-1/2,1/2), lambda table coeff.cu:1232-1257). They are evaluated
+// here by composite Gauss-Legendre quadrature (8 panels), which reproduces the
+// reference's closed forms (coeff.cu:60-1083) to ~1e-15 of each table's scale for all
+// 3-index tensors the step uses. Iac uses the analytic closed forms (see build_tables).
+// The implicit and inverse-B operators follow linear_implicit_operator.cu:46-197 and
+// inverse_B_matrix.cu:108-160 with a partial-pivot LU in place of GSL.
+#include "galerkin.h"
+#include "contract_prog.h"
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <algorithm>
+
+namespace rbchost {
+
+static const double kPi = 3.14159265358979323846;
+
+static double lambda_k(int k) // k >= 1
+{
+    static const double r[] = {0.0, 1.505618731142, 2.499752670074, 3.500010679436, 4.499999538484,
+                               5.500000019944, 6.499999999138, 7.500000000037, 8.499999999998};
+    return k > 8 ? kPi * (k + 0.5) : kPi * r[k];
+}
+
+// Basis function values: kind 0 = C, 1 = C', 2 = C'', 3 = S, 4 = S'.
+static double basis(int kind, int m, double z)
+{
+    const int k = m + 1;
+    if (kind >= 3) {
+        const double a = k * kPi;
+        return kind == 3 ? std::sin(a * (z + 0.5)) : a * std::cos(a * (z + 0.5));
+    }
+    const double l = lambda_k(k);
+    if (k & 1) {
+        const double ich = 1.0 / std::cosh(0.5 * l), ic = 1.0 / std::cos(0.5 * l);
+        if (kind == 0) return std::cosh(l * z) * ich - std::cos(l * z) * ic;
+        if (kind == 1) return l * (std::sinh(l * z) * ich + std::sin(l * z) * ic);
+        return l * l * (std::cosh(l * z) * ich + std::cos(l * z) * ic);
+    }
+    const double ish = 1.0 / std::sinh(0.5 * l), is = 1.0 / std::sin(0.5 * l);
+    if (kind == 0) return std::sinh(l * z) * ish - std::sin(l * z) * is;
+    if (kind == 1) return l * (std::cosh(l * z) * ish - std::cos(l * z) * is);
+    return l * l * (std::sinh(l * z) * ish + std::sin(l * z) * is);
+}
+
+static bool basis_odd(int kind, int m)
+{
+    const int nder = kind == 1 ? 1 : kind == 2 ? 2 : kind == 4 ? 1 : 0;
+    return ((m & 1) + nder) & 1;
+}
+
+// Composite Gauss-Legendre rule: `panels` panels of n nodes on (-1/2, 1/2).
+static void composite_gl(int panels, int n, std::vector<double>& z, std::vector<double>& w)
+{
+    std::vector<long double> xs(n), ws(n);
+    for (int i = 0; i < n; ++i) {
+        long double t = std::cos(kPi * (i + 0.75) / (n + 0.5)), p1 = 0, p0 = 0, d = 0;
+        for (int it = 0; it < 60; ++it) {
+            p0 = 1;
+            p1 = t;
+            for (int k = 2; k <= n; ++k) {
+                long double p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            d = n * (t * p1 - p0) / (t * t - 1);
+            long double step = p1 / d;
+            t -= step;
+            if (std::fabs((double)step) < 1e-20) break;
+        }
+        xs[i] = t;
+        ws[i] = 2.0L / ((1 - t * t) * d * d);
+    }
+    z.clear();
+    w.clear();
+    const long double h = 1.0L / panels;
+    for (int p = 0; p < panels; ++p) {
+        const long double a = -0.5L + p * h;
+        for (int i = 0; i < n; ++i) {
+            z.push_back((double)(a + 0.5L * h * (xs[i] + 1)));
+            w.push_back((double)(0.5L * h * ws[i]));
+        }
+    }
+}
+
+void build_tables(int L, Tables& T)
+{
+    T.L = L;
+    T.lambda.resize(L);
+    for (int m = 0; m < L; ++m) T.lambda[m] = lambda_k(m + 1);
+    std::vector<double> z, w;
+    composite_gl(8, 24 + 2 * L, z, w);
+    const int nq = (int)z.size();
+    std::vector<double> v(5 * L * nq);
+    for (int kind = 0; kind < 5; ++kind)
+        for (int m = 0; m < L; ++m)
+            for (int q = 0; q < nq; ++q) v[(kind * L + m) * nq + q] = basis(kind, m, z[q]);
+    auto col = [&](int kind, int m) { return &v[(kind * L + m) * nq]; };
+    auto int2 = [&](int ka, int kb, std::vector<double>& out) {
+        out.assign(L * L, 0.0);
+        for (int j = 0; j < L; ++j)
+            for (int i = 0; i < L; ++i) {
+                if (basis_odd(ka, i) != basis_odd(kb, j)) continue;
+                const double *a = col(ka, i), *b = col(kb, j);
+                long double s = 0;
+                for (int q = 0; q < nq; ++q) s += (long double)w[q] * a[q] * b[q];
+                out[i + j * L] = (double)s;
+            }
+    };
+    auto int3 = [&](int ka, int kb, int kc, std::vector<double>& out) {
+        out.assign(L * L * L, 0.0);
+        double mx = 0;
+        for (int k = 0; k < L; ++k)
+            for (int j = 0; j < L; ++j)
+                for (int i = 0; i < L; ++i) {
+                    if ((basis_odd(ka, i) + basis_odd(kb, j) + basis_odd(kc, k)) & 1) continue;
+                    const double *a = col(ka, i), *b = col(kb, j), *c = col(kc, k);
+                    long double s = 0;
+                    for (int q = 0; q < nq; ++q) s += (long double)w[q] * a[q] * b[q] * c[q];
+                    out[i + j * L + k * L * L] = (double)s;
+                    mx = std::max(mx, std::fabs((double)s));
+                }
+        // integrals that cancel to quadrature noise are exact zeros
+        for (double& e : out)
+            if (std::fabs(e) < 1e-13 * mx) e = 0.0;
+    };
+    int2(0, 3, T.Ia1);
+    T.CS = T.Ia1;
+    int2(1, 1, T.CpCp);
+    int2(0, 0, T.CC);
+    // Iac = int C_i C_j'': the analytic values implied by C = C' = 0 at the walls,
+    // evaluated with the tabulated lambda as the reference does (coeff.cu:76-122):
+    // t_m = lambda tan(lambda/2) (odd 1-based m) or lambda cot(lambda/2) (even m);
+    // diagonal -2t - t^2 (odd) / 2t - t^2 (even); odd-odd off-diagonal
+    // 8 l_i^2 l_j^2 (t_j - t_i) / (l_i^4 - l_j^4). Even-even off-diagonal entries are
+    // exactly 0 in the reference (its formula subtracts a term from itself,
+    // coeff.cu:112); that value is kept so the operators match the reference.
+    T.Iac.assign(L * L, 0.0);
+    for (int j = 0; j < L; ++j)
+        for (int i = 0; i < L; ++i) {
+            const int mi = i + 1, mj = j + 1;
+            if ((mi & 1) != (mj & 1)) continue;
+            const double li = T.lambda[i], lj = T.lambda[j];
+            const bool odd = mi & 1;
+            const double ti = odd ? li * std::tan(0.5 * li) : li / std::tan(0.5 * li);
+            const double tj = odd ? lj * std::tan(0.5 * lj) : lj / std::tan(0.5 * lj);
+            if (i == j) T.Iac[i + j * L] = odd ? (-2.0 * ti - ti * ti) : (2.0 * ti - ti * ti);
+            else if (odd) {
+                const double a = li * li, b = lj * lj;
+                T.Iac[i + j * L] = 8.0 * a * b * (tj - ti) / (a * a - b * b);
+            }
+        }
+    // kinds: 0 C, 1 C', 2 C'', 3 S, 4 S'
+    int3(1, 1, 3, T.Ibb1);
+    int3(1, 3, 3, T.Ib11);
+    int3(3, 3, 3, T.I111);
+    int3(0, 1, 2, T.Iabc);
+    int3(0, 2, 3, T.Iac1);
+    int3(0, 0, 1, T.Iaab);
+    int3(0, 0, 3, T.Iaa1);
+    int3(0, 1, 4, T.Iab2);
+    int3(0, 3, 4, T.Ia12);
+}
+
+double family_value(const Tables& T, int f, int i, int j, int k)
+{
+    using namespace rbcprog;
+    switch (f) {
+    case IBBB_IJK: return T.ibbb(i, j, k);
+    case IBB1_IKJ: return T.t3(T.Ibb1, i, k, j);
+    case IB11_KIJ: return T.t3(T.Ib11, k, i, j);
+    case IABC_JIK: return T.t3(T.Iabc, j, i, k);
+    case IAC1_IKJ: return T.t3(T.Iac1, i, k, j);
+    case IAAB_JKI: return T.t3(T.Iaab, j, k, i);
+    case IAA1_IKJ: return T.t3(T.Iaa1, i, k, j);
+    case IAAB_IJK: return T.t3(T.Iaab, i, j, k);
+    case IBB1_IJK: return T.t3(T.Ibb1, i, j, k);
+    case IB11_IJK: return T.t3(T.Ib11, i, j, k);
+    case I111_IJK: return T.t3(T.I111, i, j, k);
+    case IAB2_JIK: return T.t3(T.Iab2, j, i, k);
+    case IA12_IJK: return T.t3(T.Ia12, i, j, k);
+    default: return T.t3(T.Ia12, i, k, j);
+    }
+}
+
+void pack_contraction(const Tables& T, std::vector<double>& coef)
+{
+    using namespace rbcprog;
+    const int L = T.L, H = half_len(L);
+    coef.assign((size_t)NUNIT * L * L * H, 0.0);
+    for (int u = 0; u < NUNIT; ++u) {
+        const Unit U = unit_at(u);
+        const int par = family_parity(U.family);
+        for (int k = 0; k < L; ++k)
+            for (int o = 0; o < L; ++o) {
+                const int s0 = (o + k + par) & 1;
+                for (int h = 0; h < H; ++h) {
+                    const int s = s0 + 2 * h;
+                    if (s >= L) continue;
+                    const int i = U.left ? s : o, j = U.left ? o : s;
+                    coef[(((size_t)u * L + k) * L + o) * H + h] = family_value(T, U.family, i, j, k);
+                }
+            }
+    }
+}
+
+bool lu_invert(int n, const std::vector<double>& Ain, std::vector<double>& inv)
+{
+    std::vector<double> A(Ain);
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+        if (A[piv * n + c] == 0.0) return false;
+        if (piv != c) {
+            for (int j = 0; j < n; ++j) std::swap(A[c * n + j], A[piv * n + j]);
+            std::swap(perm[c], perm[piv]);
+        }
+        const double d = A[c * n + c];
+        for (int r = c + 1; r < n; ++r) {
+            const double l = A[r * n + c] / d;
+            A[r * n + c] = l;
+            for (int j = c + 1; j < n; ++j) A[r * n + j] -= l * A[c * n + j];
+        }
+    }
+    inv.assign(n * n, 0.0);
+    std::vector<double> x(n);
+    for (int e = 0; e < n; ++e) {
+        for (int i = 0; i < n; ++i) {
+            double s = perm[i] == e ? 1.0 : 0.0;
+            for (int j = 0; j < i; ++j) s -= A[i * n + j] * x[j];
+            x[i] = s;
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double s = x[i];
+            for (int j = i + 1; j < n; ++j) s -= A[i * n + j] * x[j];
+            x[i] = s / A[i * n + i];
+        }
+        for (int i = 0; i < n; ++i) inv[i * n + e] = x[i];
+    }
+    return true;
+}
+
+void grid_info(int nx, int ny, int L, double lx, double ly, double ra, double pr, double dt, GridInfo& g)
+{
+    g.nx = nx;
+    g.ny = ny;
+    g.L = L;
+    g.mox = nx / 2 + 1;
+    g.lx = lx;
+    g.ly = ly;
+    g.ra = ra;
+    g.pr = pr;
+    g.dt = dt;
+    // 2/3 rule exactly as dealias_implicit (implicit_explicit_stepping.cu:173-180)
+    g.ckeep = 0;
+    while (g.ckeep < g.mox && !(g.mox - g.ckeep <= (1.0 / 3.0) * g.mox)) ++g.ckeep;
+    g.row_kept.assign(ny, 0);
+    for (int r = 0; r < ny; ++r) g.row_kept[r] = !(std::fabs(0.5 * ny - r) <= (1.0 / 3.0) * 0.5 * ny);
+}
+
+void build_operator_tables(const GridInfo& g, const Tables& T, OperatorTables& op)
+{
+    const int L = g.L, mox = g.mox, ny = g.ny, n2 = 2 * L;
+    op.cls.assign((size_t)ny * mox, -1);
+    std::map<uint64_t, int> seen;
+    std::vector<double> q2s;
+    for (int l = 0; l < ny; ++l) {
+        if (!g.row_kept[l]) continue;
+        for (int k = 0; k < g.ckeep; ++k) {
+            const double mx = k * 2.0 * kPi / g.lx;
+            double my = 2.0 * kPi / g.ly;
+            if (l < ny / 2 + 1) my *= l;
+            else my *= (l - ny);
+            const double q2 = mx * mx + my * my;
+            uint64_t key;
+            std::memcpy(&key, &q2, 8);
+            if (k == 0 && l == 0) key = ~0ULL; // the q = 0 mode has its own operator
+            auto it = seen.find(key);
+            int c;
+            if (it == seen.end()) {
+                c = (int)q2s.size();
+                seen[key] = c;
+                q2s.push_back(q2);
+            } else {
+                c = it->second;
+            }
+            op.cls[(size_t)l * mox + k] = c;
+        }
+    }
+    op.nclass = (int)q2s.size();
+    op.binv.assign((size_t)op.nclass * L * L, 0.0);
+    op.imp.assign((size_t)op.nclass * 4 * L * L, 0.0);
+    for (const auto& kv : seen) {
+        const int c = kv.second;
+        const bool zero = kv.first == ~0ULL;
+        const double q2 = zero ? 0.0 : q2s[c];
+        double* bi = &op.binv[(size_t)c * L * L];
+        double* im = &op.imp[(size_t)c * 4 * L * L];
+        // B_ff = q^2 (q^2 delta - Iac) / Pr, inverted (inverse_B_matrix.cu:128-141); 0 at q = 0
+        if (!zero) {
+            std::vector<double> B(L * L), Bi;
+            for (int m = 0; m < L; ++m)
+                for (int m1 = 0; m1 < L; ++m1)
+                    B[m * L + m1] = q2 * (q2 * (m == m1 ? 1.0 : 0.0) - T.Iac[m + m1 * L]) / g.pr;
+            lu_invert(L, B, Bi);
+            std::memcpy(bi, Bi.data(), sizeof(double) * L * L);
+        }
+        // (I - dt B^-1 L)^-1 (linear_implicit_operator.cu:60-197)
+        std::vector<double> I(n2 * n2, 0.0), Bi2(n2 * n2, 0.0), Lm(n2 * n2, 0.0), C(n2 * n2), M;
+        for (int m = 0; m < n2; ++m) I[m * n2 + m] = 1.0;
+        if (zero) {
+            for (int m = L; m < n2; ++m) I[m * n2 + m] = 0.0;
+            for (int m = 0; m < L; ++m) Bi2[m * n2 + m] = 2.0;
+        } else {
+            std::vector<double> B2(n2 * n2, 0.0);
+            for (int m = 0; m < L; ++m) {
+                B2[m * n2 + m] = 0.5;
+                for (int m1 = 0; m1 < L; ++m1)
+                    B2[(m + L) * n2 + m1 + L] = q2 * (q2 * (m == m1 ? 1.0 : 0.0) - T.Iac[m + m1 * L]) / g.pr;
+            }
+            lu_invert(n2, B2, Bi2);
+        }
+        for (int m = 0; m < L; ++m)
+            for (int m1 = 0; m1 < L; ++m1) {
+                const double d = m == m1 ? 1.0 : 0.0;
+                const double mp = (m + 1) * kPi;
+                const double l4 = std::pow(T.lambda[m], 4.0);
+                Lm[m * n2 + m1] = -0.5 * (q2 + mp * mp) * d;
+                Lm[m * n2 + m1 + L] = q2 * T.Ia1[m1 + m * L];
+                Lm[(m + L) * n2 + m1] = g.ra * q2 * T.Ia1[m + m1 * L];
+                Lm[(m + L) * n2 + m1 + L] = -q2 * ((l4 + q2 * q2) * d - 2.0 * q2 * T.Iac[m + m1 * L]);
+            }
+        for (int a = 0; a < n2; ++a)
+            for (int b = 0; b < n2; ++b) {
+                double s = 0.0;
+                for (int c2 = 0; c2 < n2; ++c2) s += Bi2[a * n2 + c2] * Lm[c2 * n2 + b];
+                C[a * n2 + b] = I[a * n2 + b] - g.dt * s;
+            }
+        if (zero) {
+            std::vector<double> up(L * L), upi;
+            for (int m = 0; m < L; ++m)
+                for (int m1 = 0; m1 < L; ++m1) up[m * L + m1] = C[m * n2 + m1];
+            lu_invert(L, up, upi);
+            M.assign(n2 * n2, 0.0);
+            for (int m = 0; m < L; ++m)
+                for (int m1 = 0; m1 < L; ++m1) M[m * n2 + m1] = upi[m * L + m1];
+        } else {
+            lu_invert(n2, C, M);
+        }
+        for (int m = 0; m < L; ++m)
+            for (int m1 = 0; m1 < L; ++m1) {
+                im[0 * L * L + m * L + m1] = M[m * n2 + m1];
+                im[1 * L * L + m * L + m1] = M[m * n2 + m1 + L];
+                im[2 * L * L + m * L + m1] = M[(m + L) * n2 + m1];
+                im[3 * L * L + m * L + m1] = M[(m + L) * n2 + m1 + L];
+            }
+    }
+}
+
+// SplitMix64 (Steele, Lea & Flood, OOPSLA 2014) and Box-Muller.
+static inline uint64_t sm64(uint64_t& s)
+{
+    uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+static inline double unit_open(uint64_t& s) { return ((sm64(s) >> 11) + 0.5) * 0x1.0p-53; }
+
+void seeded_theta(const GridInfo& g, uint64_t seed, double amp, double kmax, double* th)
+{
+    const int mox = g.mox, ny = g.ny;
+    std::memset(th, 0, sizeof(double) * 2 * (size_t)mox * ny * g.L);
+    uint64_t s = seed;
+    for (int r = 0; r < ny; ++r) {
+        const int rr = r > ny / 2 ? r - ny : r;
+        for (int c = 0; c < mox; ++c) {
+            if ((double)(c * c + rr * rr) > kmax * kmax) continue;
+            const double u1 = unit_open(s), u2 = unit_open(s);
+            const double rad = std::sqrt(-2.0 * std::log(u1)), ang = 2.0 * kPi * u2;
+            th[2 * ((size_t)r * mox + c)] = amp * rad * std::cos(ang);
+            th[2 * ((size_t)r * mox + c) + 1] = amp * rad * std::sin(ang);
+        }
+    }
+    // Hermitian fix on the kx = 0 column (util.cu:184-209) for every mode
+    for (int k = 0; k < g.L; ++k) {
+        double* a = th + 2 * (size_t)k * mox * ny;
+        for (int r = 0; r < ny; ++r) {
+            double* e = a + 2 * (size_t)r * mox;
+            if (r == 0 || r == ny / 2) e[1] = 0.0;
+            else if (r < ny / 2) {
+                const double* src = a + 2 * (size_t)(ny - r) * mox;
+                e[0] = src[0];
+                e[1] = -src[1];
+            }
+        }
+    }
+}
+
+void seeded_positions(uint64_t seed, int n, double lx, double ly, double* xyz)
+{
+    uint64_t s = seed;
+    for (int i = 0; i < n; ++i) {
+        xyz[i] = lx * unit_open(s);
+        xyz[n + i] = ly * unit_open(s);
+        xyz[2 * n + i] = unit_open(s) - 0.5;
+    }
+}
+
+} // namespace rbchost

@@ -1,0 +1,57 @@
+// galerkin.h -- host-side precomputation for the RBC step (library side).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace rbchost {
+
+// Galerkin integrals over z in (-1/2, 1/2) of Chandrasekhar functions C_m and sines
+// S_m (m 0-based). 2-index tables at i + j*L, 3-index tables at i + j*L + k*L*L, the
+// index order of the reference getters (gpu_flow/code/util/coeff.cu:1151-1222).
+struct Tables {
+    int L = 0;
+    std::vector<double> lambda;                 // lambda_{m+1}
+    std::vector<double> Iac, Ia1;               // as the reference uses them (Iac closed forms)
+    std::vector<double> Ibb1, Ib11, I111, Iabc, Iac1, Iaab, Iaa1, Iab2, Ia12;
+    std::vector<double> CpCp, CC, CS;           // exact int C'_i C'_j, int C_i C_j, int C_i S_j (diagnostics)
+    double t3(const std::vector<double>& t, int i, int j, int k) const { return t[i + j * L + k * L * L]; }
+    double ibbb(int i, int j, int k) const { return -t3(Iabc, i, j, k) - t3(Iabc, i, k, j); }
+};
+
+void build_tables(int L, Tables& T);
+
+// Value of the contraction matrix T'(i,j) of family f at output mode k.
+double family_value(const Tables& T, int family, int i, int j, int k);
+
+// Packed contraction coefficients coef[u][k][o][h] (see contract_prog.h).
+void pack_contraction(const Tables& T, std::vector<double>& coef);
+
+// Partial-pivot LU inverse of a row-major n x n matrix; false if singular.
+bool lu_invert(int n, const std::vector<double>& A, std::vector<double>& inv);
+
+// Per-wavenumber operators, deduplicated by the exact bit pattern of q^2 as the
+// reference computes it on the host (inverse_B_matrix.cu:108-118,
+// linear_implicit_operator.cu:46-59).
+struct OperatorTables {
+    int nclass = 0;
+    std::vector<int> cls;         // [Ny][mox] class of each wavenumber (-1: dealiased)
+    std::vector<double> binv;     // [nclass][L*L]  B_ff^-1 (row-major m*L+m1)
+    std::vector<double> imp;      // [nclass][4][L*L]  (tt, tf, ft, ff) blocks of (I - dt B^-1 L)^-1
+};
+
+struct GridInfo {
+    int nx, ny, L, mox;
+    double lx, ly, ra, pr, dt;
+    int ckeep;                    // columns c < ckeep survive the 2/3 rule
+    std::vector<uint8_t> row_kept;// [Ny]
+};
+
+void grid_info(int nx, int ny, int L, double lx, double ly, double ra, double pr, double dt, GridInfo& g);
+void build_operator_tables(const GridInfo& g, const Tables& T, OperatorTables& op);
+
+// Seeded initial temperature (SplitMix64 + Box-Muller) into theta [L][Ny][mox]
+// (interleaved complex), followed by the Hermitian fix on the kx = 0 column.
+void seeded_theta(const GridInfo& g, uint64_t seed, double amp, double kmax, double* theta);
+void seeded_positions(uint64_t seed, int n, double lx, double ly, double* xyz);
+
+} // namespace rbchost

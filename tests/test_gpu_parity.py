@@ -1,0 +1,218 @@
+"""GPU parity tests: the CUDA library (through its C ABI) against the FP64 oracle on
+the same seeded inputs. FP64 form: bit-level agreement is not expected (summation order
+and FFT algorithm differ), the bar is the north-star tolerance written in each test."""
+import numpy as np
+import pytest
+
+import oracle
+import sdc_b200
+from tests.helpers import hermitian_fix, kept_mask, random_state, rel_err
+
+pytestmark = pytest.mark.gpu
+
+# (nx, ny, L, lx, ly, ra, pr, dt)
+C1 = (64, 64, 4, 8.0, 8.0, 2000.0, 1.0, 1e-3)
+SMALL_CASES = [
+    (32, 32, 2, 8.0, 8.0, 3000.0, 1.0, 1e-3),
+    (48, 32, 3, 12.0, 8.0, 2500.0, 0.7, 1e-3),   # radix 3, non-square, odd L
+    (64, 64, 4, 8.0, 8.0, 2000.0, 1.0, 1e-3),
+    (32, 64, 5, 4.0, 8.0, 4000.0, 7.0, 5e-4),
+    (64, 48, 6, 16.0, 12.0, 4500.0, 1.0, 5e-4),
+    (64, 64, 8, 8.0, 8.0, 5000.0, 0.9, 5e-4),
+]
+
+
+def make_pair(case, threads=8, **kw):
+    nx, ny, L, lx, ly, ra, pr, dt = case
+    s = sdc_b200.Solver(nx, ny, L, lx, ly, ra, pr, dt, **kw)
+    o = oracle.Oracle(nx, ny, L, lx, ly, ra, pr, dt, threads=threads)
+    return s, o
+
+
+@pytest.mark.parametrize("case", SMALL_CASES)
+def test_nonlinear_operator_matches_oracle(case):
+    s, o = make_pair(case)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=11 + L, amp=1.0)
+    o.set_state(*st)
+    ref = o.nonlinear()
+    got = s.nonlinear(*st)
+    for name, a, b in zip(("theta", "f", "g", "F", "G"), got, ref):
+        assert rel_err(a, b) < 1e-12, (name, rel_err(a, b))
+
+
+@pytest.mark.parametrize("case", SMALL_CASES[:3])
+def test_synthesis_matches_oracle(case):
+    s, o = make_pair(case)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=3, amp=1.0)
+    o.set_state(*st)
+    s.set_state(*st)
+    got = s.synthesis()
+    ref = o.synthesis()
+    for fld in range(8):
+        assert rel_err(got[fld], ref[fld]) < 1e-13, fld
+
+
+def test_set_get_state_roundtrip_applies_dealias():
+    s, _ = make_pair(C1)
+    nx, ny, L = C1[:3]
+    rng = np.random.default_rng(0)
+    full = [rng.standard_normal((L, ny, nx // 2 + 1)) + 1j * rng.standard_normal((L, ny, nx // 2 + 1)) for _ in range(3)]
+    F = rng.standard_normal(L) + 0j
+    G = rng.standard_normal(L) + 0j
+    s.set_state(full[0], full[1], full[2], F, G)
+    back = s.get_state()
+    m = kept_mask(nx, ny)
+    for a, b in zip(back[:3], full):
+        assert np.array_equal(a[:, m], b[:, m])
+        assert np.all(a[:, ~m] == 0)
+    assert np.array_equal(back[3], F) and np.array_equal(back[4], G)
+
+
+@pytest.mark.parametrize("nsteps", [1, 10, 100])
+def test_step_matches_oracle_c1(nsteps):
+    # plain FP64 64x64x4, Lx=Ly=8, Ra=2000, Pr=1, dt=1e-3 from the seeded theta (|k| <= 4)
+    s, o = make_pair(C1)
+    s.init_fields(1, 1e-3, 4.0)
+    o.init_theta(1, 1e-3, 4.0)
+    assert all(np.array_equal(a, b) for a, b in zip(s.get_state(), o.get_state()))
+    s.step(nsteps)
+    o.step(nsteps)
+    for name, a, b in zip(("theta", "f", "g", "F", "G"), s.get_state(), o.get_state()):
+        assert rel_err(a, b) < 1e-10, (name, nsteps, rel_err(a, b))
+
+
+@pytest.mark.parametrize("case", SMALL_CASES)
+def test_step_matches_oracle_random_state(case):
+    s, o = make_pair(case)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=5, amp=0.05)
+    s.set_state(*st)
+    o.set_state(*st)
+    s.step(20)
+    o.step(20)
+    for name, a, b in zip(("theta", "f", "g", "F", "G"), s.get_state(), o.get_state()):
+        assert rel_err(a, b) < 1e-10, (name, rel_err(a, b))
+
+
+def test_step_chunking_is_irrelevant():
+    s1, _ = make_pair(C1)
+    s2, _ = make_pair(C1)
+    for s in (s1, s2):
+        s.init_fields(4, 1e-3, 4.0)
+    s1.step(12)
+    for _ in range(4):
+        s2.step(3)
+    for a, b in zip(s1.get_state(), s2.get_state()):
+        assert np.array_equal(a, b)
+
+
+def test_hermitian_and_band_invariants_after_steps():
+    s, _ = make_pair(SMALL_CASES[2])
+    nx, ny, L = SMALL_CASES[2][:3]
+    s.set_state(*random_state(nx, ny, L, seed=9, amp=0.05))
+    s.step(7)
+    th, f, g, F, G = s.get_state()
+    m = kept_mask(nx, ny)
+    for a in (th, f, g):
+        assert np.all(a[:, ~m] == 0)
+        for r in range(1, ny // 2):
+            assert np.array_equal(a[:, r, 0], np.conj(a[:, ny - r, 0]))
+        assert np.all(a[:, 0, 0].imag == 0)
+    assert np.all(F.imag == 0) and np.all(G.imag == 0)
+
+
+def test_diagnostics_match_oracle():
+    case = SMALL_CASES[2]
+    s, o = make_pair(case)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=21, amp=0.05)
+    s.set_state(*st)
+    o.set_state(*st)
+    s.step(5)
+    o.step(5)
+    d = s.diagnostics()
+    r = o.diagnostics()
+    assert d["step"] == 5
+    assert abs(d["nu_wall"] - r["nu_wall"]) < 1e-12 * abs(r["nu_wall"])
+    assert abs(d["nu_vol"] - r["nu_vol"]) < 1e-11 * abs(r["nu_vol"])
+    assert abs(d["ke"] - r["ke"]) < 1e-10 * abs(r["ke"])
+    hist = s.diag_history(10)
+    assert hist.shape == (5, 4) and list(hist[:, 3]) == [1, 2, 3, 4, 5]
+
+
+@pytest.mark.parametrize("z", [0.0, 0.23])
+def test_spectrum_matches_oracle(z):
+    case = SMALL_CASES[4]
+    s, o = make_pair(case)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=31, amp=1.0)
+    s.set_state(*st)
+    o.set_state(*st)
+    nb = nx // 2 + 1
+    a = s.spectrum(nb, z)
+    b = o.spectrum(nb, z)
+    assert rel_err(a, b) < 1e-12
+
+
+def test_tracers_match_oracle():
+    case = (64, 64, 4, 8.0, 8.0, 3000.0, 1.0, 2e-3)
+    n = 4096
+    s, o = make_pair(case, n_tracers=n)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=41, amp=0.3)
+    s.set_state(*st)
+    o.set_state(*st)
+    xyz = oracle.tracer_positions(2, n, case[3], case[4])
+    s.tracers_set(xyz)
+    o.tracers_set(xyz)
+    s.step(10)
+    o.step(10)
+    got = s.tracers_get()
+    ref = o.tracers_get()
+    assert np.abs(got - ref).max() < 1e-9
+    assert np.abs(got - xyz).max() > 1e-4  # they moved
+    for name, a, b in zip(("theta", "f", "g", "F", "G"), s.get_state(), o.get_state()):
+        assert rel_err(a, b) < 1e-10
+
+
+def test_tracer_seed_matches_oracle_generator():
+    case = (32, 32, 2, 32.0, 32.0, 3000.0, 1.0, 1e-3)
+    s, _ = make_pair(case, n_tracers=1000)
+    s.tracers_seed(2)
+    assert np.array_equal(s.tracers_get(), oracle.tracer_positions(2, 1000, 32.0, 32.0))
+
+
+def test_mixed_form_close_to_fp64():
+    case = SMALL_CASES[5]
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=8, amp=0.05)
+    a = sdc_b200.Solver(*case, form="fp64")
+    b = sdc_b200.Solver(*case, form="mixed")
+    a.set_state(*st)
+    b.set_state(*st)
+    a.step(20)
+    b.step(20)
+    for x, y in zip(a.get_state()[:3], b.get_state()[:3]):
+        assert rel_err(y, x) < 1e-4
+    da, db = a.diagnostics(), b.diagnostics()
+    assert abs(da["nu_wall"] - db["nu_wall"]) < 1e-6
+
+
+def test_nan_in_state_reported():
+    s, _ = make_pair(C1)
+    nx, ny, L = C1[:3]
+    st = random_state(nx, ny, L, seed=1, amp=0.01)
+    st[0][0, 3, 2] = np.nan
+    s.set_state(*st)
+    with pytest.raises(sdc_b200.RBCError) as e:
+        s.step(2)
+    assert e.value.status == 3
+
+
+def test_kernel_launch_count():
+    s, _ = make_pair(C1)
+    s.init_fields(1)
+    s.step(3)
+    assert s.kernel_launches == 3 * 6

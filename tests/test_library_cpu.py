@@ -1,0 +1,63 @@
+"""CPU tests of the library's host side: the C-ABI library loads and exports every
+function include/rbc.h declares, its Galerkin tables match the reference's golden
+vectors, and invalid construction parameters are rejected without a GPU call."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import sdc_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def declared_functions():
+    hdr = open(os.path.join(ROOT, "include", "rbc.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(rbc_[a-z_0-9]+)\s*\(", hdr)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = sdc_b200.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(sdc_b200.EXPORTS)
+
+
+@pytest.mark.parametrize("L", [4, 8, 12])
+@pytest.mark.parametrize("name", ["Iac", "Ia1", "Ibbb", "Ibb1", "Ib11", "I111", "Iabc", "Iac1",
+                                  "Iaab", "Iaa1", "Iab2", "Ia12", "lambda"])
+def test_library_tables_match_reference_golden(L, name):
+    ref = np.load(os.path.join(GOLD, f"coeff_L{L}.npz"))[name]
+    got = sdc_b200.galerkin_table(L, name)
+    assert got.shape == ref.shape
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_unknown_table_rejected():
+    with pytest.raises(sdc_b200.RBCError):
+        sdc_b200.galerkin_table(4, "nope")
+
+
+def test_status_strings():
+    lib = sdc_b200.lib()
+    for s in range(8):
+        assert lib.rbc_status_string(s)
+
+
+def test_invalid_params_rejected_before_any_device_work():
+    # nx = 100 is not 2^a 3^b: refused by argument checks (no CUDA call is made)
+    with pytest.raises(sdc_b200.RBCError) as e:
+        sdc_b200.Solver(100, 64, 4, 8.0, 8.0, 2000.0, 1.0, 1e-3)
+    assert e.value.status == 1
+    with pytest.raises(sdc_b200.RBCError) as e:
+        sdc_b200.Solver(64, 64, 4, 8.0, 8.0, 2000.0, -1.0, 1e-3)
+    assert e.value.status == 1
+    with pytest.raises(sdc_b200.RBCError) as e:
+        sdc_b200.Solver(64, 64, 7, 8.0, 8.0, 2000.0, 1.0, 1e-3)
+    assert e.value.status == 6
