@@ -163,7 +163,7 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
@@ -190,7 +190,8 @@ def main():
     import sdc_b200
 
     s = sdc_b200.Solver(**WORK, form=args.form, n_tracers=NTRACERS, device=local)
-    stream = torch.cuda.current_stream()
+    # one dedicated stream for the library and the timing events
+    stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
     s.init_fields(SEED, 1e-3, 8.0)
     s.tracers_seed(SEED)

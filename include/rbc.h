@@ -157,6 +157,9 @@ rbc_status rbc_galerkin_table(int nz, const char* name, double* out, int* count)
  * Replaces the reference's -DTIMER host Timer (gpu_flow/code/util/util.cu:230-281). */
 #define RBC_NSTAGE 7
 rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts);
+/* FP64 FMA throughput of the device in TFLOP/s (roofline denominator of the FP64
+ * contraction; no reference counterpart). */
+rbc_status rbc_measure_fp64_peak(int device, double* tflops);
 /* Device kernel launches issued by the last rbc_step call (for launch accounting). */
 long long rbc_kernel_launches(const rbc_handle* h);
 

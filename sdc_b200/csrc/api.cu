@@ -91,12 +91,22 @@ struct rbc_handle {
     int ntr = 0;
     double* trpos = nullptr;      // [3][ntr]
     double* zbasis = nullptr;     // [128][3][L]
+    void* nv = nullptr;           // [Ny*Nx][NodeRec] node records for the tracers (R)
     bool tracer_pending = false;  // a fluid step ran whose tracer advance is not done yet
     long long launches = 0;
+    int contract_grid = 0, contract_smem = 0;
+    // CUDA graphs of one steady-state (AB2) step: [0] without, [1] with the pending
+    // tracer advance at its start
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaStream_t graph_stream[2] = {nullptr, nullptr};
+    int graph_launches[2] = {0, 0};
+    bool use_graphs = true;
     // stage timing: events recorded around each launch while `profiling`
     bool profiling = false;
     struct Mark { int stage; cudaEvent_t a, b; };
     std::vector<Mark> marks;
+    std::vector<cudaEvent_t> evpool;
+    size_t evnext = 0;
     std::string last_error;
 };
 
@@ -108,6 +118,15 @@ static rbc_status fail(rbc_handle* h, rbc_status s, const std::string& m)
 
 // Stage ids for rbc_stage_times.
 enum { ST_SYNTH = 0, ST_C2R, ST_TRACER, ST_CONTRACT, ST_R2C, ST_COMBINE, ST_UPDATE };
+static cudaEvent_t pool_event(rbc_handle* h)
+{
+    if (h->evnext == h->evpool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->evpool.push_back(e);
+    }
+    return h->evpool[h->evnext++];
+}
 struct StageScope {
     rbc_handle* h;
     int stage;
@@ -115,15 +134,14 @@ struct StageScope {
     StageScope(rbc_handle* h_, int s) : h(h_), stage(s)
     {
         if (h->profiling) {
-            cudaEventCreate(&a);
+            a = pool_event(h);
             cudaEventRecord(a, h->stream);
         }
     }
     ~StageScope()
     {
         if (h->profiling) {
-            cudaEvent_t b;
-            cudaEventCreate(&b);
+            cudaEvent_t b = pool_event(h);
             cudaEventRecord(b, h->stream);
             h->marks.push_back({stage, a, b});
         }
@@ -194,25 +212,26 @@ __global__ void k_spectrum(const double2* __restrict__ th, Geom G, double z, int
 }
 
 // ------------------------------------------------------------------ dispatch
-template <typename R, int L> static void launch_contract(rbc_handle* h)
+template <typename R, int L> static void setup_contract(rbc_handle* h)
 {
     const int smem = (int)(rbcprog::NUNIT * L * L * rbcprog::half_len(L) * sizeof(R));
-    static bool attr = false;
-    if (!attr) {
-        RBC_CUDA(cudaFuncSetAttribute(k_contract<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr = true;
-    }
-    int nsm = 148;
-    int dev = 0;
+    RBC_CUDA(cudaFuncSetAttribute(k_contract<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int dev = 0, nsm = 148, per = 0;
     RBC_CUDA(cudaGetDevice(&dev));
     RBC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int per = 0;
     RBC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_contract<R, L>, 128, smem));
     if (per < 1) per = 1;
     const int need = (h->G.P + 127) / 128;
-    const int grid = need < nsm * per ? need : nsm * per;
+    h->contract_grid = need < nsm * per ? need : nsm * per;
+    h->contract_smem = smem;
+}
+
+template <typename R, int L> static void launch_contract(rbc_handle* h)
+{
     StageScope sc(h, ST_CONTRACT);
-    k_contract<R, L><<<grid, 128, smem, h->stream>>>((const R*)h->phys, (R*)h->grp, (const R*)h->coef, h->G.P);
+    R* nv = h->tracer_pending ? (R*)h->nv : nullptr; // node records for the tracer advance
+    k_contract<R, L><<<h->contract_grid, 128, h->contract_smem, h->stream>>>((const R*)h->phys, (R*)h->grp,
+                                                                             (const R*)h->coef, h->G.P, nv);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -266,16 +285,18 @@ static bool L_supported(int L, bool mixed)
 
 template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
 {
-    return sizeof(typename cplx_t<R>::type) * (size_t)h->G.ny * (1 + (size_t)nfield * h->W);
+    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + (size_t)nfield * h->W * h->py.stride);
 }
 template <typename R> static size_t smem_combine(const rbc_handle* h)
 {
-    return smem_cols<R>(h, 1) + 3 * sizeof(double2) * (size_t)h->W * h->G.ny;
+    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + 13 * (size_t)h->py.stride);
 }
 template <typename R> static size_t smem_rows(const rbc_handle* h)
 {
-    return sizeof(typename cplx_t<R>::type) * (size_t)h->G.nx * (1 + (size_t)h->NP);
+    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.nx + (size_t)h->NP * h->px.stride);
 }
+
+template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h);
 
 // Synthesis: K1 (columns) + K2 (rows) into h->phys from the state in (th, f, g, FG).
 template <typename R>
@@ -301,15 +322,16 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G)
 {
     typedef typename cplx_t<R>::type C;
     RBC_DISPATCH_L(launch_contract, R, G.L, h);
+    if (h->tracer_pending) launch_tracer_from_synthesis<R>(h);
     const int rows = 13 * G.L * G.ny;
     {
     StageScope sc(h, ST_R2C);
     k_rows_r2c<R><<<rows / (2 * h->NP), kThreads, smem_rows<R>(h), h->stream>>>(G, h->NP, h->px, h->twx, (const R*)h->grp, (C*)h->gh);
     RBC_CUDA(cudaGetLastError());
     }
-    dim3 g5(G.ckw / h->W, G.L);
+    dim3 g5(G.ckw, G.L);
     StageScope sc(h, ST_COMBINE);
-    k_columns_combine<R><<<g5, kThreads, smem_combine<R>(h), h->stream>>>(G, h->W, h->py, h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
+    k_columns_combine<R><<<g5, kThreads, smem_combine<R>(h), h->stream>>>(G, h->py, h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
     RBC_CUDA(cudaGetLastError());
     h->launches += 2;
 }
@@ -350,13 +372,15 @@ static void tracer_setup(rbc_handle* h)
     h->zbasis = dalloc<double>(zb.size(), h->owned);
     RBC_CUDA(cudaMemcpy(h->zbasis, zb.data(), zb.size() * sizeof(double), cudaMemcpyHostToDevice));
     h->trpos = dalloc<double>(3 * (size_t)h->ntr, h->owned);
+    const size_t rsz = h->mixed ? sizeof(float) : sizeof(double);
+    h->nv = dalloc<unsigned char>((size_t)h->G.P * ((5 * L + 1) & ~1) * rsz, h->owned);
     RBC_CUDA(cudaMemset(h->trpos, 0, 3 * (size_t)h->ntr * sizeof(double)));
 }
 
 template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
 {
     TracerArgs A;
-    A.phys = h->phys;
+    A.nv = h->nv;
     A.zbasis = h->zbasis;
     A.pos = h->trpos;
     A.n = h->ntr;
@@ -386,9 +410,8 @@ template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h)
 template <typename R> static void run_step(rbc_handle* h)
 {
     run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
-    if (h->tracer_pending) launch_tracer_from_synthesis<R>(h);
+    run_analysis<R>(h, h->G); // the contraction also writes the tracers' node records
     h->tracer_pending = false;
-    run_analysis<R>(h, h->G);
     RBC_DISPATCH_L(launch_update, R, h->G.L, h);
     h->have_hist = true;
     h->tracer_pending = h->ntr > 0;
@@ -399,6 +422,7 @@ template <typename R> static void flush_tracers_t(rbc_handle* h)
 {
     if (!h->tracer_pending) return;
     run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
+    RBC_DISPATCH_L(launch_contract, R, h->G.L, h); // writes the node records
     launch_tracer_from_synthesis<R>(h);
     h->tracer_pending = false;
 }
@@ -438,6 +462,10 @@ const char* rbc_last_error(const rbc_handle* h) { return h ? h->last_error.c_str
 
 static void free_all(rbc_handle* h)
 {
+    for (int v = 0; v < 2; ++v)
+        if (h->graph[v]) cudaGraphExecDestroy(h->graph[v]);
+    for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
+    h->evpool.clear();
     for (void* p : h->owned) cudaFree(p);
     h->owned.clear();
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -482,13 +510,16 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         rbchost::grid_info(p->nx, p->ny, p->nz, p->lx, p->ly, p->ra, p->pr, p->dt, h->gi);
         rbchost::build_tables(p->nz, h->tab);
         const size_t csz = h->mixed ? sizeof(float2) : sizeof(double2);
-        // column block: 8 synthesis columns per (W, Ny) tile within ~200 KB of shared memory
-        int W = 8;
-        while (W > 1 && ((size_t)8 * W * p->ny + p->ny) * csz > 200 * 1024) W /= 2;
-        while (W > 1 && W * p->ny > 8 * kThreads) W /= 2;
+        h->px = rbcfft::make_plan(p->nx);
+        h->py = rbcfft::make_plan(p->ny);
+        // synthesis CTAs take W columns (8 W transforms) to fill one FFT chunk
+        int W = 1;
+        while (W < 4 && 8 * (2 * W) <= h->py.chunk) W *= 2;
         h->W = W;
-        int NP = 8;
-        while (NP > 1 && ((p->ny / 2) % NP != 0)) NP /= 2;
+        // row kernels: NP row pairs per CTA, a divisor of Ny/2 that fits one FFT chunk
+        int NP = 1;
+        for (int c = 1; c <= 32 && c <= h->px.chunk; ++c)
+            if ((p->ny / 2) % c == 0) NP = c;
         h->NP = NP;
         Geom& G = h->G;
         G.nx = p->nx;
@@ -503,8 +534,6 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         G.ly = p->ly;
         G.pr = p->pr;
         G.dt = p->dt;
-        h->px = rbcfft::make_plan(p->nx);
-        h->py = rbcfft::make_plan(p->ny);
         RBC_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
         h->stream = h->own_stream;
         const int L = G.L;
@@ -558,7 +587,14 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         h->gh = dalloc<unsigned char>(13 * plane * L * csz, h->owned);
         h->N = dalloc<unsigned char>(3 * plane * L * csz, h->owned);
         h->NFG = dalloc<double>(2 * L, h->owned);
-        h->upd_blocks = (G.ckeep * G.ny + kThreads - 1) / kThreads;
+        switch (L) {
+        case 2: h->upd_blocks = update_blocks<2>(G.ckeep, G.ny); break;
+        case 3: h->upd_blocks = update_blocks<3>(G.ckeep, G.ny); break;
+        case 4: h->upd_blocks = update_blocks<4>(G.ckeep, G.ny); break;
+        case 5: h->upd_blocks = update_blocks<5>(G.ckeep, G.ny); break;
+        case 6: h->upd_blocks = update_blocks<6>(G.ckeep, G.ny); break;
+        default: h->upd_blocks = update_blocks<8>(G.ckeep, G.ny); break;
+        }
         h->partial = dalloc<double>(2 * (size_t)h->upd_blocks, h->owned);
         h->th00 = dalloc<double>(L, h->owned);
         h->ring = dalloc<double>(4 * (size_t)h->ring_cap, h->owned);
@@ -579,8 +615,13 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         RBC_CUDA(cudaMemset(h->H, 0, 8 * plane * L * csz));
         RBC_CUDA(cudaMemset(h->gh, 0, 13 * plane * L * csz));
         RBC_CUDA(cudaMemset(h->N, 0, 3 * plane * L * csz));
-        if (h->mixed) set_attributes<float>(h);
-        else set_attributes<double>(h);
+        if (h->mixed) {
+            set_attributes<float>(h);
+            RBC_DISPATCH_L(setup_contract, float, G.L, h);
+        } else {
+            set_attributes<double>(h);
+            RBC_DISPATCH_L(setup_contract, double, G.L, h);
+        }
         tracer_setup(h);
         RBC_CUDA(cudaDeviceSynchronize());
     } catch (const CudaError& e) {
@@ -692,14 +733,59 @@ static rbc_status check_err(rbc_handle* h)
     return RBC_OK;
 }
 
+// Captures one steady-state step (history present; tracer advance pending or not) on
+// the current stream into an executable graph.
+static void capture_step(rbc_handle* h, int variant)
+{
+    if (h->graph[variant]) {
+        cudaGraphExecDestroy(h->graph[variant]);
+        h->graph[variant] = nullptr;
+    }
+    const bool hist = h->have_hist, pend = h->tracer_pending;
+    const long long launches = h->launches, hs = h->host_steps;
+    h->have_hist = true;
+    h->tracer_pending = variant == 1;
+    cudaGraph_t g = nullptr;
+    RBC_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->launches = 0;
+    try {
+        if (h->mixed) run_step<float>(h);
+        else run_step<double>(h);
+    } catch (...) {
+        cudaStreamEndCapture(h->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    RBC_CUDA(cudaStreamEndCapture(h->stream, &g));
+    h->graph_launches[variant] = (int)h->launches;
+    cudaError_t e = cudaGraphInstantiate(&h->graph[variant], g, 0);
+    cudaGraphDestroy(g);
+    RBC_CUDA(e);
+    h->graph_stream[variant] = h->stream;
+    h->have_hist = hist;
+    h->tracer_pending = pend;
+    h->launches = launches;
+    h->host_steps = hs;
+}
+
 rbc_status rbc_step_async(rbc_handle* h, int nsteps)
 {
     if (nsteps < 0) return fail(h, RBC_ERR_INVALID_ARG, "negative step count");
     RBC_GUARD(h)
     h->launches = 0;
     for (int s = 0; s < nsteps; ++s) {
-        if (h->mixed) run_step<float>(h);
-        else run_step<double>(h);
+        // graphs need a real stream (the legacy default stream cannot be captured)
+        if (h->use_graphs && h->have_hist && !h->profiling && h->stream != nullptr) {
+            const int v = h->tracer_pending ? 1 : 0;
+            if (!h->graph[v] || h->graph_stream[v] != h->stream) capture_step(h, v);
+            RBC_CUDA(cudaGraphLaunch(h->graph[v], h->stream));
+            h->launches += h->graph_launches[v];
+            h->tracer_pending = h->ntr > 0;
+            ++h->host_steps;
+        } else {
+            if (h->mixed) run_step<float>(h);
+            else run_step<double>(h);
+        }
     }
     return RBC_OK;
     RBC_GUARD_END(h)
@@ -727,6 +813,16 @@ rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts)
     if (!ms || !counts || nsteps <= 0) return fail(h, RBC_ERR_INVALID_ARG, "bad arguments");
     RBC_GUARD(h)
     h->marks.clear();
+    // events for all launches exist before anything is queued
+    h->evnext = 0;
+    for (int i = 0; i < 2 * RBC_NSTAGE * (nsteps + 1); ++i) pool_event(h);
+    h->evnext = 0;
+    // head start: queue unprofiled steps first so that the profiled launches are
+    // enqueued while the GPU is still busy (no host gaps inside the event pairs)
+    for (int s = 0; s < nsteps; ++s) {
+        if (h->mixed) run_step<float>(h);
+        else run_step<double>(h);
+    }
     h->profiling = true;
     for (int s = 0; s < nsteps; ++s) {
         if (h->mixed) run_step<float>(h);
@@ -742,8 +838,6 @@ rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts)
         cudaEventElapsedTime(&t, m.a, m.b);
         tot[m.stage] += t;
         cnt[m.stage] += 1;
-        cudaEventDestroy(m.a);
-        cudaEventDestroy(m.b);
     }
     h->marks.clear();
     for (int i = 0; i < RBC_NSTAGE; ++i) {
@@ -871,14 +965,15 @@ rbc_status rbc_diag_history(rbc_handle* h, rbc_diag* out, int n, int* count)
     RBC_GUARD(h)
     long long steps = 0;
     RBC_CUDA(cudaMemcpyAsync(&steps, h->step_counter, sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
-    std::vector<double> ring(4 * (size_t)h->ring_cap);
-    RBC_CUDA(cudaMemcpyAsync(ring.data(), h->ring, ring.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     RBC_CUDA(cudaStreamSynchronize(h->stream));
     long long avail = steps < h->ring_cap ? steps : h->ring_cap;
     if (avail > n) avail = n;
+    std::vector<double> slot(4);
     for (long long i = 0; i < avail; ++i) {
         const long long s = steps - avail + 1 + i; // 1-based step number
-        const double* slot = &ring[4 * (size_t)((s - 1) % h->ring_cap)];
+        RBC_CUDA(cudaMemcpyAsync(slot.data(), h->ring + 4 * (size_t)((s - 1) % h->ring_cap), 4 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        RBC_CUDA(cudaStreamSynchronize(h->stream));
         out[i].nu_wall = slot[0];
         out[i].nu_vol = slot[1];
         out[i].ke = slot[2];
@@ -986,10 +1081,8 @@ rbc_status rbc_tracers_advance(rbc_handle* h)
     RBC_GUARD(h)
     if (h->ntr == 0) return RBC_OK;
     flush_tracers(h);
-    if (h->mixed) run_synthesis<float>(h, h->th, h->f, h->g, h->FG);
-    else run_synthesis<double>(h, h->th, h->f, h->g, h->FG);
-    if (h->mixed) launch_tracer_from_synthesis<float>(h);
-    else launch_tracer_from_synthesis<double>(h);
+    h->tracer_pending = true; // one more advance with the current field
+    flush_tracers(h);
     RBC_CUDA(cudaStreamSynchronize(h->stream));
     return RBC_OK;
     RBC_GUARD_END(h)

@@ -57,11 +57,16 @@ RBC_D void contract_mode(const R (&in)[rbcprog::NFIELD][L], const R* __restrict_
     for (int gi = 0; gi < rbcprog::NGROUP; ++gi) grp[((size_t)gi * L + k) * P + x] = acc[gi];
 }
 
+// Length of one node record of the tracer velocity array: the 5 L velocity-field values
+// u11, u21, u31, u12, u22 of a grid point, padded to an even count (16-byte records).
+template <int L> struct NodeRec { static constexpr int value = (5 * L + 1) & ~1; };
+
 // Grid-stride over points; coef (global) is the packed array of pack_contraction,
-// copied once per CTA into shared memory.
+// copied once per CTA into shared memory. When nv is not null the kernel also writes
+// every point's node record nv[x * NodeRec] (the tracers gather those records).
 template <typename R, int L>
 __global__ void __launch_bounds__(128) k_contract(const R* __restrict__ phys, R* __restrict__ grp,
-                                                  const R* __restrict__ coef_g, int P)
+                                                  const R* __restrict__ coef_g, int P, R* __restrict__ nv)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* coef = reinterpret_cast<R*>(smem_raw);
@@ -74,6 +79,24 @@ __global__ void __launch_bounds__(128) k_contract(const R* __restrict__ phys, R*
         for (int f = 0; f < rbcprog::NFIELD; ++f)
 #pragma unroll
             for (int i = 0; i < L; ++i) in[f][i] = phys[((size_t)f * L + i) * P + x];
+        if (nv) {
+            constexpr int NR = NodeRec<L>::value;
+            typedef typename cplx_t<R>::type R2;
+            R rec[NR];
+#pragma unroll
+            for (int f = 0; f < 5; ++f)
+#pragma unroll
+                for (int i = 0; i < L; ++i) rec[f * L + i] = in[f][i];
+            if (NR > 5 * L) rec[NR - 1] = 0;
+            R2* dst = reinterpret_cast<R2*>(nv + (size_t)x * NR);
+#pragma unroll
+            for (int q = 0; q < NR / 2; ++q) {
+                R2 v;
+                v.x = rec[2 * q];
+                v.y = rec[2 * q + 1];
+                dst[q] = v;
+            }
+        }
         for (int k = 0; k < L; k += 2) {
             contract_mode<R, L, 0>(in, coef, k, grp, P, x);
             if (k + 1 < L) contract_mode<R, L, 1>(in, coef, k + 1, grp, P, x);

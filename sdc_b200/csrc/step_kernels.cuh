@@ -21,14 +21,11 @@
 namespace rbck {
 
 constexpr double kPi = 3.14159265358979323846;
-constexpr int kThreads = 256;
-constexpr int kMaxB = 4; // butterflies per thread per FFT pass
+constexpr int kThreads = rbcfft::kPlanThreads;
 
 RBC_HD int wrap_row(int r, int ny) { return r > ny / 2 ? r - ny : r; }
 RBC_HD bool row_kept(int r, int ny) { return !(fabs(0.5 * ny - r) <= (1.0 / 3.0) * 0.5 * ny); }
 
-// Transforms of length n processed per FFT call so that nb * n / 2 <= kMaxB * kThreads.
-RBC_HD int fft_chunk(int n) { int c = (kMaxB * kThreads * 2) / n; return c < 1 ? 1 : c; }
 
 template <typename R>
 RBC_D void load_twiddles(typename cplx_t<R>::type* tw, const double2* twg, int n)
@@ -41,10 +38,10 @@ template <typename R>
 RBC_D void fft_batched(typename cplx_t<R>::type* buf, const rbcfft::Plan& p, int nb,
                        const typename cplx_t<R>::type* tw, int sign)
 {
-    const int ch = fft_chunk(p.n);
+    const int ch = p.chunk;
     for (int b0 = 0; b0 < nb; b0 += ch) {
         const int cnt = nb - b0 < ch ? nb - b0 : ch;
-        rbcfft::run<kMaxB, R>(buf + b0 * p.n, p, cnt, tw, sign);
+        rbcfft::run<R>(buf + b0 * p.stride, p, cnt, tw, sign);
     }
 }
 
@@ -85,6 +82,7 @@ __global__ void __launch_bounds__(kThreads) k_synth_columns(
     C* buf = tw + G.ny;
     const int k = blockIdx.y;
     const int c0 = blockIdx.x * W;
+    const int st = py.stride;
     load_twiddles<R>(tw, twy, G.ny);
     const size_t base = ((size_t)k * G.ckp + c0) * G.ny;
     for (int e = threadIdx.x; e < W * G.ny; e += blockDim.x) {
@@ -106,14 +104,15 @@ __global__ void __launch_bounds__(kThreads) k_synth_columns(
                                  vf * (-m.lap), u12, u22, vt,
                                  cmul_is<double2, double>(vt, m.fx), cmul_is<double2, double>(vt, m.fy)};
 #pragma unroll
-        for (int fld = 0; fld < 8; ++fld) buf[(fld * W + cc) * G.ny + r] = cmk<C>(vals[fld].x, vals[fld].y);
+        for (int fld = 0; fld < 8; ++fld) buf[(fld * W + cc) * st + rbcfft::pad(r)] = cmk<C>(vals[fld].x, vals[fld].y);
     }
     __syncthreads();
     fft_batched<R>(buf, py, 8 * W, tw, +1);
     for (int e = threadIdx.x; e < 8 * W * G.ny; e += blockDim.x) {
         const int fld = e / (W * G.ny);
         const int rem = e - fld * W * G.ny;
-        H[(((size_t)fld * G.L + k) * G.ckp + c0) * G.ny + rem] = buf[fld * W * G.ny + rem];
+        const int cc = rem / G.ny, r = rem - cc * G.ny;
+        H[(((size_t)fld * G.L + k) * G.ckp + c0) * G.ny + rem] = buf[(fld * W + cc) * st + rbcfft::pad(r)];
     }
 }
 
@@ -132,12 +131,12 @@ __global__ void __launch_bounds__(kThreads) k_rows_c2r(
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + G.nx;
     load_twiddles<R>(tw, twx, G.nx);
-    const int nx = G.nx;
+    const int nx = G.nx, st = px.stride;
     const int row0 = 2 * NP * blockIdx.x;           // first row (plane * Ny + y)
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     for (int e = threadIdx.x; e < NP * nx; e += blockDim.x) {
         const int pp = e / nx, n = e - pp * nx;
-        if (n >= G.ckeep && n <= nx - G.ckeep) buf[pp * nx + n] = cmk<C>(0, 0);
+        if (n >= G.ckeep && n <= nx - G.ckeep) buf[pp * st + rbcfft::pad(n)] = cmk<C>(0, 0);
     }
     const C* src = H + (size_t)plane * G.ckp * G.ny + y0;
     for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
@@ -145,10 +144,10 @@ __global__ void __launch_bounds__(kThreads) k_rows_c2r(
         C A = src[(size_t)n * G.ny + 2 * pp], B = src[(size_t)n * G.ny + 2 * pp + 1];
         if (n == 0) { A.y = 0; B.y = 0; }
         C z; z.x = A.x - B.y; z.y = A.y + B.x;       // A + iB
-        buf[pp * nx + n] = z;
+        buf[pp * st + rbcfft::pad(n)] = z;
         if (n > 0) {
             C zm; zm.x = A.x + B.y; zm.y = B.x - A.y; // conj(A) + i conj(B)
-            buf[pp * nx + nx - n] = zm;
+            buf[pp * st + rbcfft::pad(nx - n)] = zm;
         }
     }
     __syncthreads();
@@ -156,7 +155,7 @@ __global__ void __launch_bounds__(kThreads) k_rows_c2r(
     R* dst = phys + (size_t)row0 * nx;
     for (int e = threadIdx.x; e < NP * nx; e += blockDim.x) {
         const int pp = e / nx, x = e - pp * nx;
-        const C z = buf[pp * nx + x];
+        const C z = buf[pp * st + rbcfft::pad(x)];
         dst[(size_t)(2 * pp) * nx + x] = z.x;
         dst[(size_t)(2 * pp + 1) * nx + x] = z.y;
     }
@@ -176,13 +175,13 @@ __global__ void __launch_bounds__(kThreads) k_rows_r2c(
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + G.nx;
     load_twiddles<R>(tw, twx, G.nx);
-    const int nx = G.nx;
+    const int nx = G.nx, st = px.stride;
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     const R* src = grp + (size_t)row0 * nx;
     for (int e = threadIdx.x; e < NP * nx; e += blockDim.x) {
         const int pp = e / nx, x = e - pp * nx;
-        buf[pp * nx + x] = cmk<C>(src[(size_t)(2 * pp) * nx + x], src[(size_t)(2 * pp + 1) * nx + x]);
+        buf[pp * st + rbcfft::pad(x)] = cmk<C>(src[(size_t)(2 * pp) * nx + x], src[(size_t)(2 * pp + 1) * nx + x]);
     }
     __syncthreads();
     fft_batched<R>(buf, px, NP, tw, -1);
@@ -192,8 +191,8 @@ __global__ void __launch_bounds__(kThreads) k_rows_r2c(
         const int n = e / NP, pp = e - n * NP;
         C A = cmk<C>(0, 0), B = A;
         if (n < G.ckeep) {
-            const C z = buf[pp * nx + n];
-            const C zm = buf[pp * nx + (n == 0 ? 0 : nx - n)];
+            const C z = buf[pp * st + rbcfft::pad(n)];
+            const C zm = buf[pp * st + rbcfft::pad(n == 0 ? 0 : nx - n)];
             A.x = half * (z.x + zm.x);
             A.y = half * (z.y - zm.y);
             B.x = half * (z.y + zm.y);
@@ -205,15 +204,15 @@ __global__ void __launch_bounds__(kThreads) k_rows_r2c(
 }
 
 // ---------------------------------------------------------------------------------
-// K5: forward y transform of the 13 group planes of one mode k and W columns, the
+// K5: forward y transform of the 13 group columns of one (column c, mode k), the
 // derivative multiplier of each group, and the reference's final scaling
 // (nonlinear_operator_rayleigh_noslip.cu:1366-1370) with the 1/P of its products:
 //   N_theta = -(1/P) sum,  N_f = N_g = -(1/(Pr P)) sum.
 // F_k and G_k (reference :950-1003) are the q = 0 entries of the g-y group and of
-// the negated g-x group, scaled like f.
+// the negated g-x group, scaled like f. Grid (ckw, L).
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_columns_combine(
-    Geom G, int W, rbcfft::Plan py, const double2* __restrict__ twy,
+    Geom G, rbcfft::Plan py, const double2* __restrict__ twy,
     const typename cplx_t<R>::type* __restrict__ gh, typename cplx_t<R>::type* __restrict__ N,
     double* __restrict__ NFG)
 {
@@ -221,56 +220,43 @@ __global__ void __launch_bounds__(kThreads) k_columns_combine(
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + G.ny;
-    const int k = blockIdx.y;
-    const int c0 = blockIdx.x * W;
-    load_twiddles<R>(tw, twy, G.ny);
-    const int nel = W * G.ny;
-    // accumulators of theta, f, g for this tile (each element owned by one thread)
-    double2* acc = reinterpret_cast<double2*>(buf + nel);
-    for (int e = threadIdx.x; e < 3 * nel; e += blockDim.x) acc[e] = make_double2(0, 0);
-    const double invP = 1.0 / ((double)G.nx * G.ny);
-    for (int grpi = 0; grpi < 13; ++grpi) {
-        const C* src = gh + (((size_t)grpi * G.L + k) * G.ckp + c0) * G.ny;
-        __syncthreads();
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) buf[e] = src[e];
-        __syncthreads();
-        fft_batched<R>(buf, py, W, tw, -1);
-        double2* at = acc + (grpi < 8 ? 1 : (grpi < 12 ? 2 : 0)) * nel;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            const int cc = e / G.ny, r = e - cc * G.ny, c = c0 + cc;
-            const C zv = buf[e];
-            const double2 v = make_double2(zv.x, zv.y);
-            if (c == 0 && r == 0) {
-                if (grpi == 10) NFG[k] = v.x * (-invP / G.pr);           // F
-                if (grpi == 11) NFG[G.L + k] = -v.x * (-invP / G.pr);    // G
-            }
-            const Mult m(c, r, G);
-            double2 o;
-            switch (grpi) {
-            case 0: o = v * (-(m.fx * m.fx)); break;                          // f: xx
-            case 1: o = v * m.xy; break;                                      // f: xy
-            case 2: o = v * (-(m.fy * m.fy)); break;                          // f: yy
-            case 3: o = cmul_is<double2, double>(v, m.fx); break;             // f: x
-            case 4: o = cmul_is<double2, double>(v, m.fy); break;             // f: y
-            case 5: o = cmul_is<double2, double>(v, m.fx) * m.lap; break;     // f: lap o x
-            case 6: o = cmul_is<double2, double>(v, m.fy) * m.lap; break;     // f: lap o y
-            case 7: o = v * m.lap; break;                                     // f: lap
-            case 8: o = v * m.xy; break;                                      // g: xy
-            case 9: o = v * ((m.fx * m.fx) - (m.fy * m.fy)); break;           // g: yy - xx
-            case 10: o = cmul_is<double2, double>(v, m.fy); break;            // g: y
-            case 11: o = cmul_is<double2, double>(v, m.fx); break;            // g: x
-            default: o = v; break;                                            // theta
-            }
-            at[e] = at[e] + o;
-        }
+    const int c = blockIdx.x, k = blockIdx.y, ny = G.ny;
+    load_twiddles<R>(tw, twy, ny);
+    const size_t cstride = (size_t)G.L * G.ckp * ny; // between groups
+    const C* src = gh + ((size_t)k * G.ckp + c) * ny;
+    for (int e = threadIdx.x; e < 13 * ny; e += blockDim.x) {
+        const int grpi = e / ny, r = e - grpi * ny;
+        buf[grpi * py.stride + rbcfft::pad(r)] = src[grpi * cstride + r];
     }
-    const double sc[3] = {-invP, -invP / G.pr, -invP / G.pr};
-    for (int a = 0; a < 3; ++a) {
-        C* dst = N + (((size_t)a * G.L + k) * G.ckp + c0) * G.ny;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            const double2 v = acc[a * nel + e] * sc[a];
-            dst[e] = cmk<C>(v.x, v.y);
+    __syncthreads();
+    fft_batched<R>(buf, py, 13, tw, -1);
+    const double invP = 1.0 / ((double)G.nx * ny);
+    for (int r = threadIdx.x; r < ny; r += blockDim.x) {
+        double2 v[13];
+#pragma unroll
+        for (int gi = 0; gi < 13; ++gi) {
+            const C z = buf[gi * py.stride + rbcfft::pad(r)];
+            v[gi] = make_double2(z.x, z.y);
         }
+        if (c == 0 && r == 0) {
+            NFG[k] = v[10].x * (-invP / G.pr);          // F: mean of the g-y group
+            NFG[G.L + k] = -v[11].x * (-invP / G.pr);   // G: minus mean of the g-x group
+        }
+        const Mult m(c, r, G);
+        const double xx = -(m.fx * m.fx), yy = -(m.fy * m.fy);
+        double2 af = v[0] * xx + v[1] * m.xy + v[2] * yy + cmul_is<double2, double>(v[3], m.fx) +
+                     cmul_is<double2, double>(v[4], m.fy) + cmul_is<double2, double>(v[5], m.fx) * m.lap +
+                     cmul_is<double2, double>(v[6], m.fy) * m.lap + v[7] * m.lap;
+        double2 ag = v[8] * m.xy + v[9] * (yy - xx) + cmul_is<double2, double>(v[10], m.fy) +
+                     cmul_is<double2, double>(v[11], m.fx);
+        const double2 at = v[12] * (-invP);
+        af = af * (-invP / G.pr);
+        ag = ag * (-invP / G.pr);
+        const size_t o = ((size_t)k * G.ckp + c) * ny + r;
+        const size_t pl = (size_t)G.L * G.ckp * ny;
+        N[o] = cmk<C>(at.x, at.y);
+        N[pl + o] = cmk<C>(af.x, af.y);
+        N[2 * pl + o] = cmk<C>(ag.x, ag.y);
     }
 }
 

@@ -6,8 +6,9 @@
 // with RK4 on that frozen field with trilinear interpolation (vel_interpolate :508-607,
 // PERIODIC wrap), then reflects z at +-zmax (periodic_boundaries :722-764).
 // Here the grid is never materialised: the velocity at a grid node (x, y, z_l) is
-// evaluated when needed from the 5 L synthesised planes u11, u21, u31, u12, u22 of the
-// fluid step, with the same sums as compose_u_from_derivs:
+// evaluated when needed from the 5 L synthesised values u11, u21, u31, u12, u22 of that
+// node (one contiguous record per node, written by the contraction kernel that reads
+// them anyway), with the same sums as compose_u_from_derivs:
 //   u = sum_i C'_i(z_l) u11_i + S_i(z_l) u12_i,  v = sum_i C'_i u21_i + S_i u22_i,
 //   w = sum_i C_i(z_l) u31_i.
 #pragma once
@@ -18,25 +19,32 @@ namespace rbck {
 constexpr int kZNum = 128;
 
 struct TracerArgs {
-    const void* phys;     // [8][L][Ny][Nx] (R): fields 0..4 are u11, u21, u31, u12, u22
+    const void* nv;       // [Ny*Nx][NodeRec] (R): u11, u21, u31, u12, u22 per grid point
     const double* zbasis; // [128][3][L]: C_i(z_l), S_i(z_l), C'_i(z_l)
     double* pos;          // [3][n] x, y, z
     int n, nx, ny, L;
     double lx, ly, dt, zmax;
 };
 
+// Velocity (u, v, w) at the grid node xy on the levels z0 and z1 from the node record.
 template <typename R, int L>
-RBC_D void node_velocity(const R* __restrict__ ph, size_t P, size_t xy, const double* zb0, const double* zb1,
+RBC_D void node_velocity(const R* __restrict__ nv, size_t xy, const double* zb0, const double* zb1,
                          double (&u0)[3], double (&u1)[3])
 {
+    constexpr int NR = (5 * L + 1) & ~1;
+    typedef typename cplx_t<R>::type R2;
+    R rec[NR];
+    const R2* src = reinterpret_cast<const R2*>(nv + xy * NR);
+#pragma unroll
+    for (int q = 0; q < NR / 2; ++q) {
+        const R2 v = __ldg(src + q);
+        rec[2 * q] = v.x;
+        rec[2 * q + 1] = v.y;
+    }
     double a0 = 0, b0 = 0, c0 = 0, a1 = 0, b1 = 0, c1 = 0;
 #pragma unroll
     for (int i = 0; i < L; ++i) {
-        const double v11 = ph[((size_t)0 * L + i) * P + xy];
-        const double v21 = ph[((size_t)1 * L + i) * P + xy];
-        const double v31 = ph[((size_t)2 * L + i) * P + xy];
-        const double v12 = ph[((size_t)3 * L + i) * P + xy];
-        const double v22 = ph[((size_t)4 * L + i) * P + xy];
+        const double v11 = rec[i], v21 = rec[L + i], v31 = rec[2 * L + i], v12 = rec[3 * L + i], v22 = rec[4 * L + i];
         const double C0 = zb0[i], S0 = zb0[L + i], D0 = zb0[2 * L + i];
         const double C1 = zb1[i], S1 = zb1[L + i], D1 = zb1[2 * L + i];
         a0 += D0 * v11 + S0 * v12;
@@ -53,9 +61,8 @@ RBC_D void node_velocity(const R* __restrict__ ph, size_t P, size_t xy, const do
 template <typename R, int L>
 RBC_D void vel_interp(const TracerArgs& A, const double* zb, double x, double y, double z, double& rx, double& ry, double& rz)
 {
-    const R* ph = reinterpret_cast<const R*>(A.phys);
+    const R* nv = reinterpret_cast<const R*>(A.nv);
     const int xs = A.nx, ys = A.ny;
-    const size_t P = (size_t)xs * ys;
     double xg = x * xs / A.lx;
     double yg = y * ys / A.ly;
     double zg = (A.zmax + z) / (2 * A.zmax) * (kZNum - 1);
@@ -73,10 +80,10 @@ RBC_D void vel_interp(const TracerArgs& A, const double* zb, double x, double y,
     const double* zb0 = zb + (size_t)iz0 * 3 * L;
     const double* zb1 = zb + (size_t)iz1 * 3 * L;
     double v00[2][3], v10[2][3], v01[2][3], v11[2][3]; // [z level][component], corners (x, y)
-    node_velocity<R, L>(ph, P, (size_t)iy0 * xs + ix0, zb0, zb1, v00[0], v00[1]);
-    node_velocity<R, L>(ph, P, (size_t)iy0 * xs + ix1, zb0, zb1, v10[0], v10[1]);
-    node_velocity<R, L>(ph, P, (size_t)iy1 * xs + ix0, zb0, zb1, v01[0], v01[1]);
-    node_velocity<R, L>(ph, P, (size_t)iy1 * xs + ix1, zb0, zb1, v11[0], v11[1]);
+    node_velocity<R, L>(nv, (size_t)iy0 * xs + ix0, zb0, zb1, v00[0], v00[1]);
+    node_velocity<R, L>(nv, (size_t)iy0 * xs + ix1, zb0, zb1, v10[0], v10[1]);
+    node_velocity<R, L>(nv, (size_t)iy1 * xs + ix0, zb0, zb1, v01[0], v01[1]);
+    node_velocity<R, L>(nv, (size_t)iy1 * xs + ix1, zb0, zb1, v11[0], v11[1]);
     double wR = xg - (double)ix0, wL = 1 - wR;
     double cz0y0[3], cz0y1[3], cz1y0[3], cz1y1[3];
 #pragma unroll
