@@ -160,6 +160,32 @@ rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts);
 /* FP64 FMA throughput of the device in TFLOP/s (roofline denominator of the FP64
  * contraction; no reference counterpart). */
 rbc_status rbc_measure_fp64_peak(int device, double* tflops);
+/* --- nonlinear operator without device allocation ----------------------------- */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc (code that
+ * runs inside another framework's memory pool, or that must not change the device's
+ * allocation state, e.g. while it is captured or checkpointed): the same operator as
+ * rbc_nonlinear, without a handle, on DEVICE buffers in the reference layout (inputs
+ * theta, f, g [nz][ny][nx/2+1] and F, G [nz] complex; the five outputs alike). It calls
+ * no cudaMalloc, cudaFree or allocating library routine: all scratch lives in one
+ * file-scope __device__ array of RBC_NOALLOC_SCRATCH_BYTES, which every GPU that loads
+ * this library holds until the process exits. Limits: nx, ny <= 64 (2^a 3^b, even),
+ * 2 <= nz <= 4; larger sizes return RBC_ERR_INVALID_ARG with the reason in errbuf (may be
+ * NULL). The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call before any
+ * stream capture. Every call shares the array and leaves its contents behind (each call
+ * rewrites all it reads): calls that overlap on the GPU -- on different streams, or from
+ * several host threads -- race and must be serialised by the caller. Work is enqueued on
+ * `stream` (cudaStream_t, NULL = legacy default stream) and not waited for. */
+#define RBC_NOALLOC_MAX_NX 64
+#define RBC_NOALLOC_MAX_NY 64
+#define RBC_NOALLOC_MAX_NZ 4
+#define RBC_NOALLOC_SCRATCH_BYTES (8u << 20)
+rbc_status rbc_nonlinear_noalloc(int device, int nx, int ny, int nz, double lx, double ly, double pr,
+                                 const double* theta, const double* f, const double* g,
+                                 const double* F, const double* G,
+                                 double* out_theta, double* out_f, double* out_g,
+                                 double* out_F, double* out_G, void* stream, char* errbuf, int errlen);
+
 /* Device kernel launches issued by the last rbc_step call (for launch accounting). */
 long long rbc_kernel_launches(const rbc_handle* h);
 

@@ -47,7 +47,7 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_init_fields", "rbc_set_state", "rbc_get_state", "rbc_step", "rbc_step_async",
            "rbc_synchronize", "rbc_nonlinear", "rbc_tracers_set", "rbc_tracers_get", "rbc_tracers_seed",
            "rbc_tracers_advance", "rbc_diagnostics", "rbc_diag_history", "rbc_spectrum", "rbc_synthesis",
-           "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_measure_fp64_peak", "rbc_kernel_launches"]
+           "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_measure_fp64_peak", "rbc_nonlinear_noalloc", "rbc_kernel_launches"]
 
 
 def lib():
@@ -86,6 +86,8 @@ def lib():
     L.rbc_galerkin_table.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp, ctypes.POINTER(ctypes.c_int)]
     L.rbc_stage_times.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]
     L.rbc_measure_fp64_peak.argtypes = [ctypes.c_int, _dp]
+    L.rbc_nonlinear_noalloc.argtypes = ([ctypes.c_int] * 4 + [ctypes.c_double] * 3 + [ctypes.c_void_p] * 10 +
+                                        [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int])
     L.rbc_kernel_launches.argtypes = [vp]
     L.rbc_kernel_launches.restype = ctypes.c_longlong
     _LIB = L
