@@ -55,6 +55,28 @@ def stage_bytes(nx, ny, L, ckeep, nkept, ntr):
     }
 
 
+def dist_env():
+    """(world, rank, local_rank) from the torchrun environment (1, 0, 0 without it)."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(value, world, device=None):
+    """The largest of every rank's `value` (all ranks get it); identity for one rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_scaling_value(world, steps, dt, ms_max):
+    """Whole-job sim time per second: every replica advances `steps` steps of dt."""
+    return world * steps * dt / (ms_max / 1000.0)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -91,6 +113,14 @@ class ClockSampler:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # the timed region starts once the sampler has produced its first line
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.out) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -163,7 +193,7 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
@@ -171,9 +201,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank)
         return
@@ -215,11 +243,8 @@ def main():
     barrier()
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * WORK["dt"] / (ms_max / 1000.0)
+    ms_max = max_over_ranks(ms, world, device="cuda")
+    value = weak_scaling_value(world, args.steps, WORK["dt"], ms_max)
 
     # ---- per-kernel timing (roofline of the dominant kernel)
     stages = s.stage_times(max(5, min(50, args.steps // 10)))
@@ -252,11 +277,7 @@ def main():
         s.diagnostics()
     out_state = s.get_state()
     out_tr = s.tracers_get()
-    el = time.perf_counter() - t0
-    te = torch.tensor([el], device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    el = float(te.item())
+    el = max_over_ranks(time.perf_counter() - t0, world, device="cuda")
     state_bytes = sum(a.nbytes for a in host_state)
     tr_bytes = host_tr.nbytes
     e2e = {"value": world * args.steps * WORK["dt"] / el, "unit": "sim-time/s",

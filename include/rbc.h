@@ -58,9 +58,11 @@ typedef struct {
     int n_tracers;   /* passive tracers (0: none) */
     int device;      /* CUDA device ordinal */
     int diag_capacity; /* per-step diagnostics ring entries (0: 4096) */
+    int tune;        /* 1: time the launch tilings of the FFT kernels at creation and keep
+                        the fastest (project autotuner); 0: built-in heuristic */
 } rbc_params;
 
-/* Diagnostics of the state after a step (no reference counterpart; see DESIGN). */
+/* Diagnostics of the state after a step (no reference counterpart). */
 typedef struct {
     double nu_wall;  /* 1 - d<theta>_xy/dz at z = -1/2 */
     double nu_vol;   /* 1 + <w theta>_V */
@@ -97,6 +99,30 @@ rbc_status rbc_init_fields(rbc_handle* h, unsigned long long seed, double amplit
 rbc_status rbc_set_state(rbc_handle* h, const double* theta, const double* f, const double* g,
                          const double* F, const double* G);
 rbc_status rbc_get_state(rbc_handle* h, double* theta, double* f, double* g, double* F, double* G);
+
+/* --- files in the reference's dump format ------------------------------------- */
+/* One matrix of a dump file (matrix_folder_writer::read_binary_file,
+ * gpu_flow/code/output/matrix_folder_writer.cu:3-58): FP32 (the reference's default
+ * build) or FP64 complex, told apart by the file size; values are returned as FP64
+ * interleaved complex. dims receives the matrix dimensions (x fastest), *ndims their
+ * count; out may be NULL to query the dimensions only. Host only, no GPU needed. */
+rbc_status rbc_dump_read(const char* path, int index, int* dims, int maxdims, int* ndims,
+                         double* out, long long maxvals);
+/* Writes one matrix (write_binary_file, matrix_folder_writer.cu:61-101) with 4- or
+ * 8-byte reals. Host only. */
+rbc_status rbc_dump_write(const char* path, const int* dims, int ndims, const double* data, int real_bytes);
+/* The state as the five files theta_%08d.bin, f_, g_, F_, G_ in directory dir, as
+ * main.cu:697-713 names them (real_bytes 4 = the reference's FP32 files, 8 = FP64). */
+rbc_status rbc_save_state(rbc_handle* h, const char* dir, long long step, int real_bytes);
+/* Reads the five files of a reference run (main.cu:355-385, with the same dimension
+ * checks) into the state; like rbc_set_state the next step is an Euler step. */
+rbc_status rbc_load_state(rbc_handle* h, const char* theta, const char* f, const char* g,
+                          const char* F, const char* G);
+/* AB2 history (B^-1 N of the previous step) as one FP64 file of five matrices. The
+ * reference never saves it, so its restarts take an Euler step
+ * (implicit_explicit_stepping.cu:43-52); with this file a restart continues exactly. */
+rbc_status rbc_save_history(rbc_handle* h, const char* path);
+rbc_status rbc_load_history(rbc_handle* h, const char* path);
 
 /* --- step ---------------------------------------------------------------------- */
 /* nsteps iterations of the reference loop body (main.cu:612-637): step_time
@@ -138,6 +164,24 @@ rbc_status rbc_diag_history(rbc_handle* h, rbc_diag* out, int n, int* count);
  * in nbins shells of width |q_max| / nbins, as energy_spectrum_2d::reduce_spectrum
  * (gpu_flow/code/postProcessing/energy_spectrum_2d.cu:85-129). */
 rbc_status rbc_spectrum(rbc_handle* h, double z, double* bins, int nbins);
+
+/* --- ensembles ------------------------------------------------------------------ */
+/* Batched form (no reference counterpart): n independent runs with their own grids,
+ * mode counts, Ra, Pr and dt, advanced together. Every ensemble step is one CUDA graph
+ * in which each member's step is a branch on one of `nstreams` worker streams (members
+ * are spread over the streams by estimated cost, longest first), so the members' kernels
+ * run concurrently. Members are ordinary handles (initialise them with
+ * rbc_ensemble_member + rbc_init_fields / rbc_set_state). */
+typedef struct rbc_ensemble rbc_ensemble;
+rbc_status rbc_ensemble_create(const rbc_params* members, int n, int nstreams, rbc_ensemble** out);
+void rbc_ensemble_destroy(rbc_ensemble* e);
+rbc_handle* rbc_ensemble_member(rbc_ensemble* e, int i);
+/* nsteps steps of every member; waits for completion (RBC_ERR_NAN if any member blew up). */
+rbc_status rbc_ensemble_step(rbc_ensemble* e, int nsteps);
+/* Text of the last error of rbc_ensemble_step ("" when none). */
+const char* rbc_ensemble_last_error(const rbc_ensemble* e);
+/* Column-block width W and row pairs per CTA NP chosen for a handle (after tuning). */
+rbc_status rbc_launch_config(const rbc_handle* h, int* W, int* NP);
 
 /* --- inspection (tests, tools) ------------------------------------------------- */
 /* Physical fields of the current state: 8 blocks [L][Ny][Nx] in the order

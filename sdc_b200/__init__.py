@@ -10,7 +10,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libsdc_b200.so")
+LIB_PATH = os.environ.get("SDC_B200_LIB") or os.path.join(_HERE, "_lib", "libsdc_b200.so")
 _LIB = None
 
 RBC_OK = 0
@@ -29,7 +29,8 @@ class _Params(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("ra", ctypes.c_double),
                 ("pr", ctypes.c_double), ("dt", ctypes.c_double), ("form", ctypes.c_int),
-                ("n_tracers", ctypes.c_int), ("device", ctypes.c_int), ("diag_capacity", ctypes.c_int)]
+                ("n_tracers", ctypes.c_int), ("device", ctypes.c_int), ("diag_capacity", ctypes.c_int),
+                ("tune", ctypes.c_int)]
 
 
 class _Diag(ctypes.Structure):
@@ -47,7 +48,10 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_init_fields", "rbc_set_state", "rbc_get_state", "rbc_step", "rbc_step_async",
            "rbc_synchronize", "rbc_nonlinear", "rbc_tracers_set", "rbc_tracers_get", "rbc_tracers_seed",
            "rbc_tracers_advance", "rbc_diagnostics", "rbc_diag_history", "rbc_spectrum", "rbc_synthesis",
-           "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_measure_fp64_peak", "rbc_nonlinear_noalloc", "rbc_kernel_launches"]
+           "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_measure_fp64_peak", "rbc_nonlinear_noalloc", "rbc_dump_read", "rbc_dump_write",
+           "rbc_save_state", "rbc_load_state", "rbc_save_history", "rbc_load_history", "rbc_ensemble_create",
+           "rbc_ensemble_destroy", "rbc_ensemble_member", "rbc_ensemble_step", "rbc_ensemble_last_error", "rbc_launch_config",
+           "rbc_kernel_launches"]
 
 
 def lib():
@@ -88,6 +92,23 @@ def lib():
     L.rbc_measure_fp64_peak.argtypes = [ctypes.c_int, _dp]
     L.rbc_nonlinear_noalloc.argtypes = ([ctypes.c_int] * 4 + [ctypes.c_double] * 3 + [ctypes.c_void_p] * 10 +
                                         [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int])
+    cp = ctypes.c_char_p
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.rbc_dump_read.argtypes = [cp, ctypes.c_int, ip, ctypes.c_int, ip, _dp, ctypes.c_longlong]
+    L.rbc_dump_write.argtypes = [cp, ip, ctypes.c_int, _dp, ctypes.c_int]
+    L.rbc_save_state.argtypes = [vp, cp, ctypes.c_longlong, ctypes.c_int]
+    L.rbc_load_state.argtypes = [vp, cp, cp, cp, cp, cp]
+    L.rbc_save_history.argtypes = [vp, cp]
+    L.rbc_load_history.argtypes = [vp, cp]
+    L.rbc_ensemble_create.argtypes = [ctypes.POINTER(_Params), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.rbc_ensemble_destroy.argtypes = [vp]
+    L.rbc_ensemble_destroy.restype = None
+    L.rbc_ensemble_member.argtypes = [vp, ctypes.c_int]
+    L.rbc_ensemble_member.restype = vp
+    L.rbc_ensemble_step.argtypes = [vp, ctypes.c_int]
+    L.rbc_ensemble_last_error.argtypes = [vp]
+    L.rbc_ensemble_last_error.restype = ctypes.c_char_p
+    L.rbc_launch_config.argtypes = [vp, ip, ip]
     L.rbc_kernel_launches.argtypes = [vp]
     L.rbc_kernel_launches.restype = ctypes.c_longlong
     _LIB = L
@@ -113,6 +134,64 @@ def fp64_peak_tflops(device=0):
     return v.value
 
 
+def dump_read(path, index=0):
+    """One matrix of a reference dump file as a complex array shaped [dims reversed]."""
+    dims = (ctypes.c_int * 8)()
+    nd = ctypes.c_int(0)
+    st = lib().rbc_dump_read(os.fsencode(path), index, dims, 8, ctypes.byref(nd), None, 0)
+    if st != RBC_OK:
+        raise RBCError(st, f"rbc_dump_read({path})")
+    d = [dims[i] for i in range(nd.value)]
+    n = int(np.prod(d))
+    out = np.zeros(2 * n)
+    st = lib().rbc_dump_read(os.fsencode(path), index, dims, 8, ctypes.byref(nd), out.ctypes.data_as(_dp), n)
+    if st != RBC_OK:
+        raise RBCError(st, f"rbc_dump_read({path})")
+    return out.view(np.complex128).reshape(d[::-1])
+
+
+def dump_write(path, arr, real_bytes=8):
+    """Writes a complex array (shape [dims reversed]) as a one-matrix dump file."""
+    a = np.ascontiguousarray(arr, dtype=np.complex128)
+    d = (ctypes.c_int * a.ndim)(*a.shape[::-1])
+    st = lib().rbc_dump_write(os.fsencode(path), d, a.ndim, a.view(np.float64).ctypes.data_as(_dp), real_bytes)
+    if st != RBC_OK:
+        raise RBCError(st, f"rbc_dump_write({path})")
+
+
+def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False):
+    return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)))
+
+
+class Ensemble:
+    """n independent runs advanced together, one CUDA graph per step (rbc_ensemble_*)."""
+
+    def __init__(self, configs, nstreams=16, device=0, tune=False):
+        arr = (_Params * len(configs))(*[make_params(*c[:8], form=c[8] if len(c) > 8 else "fp64", device=device,
+                                                     tune=tune) for c in configs])
+        e = ctypes.c_void_p()
+        st = lib().rbc_ensemble_create(arr, len(configs), nstreams, ctypes.byref(e))
+        if st != RBC_OK:
+            raise RBCError(st, "rbc_ensemble_create failed")
+        self.e = e
+        self.members = [Solver(*c[:8], _handle=ctypes.c_void_p(lib().rbc_ensemble_member(e, i)))
+                        for i, c in enumerate(configs)]
+
+    def step(self, n=1):
+        st = lib().rbc_ensemble_step(self.e, n)
+        if st != RBC_OK:
+            raise RBCError(st, "rbc_ensemble_step: " + lib().rbc_ensemble_last_error(self.e).decode())
+
+    def close(self):
+        if getattr(self, "e", None):
+            for m in self.members:
+                m.h = None
+            lib().rbc_ensemble_destroy(self.e)
+            self.e = None
+
+    __del__ = close
+
+
 def _p(a):
     assert a.flags["C_CONTIGUOUS"] and a.dtype in (np.float64, np.complex128)
     return a.ctypes.data_as(_dp)
@@ -121,12 +200,17 @@ def _p(a):
 class Solver:
     """One RBC run on one GPU (mirrors the reference's operator set, see include/rbc.h)."""
 
-    def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0):
+    def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0,
+                 tune=False, _handle=None):
         self.nx, self.ny, self.L = nx, ny, nz
         self.mox = nx // 2 + 1
         self.n_tracers = n_tracers
         self.params = dict(nx=nx, ny=ny, nz=nz, lx=lx, ly=ly, ra=ra, pr=pr, dt=dt, form=form)
-        p = _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity)
+        self._owned = _handle is None
+        if _handle is not None:
+            self.h = _handle
+            return
+        p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune)
         h = ctypes.c_void_p()
         st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
         if st != RBC_OK:
@@ -134,9 +218,15 @@ class Solver:
         self.h = h
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self, "_owned", True):
             lib().rbc_destroy(self.h)
-            self.h = None
+        self.h = None
+
+    @property
+    def launch_config(self):
+        W, NP = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().rbc_launch_config(self.h, ctypes.byref(W), ctypes.byref(NP)))
+        return W.value, NP.value
 
     __del__ = close
 
@@ -160,6 +250,19 @@ class Solver:
         b = self._bufs()
         self._check(lib().rbc_get_state(self.h, *[_p(x) for x in b]))
         return b
+
+    # files (reference dump format)
+    def save_state(self, directory, step, real_bytes=8):
+        self._check(lib().rbc_save_state(self.h, os.fsencode(directory), step, real_bytes))
+
+    def load_state(self, theta, f, g, F, G):
+        self._check(lib().rbc_load_state(self.h, *[os.fsencode(p) for p in (theta, f, g, F, G)]))
+
+    def save_history(self, path):
+        self._check(lib().rbc_save_history(self.h, os.fsencode(path)))
+
+    def load_history(self, path):
+        self._check(lib().rbc_load_history(self.h, os.fsencode(path)))
 
     # step
     def step(self, n=1):

@@ -13,6 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OBJ_DIR = os.path.join(HERE, "_lib", "obj")
 LIB = os.path.join(OUT_DIR, "libsdc_b200.so")
+DRIVER = os.path.join(OUT_DIR, "rbc_run")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -22,7 +23,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
 CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-I" + INCLUDE, "-I" + CSRC, "-I/usr/local/cuda/include"]
 
 CU_SOURCES = ["api.cu", "peak_fp64.cu", "nonlinear_static.cu"]
-CPP_SOURCES = ["galerkin.cpp"]
+CPP_SOURCES = ["galerkin.cpp", "dump_io.cpp"]
 
 
 def _deps():
@@ -68,6 +69,11 @@ def build(force=False, verbose=False, extra_nvflags=()):
             list(ex.map(lambda c: _run(c, verbose), jobs))
     if jobs or force or not os.path.exists(LIB):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], verbose)
+    drv_src = os.path.join(CSRC, "rbc_run.cpp")
+    if force or not os.path.exists(DRIVER) or os.path.getmtime(DRIVER) < max(os.path.getmtime(drv_src),
+                                                                              os.path.getmtime(LIB)):
+        _run(["g++", "-O2", "-std=c++17", "-I" + INCLUDE, drv_src, "-o", DRIVER, "-L" + OUT_DIR, "-lsdc_b200",
+              "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 

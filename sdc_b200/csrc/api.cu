@@ -1,6 +1,6 @@
 // api.cu -- C ABI (include/rbc.h) of the B200-native RBC step: handle, device buffers,
 // launch sequence, layout conversion, spectrum. Kernels live in the *.cuh headers.
-#include "../../include/rbc.h"
+#include "rbc.h"
 #include "common.cuh"
 #include "contract_kernel.cuh"
 #include "fft.cuh"
@@ -9,6 +9,7 @@
 #include "tracer_kernel.cuh"
 #include "update_kernel.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -274,13 +275,14 @@ template <typename R, int L> static void launch_update(rbc_handle* h)
     case 5: FN<R, 5>(h); break;                                                           \
     case 6: FN<R, 6>(h); break;                                                           \
     case 8: FN<R, 8>(h); break;                                                           \
+    case 12: FN<R, 12>(h); break;                                                         \
     default: throw ArgError{"unsupported number of vertical modes"};                      \
     }
 
 static bool L_supported(int L, bool mixed)
 {
     (void)mixed;
-    return L == 2 || L == 3 || L == 4 || L == 5 || L == 6 || L == 8;
+    return L == 2 || L == 3 || L == 4 || L == 5 || L == 6 || L == 8 || L == 12;
 }
 
 template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
@@ -392,7 +394,7 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.dt = h->G.dt;
     A.zmax = 0.5f - 1e-3;
     StageScope sc(h, ST_TRACER);
-    k_tracers<R, L><<<(h->ntr + 127) / 128, 128, 0, h->stream>>>(A);
+    k_tracers<R, L><<<(4 * h->ntr + 127) / 128, 128, 0, h->stream>>>(A); // 4 lanes per tracer
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -432,12 +434,69 @@ static void flush_tracers(rbc_handle* h)
     else flush_tracers_t<double>(h);
 }
 
+// The dynamic shared-memory limit is an attribute of the kernel, shared by every handle
+// in the process; it is set to the device's opt-in maximum (a cap only: occupancy follows
+// the size each launch asks for), so handles of different shapes can run side by side.
 template <typename R> static void set_attributes(rbc_handle* h)
 {
-    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols<R>(h, 8)));
-    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_combine<R>(h)));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows<R>(h)));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows<R>(h)));
+    int dev = 0, optin = 0;
+    RBC_CUDA(cudaGetDevice(&dev));
+    RBC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t need = std::max({smem_cols<R>(h, 8), smem_combine<R>(h), smem_rows<R>(h)});
+    if (need > (size_t)optin) throw ArgError{"grid too large for the FFT kernels' shared memory"};
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+}
+
+// ------------------------------------------------------------------ autotuner
+// Times the four FFT kernels (synthesis columns and rows, analysis rows and columns)
+// for every admissible column block W in {1, 2, 4} and row-pair count NP (divisors of
+// Ny/2 up to the FFT chunk) on the handle's own scratch, and keeps the fastest pair.
+static void autotune(rbc_handle* h)
+{
+    Geom& G = h->G;
+    const bool mixed = h->mixed;
+    const size_t csz = mixed ? sizeof(float2) : sizeof(double2);
+    int best_W = h->W, best_NP = h->NP;
+    float best = 1e30f;
+    cudaEvent_t a, b;
+    RBC_CUDA(cudaEventCreate(&a));
+    RBC_CUDA(cudaEventCreate(&b));
+    for (int W = 1; W <= 4; W *= 2) {
+        if (8 * W > h->py.chunk && W > 1) continue;
+        if (csz * ((size_t)G.ny + 8 * (size_t)W * h->py.stride) > 200 * 1024) continue;
+        for (int NP = 1; NP <= 32 && NP <= h->px.chunk; ++NP) {
+            if ((G.ny / 2) % NP) continue;
+            if (csz * ((size_t)G.nx + (size_t)NP * h->px.stride) > 200 * 1024) continue;
+            h->W = W;
+            h->NP = NP;
+            G.ckw = ((G.ckeep + W - 1) / W) * W;
+            if (mixed) set_attributes<float>(h);
+            else set_attributes<double>(h);
+            float t = 0;
+            for (int rep = 0; rep < 4; ++rep) {
+                RBC_CUDA(cudaEventRecord(a, h->stream));
+                if (mixed) { run_synthesis<float>(h, h->th, h->f, h->g, h->FG); run_analysis<float>(h, G); }
+                else { run_synthesis<double>(h, h->th, h->f, h->g, h->FG); run_analysis<double>(h, G); }
+                RBC_CUDA(cudaEventRecord(b, h->stream));
+                RBC_CUDA(cudaEventSynchronize(b));
+                float ms = 0;
+                RBC_CUDA(cudaEventElapsedTime(&ms, a, b));
+                if (rep > 0) t += ms; // first repetition warms up
+            }
+            if (t < best) { best = t; best_W = W; best_NP = NP; }
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->W = best_W;
+    h->NP = best_NP;
+    G.ckw = ((G.ckeep + best_W - 1) / best_W) * best_W;
+    if (mixed) set_attributes<float>(h);
+    else set_attributes<double>(h);
+    h->launches = 0;
 }
 
 // ------------------------------------------------------------------ C ABI
@@ -528,7 +587,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         G.L = p->nz;
         G.ckeep = h->gi.ckeep;
         G.ckw = ((G.ckeep + W - 1) / W) * W;
-        G.ckp = ((G.mox + W - 1) / W) * W;
+        G.ckp = ((G.mox + 3) / 4) * 4; // stride padded for any column block W <= 4
         G.P = p->nx * p->ny;
         G.lx = p->lx;
         G.ly = p->ly;
@@ -593,7 +652,8 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         case 4: h->upd_blocks = update_blocks<4>(G.ckeep, G.ny); break;
         case 5: h->upd_blocks = update_blocks<5>(G.ckeep, G.ny); break;
         case 6: h->upd_blocks = update_blocks<6>(G.ckeep, G.ny); break;
-        default: h->upd_blocks = update_blocks<8>(G.ckeep, G.ny); break;
+        case 8: h->upd_blocks = update_blocks<8>(G.ckeep, G.ny); break;
+        default: h->upd_blocks = update_blocks<12>(G.ckeep, G.ny); break;
         }
         h->partial = dalloc<double>(2 * (size_t)h->upd_blocks, h->owned);
         h->th00 = dalloc<double>(L, h->owned);
@@ -624,6 +684,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         }
         tracer_setup(h);
         RBC_CUDA(cudaDeviceSynchronize());
+        if (p->tune) autotune(h);
     } catch (const CudaError& e) {
         std::string m = std::string("rbc_create: ") + e.what + ": " + cudaGetErrorString(e.e);
         std::fprintf(stderr, "%s\n", m.c_str());
@@ -845,6 +906,114 @@ rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts)
         counts[i] = cnt[i] / nsteps;
     }
     return check_err(h);
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_save_state(rbc_handle* h, const char* dir, long long step, int real_bytes)
+{
+    if (!h || !dir || (real_bytes != 4 && real_bytes != 8)) return fail(h, RBC_ERR_INVALID_ARG, "bad arguments");
+    const Geom& G = h->G;
+    const int L = G.L;
+    const size_t n = (size_t)L * G.ny * G.mox;
+    std::vector<double> th(2 * n), f(2 * n), g(2 * n), F(2 * L), Gm(2 * L);
+    rbc_status s = rbc_get_state(h, th.data(), f.data(), g.data(), F.data(), Gm.data());
+    if (s != RBC_OK) return s;
+    const int d3[3] = {G.mox, G.ny, L}, d1[3] = {1, 1, L};
+    const char* names[5] = {"theta", "f", "g", "F", "G"};
+    const double* data[5] = {th.data(), f.data(), g.data(), F.data(), Gm.data()};
+    for (int i = 0; i < 5; ++i) {
+        char path[4096];
+        std::snprintf(path, sizeof path, "%s/%s_%08lld.bin", dir, names[i], step);
+        s = rbc_dump_write(path, i < 3 ? d3 : d1, 3, data[i], real_bytes);
+        if (s != RBC_OK) return fail(h, s, std::string("cannot write ") + path);
+    }
+    return RBC_OK;
+}
+
+rbc_status rbc_load_state(rbc_handle* h, const char* tp, const char* fp, const char* gp, const char* Fp, const char* Gp)
+{
+    if (!h || !tp || !fp || !gp || !Fp || !Gp) return fail(h, RBC_ERR_INVALID_ARG, "null path");
+    const Geom& G = h->G;
+    const int L = G.L;
+    const size_t n = (size_t)L * G.ny * G.mox;
+    std::vector<double> buf[5];
+    const char* paths[5] = {tp, fp, gp, Fp, Gp};
+    for (int i = 0; i < 5; ++i) {
+        int dims[8], nd = 0;
+        const size_t want = i < 3 ? n : (size_t)L;
+        buf[i].assign(2 * want, 0.0);
+        rbc_status s = rbc_dump_read(paths[i], 0, dims, 8, &nd, nullptr, 0);
+        if (s != RBC_OK) return fail(h, s, std::string("cannot read ") + paths[i]);
+        // matrix_has_size (gpu_flow/code/util/util.cu:32-43)
+        const bool ok = nd == 3 && (i < 3 ? (dims[0] == G.mox && dims[1] == G.ny && dims[2] == L)
+                                          : (dims[0] == 1 && dims[1] == 1 && dims[2] == L));
+        if (!ok) return fail(h, RBC_ERR_INVALID_ARG, std::string("wrong dimensions in ") + paths[i]);
+        s = rbc_dump_read(paths[i], 0, dims, 8, &nd, buf[i].data(), (long long)want);
+        if (s != RBC_OK) return fail(h, s, std::string("cannot read ") + paths[i]);
+    }
+    return rbc_set_state(h, buf[0].data(), buf[1].data(), buf[2].data(), buf[3].data(), buf[4].data());
+}
+
+rbc_status rbc_save_history(rbc_handle* h, const char* path)
+{
+    if (!path) return fail(h, RBC_ERR_INVALID_ARG, "null path");
+    RBC_GUARD(h)
+    if (!h->have_hist) return fail(h, RBC_ERR_INVALID_ARG, "no AB2 history yet (no step since the state was set)");
+    const Geom& G = h->G;
+    const int L = G.L;
+    const size_t n = (size_t)L * G.ny * G.mox, plane = (size_t)G.ckp * G.ny;
+    std::vector<double> hv[3];
+    for (int a = 0; a < 3; ++a) {
+        hv[a].resize(2 * n);
+        download_field(h, h->hist + a * plane * L, hv[a].data(), L);
+    }
+    std::vector<double2> fg(2 * L);
+    RBC_CUDA(cudaMemcpyAsync(fg.data(), h->hFG, 2 * L * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    FILE* fpo = std::fopen(path, "wb");
+    if (!fpo) return fail(h, RBC_ERR_IO, std::string("cannot write ") + path);
+    bool ok = true;
+    const int nmat = 5, nd = 3;
+    ok &= std::fwrite(&nmat, 4, 1, fpo) == 1;
+    for (int a = 0; a < 5; ++a) {
+        const int d3[3] = {G.mox, G.ny, L}, d1[3] = {1, 1, L};
+        ok &= std::fwrite(&nd, 4, 1, fpo) == 1;
+        ok &= std::fwrite(a < 3 ? d3 : d1, 4, 3, fpo) == 3;
+        if (a < 3) ok &= std::fwrite(hv[a].data(), 8, hv[a].size(), fpo) == hv[a].size();
+        else ok &= std::fwrite(fg.data() + (a - 3) * L, 16, L, fpo) == (size_t)L;
+    }
+    ok &= std::fclose(fpo) == 0;
+    return ok ? RBC_OK : fail(h, RBC_ERR_IO, std::string("cannot write ") + path);
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_load_history(rbc_handle* h, const char* path)
+{
+    if (!path) return fail(h, RBC_ERR_INVALID_ARG, "null path");
+    RBC_GUARD(h)
+    const Geom& G = h->G;
+    const int L = G.L;
+    const size_t n = (size_t)L * G.ny * G.mox, plane = (size_t)G.ckp * G.ny;
+    std::vector<double> hv[5];
+    for (int a = 0; a < 5; ++a) {
+        int dims[8], nd = 0;
+        const size_t want = a < 3 ? n : (size_t)L;
+        hv[a].assign(2 * want, 0.0);
+        rbc_status s = rbc_dump_read(path, a, dims, 8, &nd, hv[a].data(), (long long)want);
+        if (s != RBC_OK) return fail(h, s, std::string("cannot read history ") + path);
+        const bool ok = nd == 3 && (a < 3 ? (dims[0] == G.mox && dims[1] == G.ny && dims[2] == L)
+                                          : (dims[0] == 1 && dims[1] == 1 && dims[2] == L));
+        if (!ok) return fail(h, RBC_ERR_INVALID_ARG, std::string("wrong dimensions in ") + path);
+    }
+    flush_tracers(h);
+    for (int a = 0; a < 3; ++a) upload_field(h, hv[a].data(), h->hist + a * plane * L, L);
+    std::vector<double2> fg(2 * L);
+    std::memcpy(fg.data(), hv[3].data(), L * sizeof(double2));
+    std::memcpy(fg.data() + L, hv[4].data(), L * sizeof(double2));
+    RBC_CUDA(cudaMemcpyAsync(h->hFG, fg.data(), 2 * L * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    h->have_hist = true;
+    return RBC_OK;
     RBC_GUARD_END(h)
 }
 
@@ -1086,6 +1255,180 @@ rbc_status rbc_tracers_advance(rbc_handle* h)
     RBC_CUDA(cudaStreamSynchronize(h->stream));
     return RBC_OK;
     RBC_GUARD_END(h)
+}
+
+rbc_status rbc_launch_config(const rbc_handle* h, int* W, int* NP)
+{
+    if (!h || !W || !NP) return RBC_ERR_INVALID_ARG;
+    *W = h->W;
+    *NP = h->NP;
+    return RBC_OK;
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------------ ensembles
+struct rbc_ensemble {
+    std::vector<rbc_handle*> members;
+    std::vector<int> stream_of;             // worker stream of each member
+    std::vector<cudaStream_t> streams;      // worker streams
+    cudaStream_t root = nullptr;
+    std::vector<cudaEvent_t> ev;            // fork + one join event per worker
+    cudaGraphExec_t graph = nullptr;
+    int device = 0;
+    std::string last_error;
+};
+
+static double member_cost(const rbc_params& p)
+{
+    // algorithmic bytes of one plain step (S = (Nx/2+1) Ny, P = Nx Ny)
+    const double S = (p.nx / 2 + 1.0) * p.ny, P = (double)p.nx * p.ny, L = p.nz;
+    return L * (12 * S * 16 + 44 * P * 8) + 40 * L * L * S;
+}
+
+extern "C" {
+
+rbc_status rbc_ensemble_create(const rbc_params* members, int n, int nstreams, rbc_ensemble** out)
+{
+    if (!members || n <= 0 || !out) return RBC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (nstreams <= 0) nstreams = 16;
+    if (nstreams > n) nstreams = n;
+    for (int i = 0; i < n; ++i)
+        if (members[i].device != members[0].device) return RBC_ERR_INVALID_ARG;
+    rbc_ensemble* e = new rbc_ensemble;
+    e->device = members[0].device;
+    for (int i = 0; i < n; ++i) {
+        rbc_handle* h = nullptr;
+        rbc_status s = rbc_create(&members[i], &h);
+        if (s != RBC_OK) {
+            rbc_ensemble_destroy(e);
+            return s;
+        }
+        e->members.push_back(h);
+    }
+    // longest-processing-time-first assignment of members to worker streams
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return member_cost(members[a]) > member_cost(members[b]); });
+    std::vector<double> load(nstreams, 0.0);
+    e->stream_of.assign(n, 0);
+    for (int i : order) {
+        const int s = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        e->stream_of[i] = s;
+        load[s] += member_cost(members[i]);
+    }
+    cudaSetDevice(e->device);
+    e->streams.resize(nstreams);
+    bool ok = cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking) == cudaSuccess;
+    for (int s = 0; s < nstreams && ok; ++s) ok = cudaStreamCreateWithFlags(&e->streams[s], cudaStreamNonBlocking) == cudaSuccess;
+    e->ev.resize(nstreams + 1);
+    for (auto& x : e->ev) ok = ok && cudaEventCreateWithFlags(&x, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        rbc_ensemble_destroy(e);
+        return RBC_ERR_CUDA;
+    }
+    *out = e;
+    return RBC_OK;
+}
+
+void rbc_ensemble_destroy(rbc_ensemble* e)
+{
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    for (auto* h : e->members) rbc_destroy(h);
+    for (auto s : e->streams) if (s) cudaStreamDestroy(s);
+    if (e->root) cudaStreamDestroy(e->root);
+    for (auto x : e->ev) if (x) cudaEventDestroy(x);
+    delete e;
+}
+
+const char* rbc_ensemble_last_error(const rbc_ensemble* e)
+{
+    return e ? e->last_error.c_str() : "null ensemble";
+}
+
+rbc_handle* rbc_ensemble_member(rbc_ensemble* e, int i)
+{
+    if (!e || i < 0 || i >= (int)e->members.size()) return nullptr;
+    return e->members[i];
+}
+
+rbc_status rbc_ensemble_step(rbc_ensemble* e, int nsteps)
+{
+    if (!e || nsteps < 0) return RBC_ERR_INVALID_ARG;
+    if (cudaSetDevice(e->device) != cudaSuccess) return RBC_ERR_CUDA;
+    e->last_error.clear();
+    try {
+        const int n = (int)e->members.size();
+        int s = 0;
+        // work a member queued on another stream completes before its worker stream takes over
+        for (int i = 0; i < n; ++i) {
+            rbc_handle* h = e->members[i];
+            if (h->stream != e->streams[e->stream_of[i]]) {
+                if (h->stream) RBC_CUDA(cudaStreamSynchronize(h->stream));
+                h->stream = e->streams[e->stream_of[i]];
+            }
+        }
+        // members still waiting for their first (Euler) step, or with tracers, step eagerly
+        bool graphable = true;
+        for (auto* h : e->members) graphable = graphable && h->have_hist && h->ntr == 0;
+        for (; s < nsteps && !graphable; ++s) {
+            for (int i = 0; i < n; ++i) {
+                rbc_handle* h = e->members[i];
+                h->stream = e->streams[e->stream_of[i]];
+                if (h->mixed) run_step<float>(h);
+                else run_step<double>(h);
+            }
+            graphable = true;
+            for (auto* h : e->members) graphable = graphable && h->have_hist && h->ntr == 0;
+        }
+        if (s < nsteps && !e->graph) {
+            // one graph: fork from root to the worker streams, every member's step on its
+            // stream, join back to root
+            cudaGraph_t g = nullptr;
+            RBC_CUDA(cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal));
+            RBC_CUDA(cudaEventRecord(e->ev[0], e->root));
+            for (auto st : e->streams) RBC_CUDA(cudaStreamWaitEvent(st, e->ev[0], 0));
+            for (int i = 0; i < n; ++i) {
+                rbc_handle* h = e->members[i];
+                h->stream = e->streams[e->stream_of[i]];
+                const long long hs = h->host_steps;
+                if (h->mixed) run_step<float>(h);
+                else run_step<double>(h);
+                h->host_steps = hs;
+            }
+            for (size_t w = 0; w < e->streams.size(); ++w) {
+                RBC_CUDA(cudaEventRecord(e->ev[w + 1], e->streams[w]));
+                RBC_CUDA(cudaStreamWaitEvent(e->root, e->ev[w + 1], 0));
+            }
+            RBC_CUDA(cudaStreamEndCapture(e->root, &g));
+            cudaError_t ce = cudaGraphInstantiate(&e->graph, g, 0);
+            cudaGraphDestroy(g);
+            RBC_CUDA(ce);
+        }
+        for (; s < nsteps; ++s) {
+            RBC_CUDA(cudaGraphLaunch(e->graph, e->root));
+            for (auto* h : e->members) ++h->host_steps;
+        }
+        RBC_CUDA(cudaStreamSynchronize(e->root));
+        for (auto st : e->streams) RBC_CUDA(cudaStreamSynchronize(st));
+        for (auto* h : e->members) {
+            rbc_status st = check_err(h);
+            if (st != RBC_OK) {
+                e->last_error = rbc_last_error(h);
+                return st;
+            }
+        }
+    } catch (const CudaError& x) {
+        e->last_error = std::string(x.what) + ": " + cudaGetErrorString(x.e);
+        return RBC_ERR_CUDA;
+    } catch (const ArgError& x) {
+        e->last_error = x.msg;
+        return RBC_ERR_UNSUPPORTED;
+    }
+    return RBC_OK;
 }
 
 } // extern "C"

@@ -35,10 +35,14 @@ RBC_D void contract_units(const R (&in)[rbcprog::NFIELD][L], R (&acc)[rbcprog::N
         }
 #pragma unroll
         for (int ed = 0; ed < u.nedge; ++ed) {
-            R d = 0;
+            // two interleaved partial sums halve the FMA dependency chain
+            R d0 = 0, d1 = 0;
 #pragma unroll
-            for (int o = 0; o < L; ++o) d = fma(w[o], in[u.e[ed].other][o], d);
-            acc[u.e[ed].group] = fma((R)u.e[ed].weight, d, acc[u.e[ed].group]);
+            for (int o = 0; o < L; o += 2) {
+                d0 = fma(w[o], in[u.e[ed].other][o], d0);
+                if (o + 1 < L) d1 = fma(w[o + 1], in[u.e[ed].other][o + 1], d1);
+            }
+            acc[u.e[ed].group] = fma((R)u.e[ed].weight, d0 + d1, acc[u.e[ed].group]);
         }
         contract_units<R, L, KP, U + 1>(in, acc, cbase);
     }

@@ -1,8 +1,8 @@
 // fft.cuh -- batched complex FFTs staged in shared memory (sm_100a, FP64 or FP32).
 //
-// Lengths N = 2^a 3^b (8 <= N <= 1024) run as Stockham autosort passes whose first
-// radix is 16 (or 8) and whose later radices are 16, 8, 4, 2 or 3, e.g. 256 = 16 x 16,
-// 512 = 16 x 16 x 2, 192 = 16 x 4 x 3. Each thread does one radix-R butterfly per pass
+// Lengths N = 2^a 3^b (8 <= N <= 1024) run as Stockham autosort passes with radices
+// 16, 8 and one leftover 4 or 2, then 3s, largest first: e.g. 256 = 16 x 16,
+// 512 = 8 x 8 x 8, 192 = 8 x 8 x 3. Each thread does one radix-R butterfly per pass
 // in registers (the 8- and 16-point DFTs are split into radix-2/4 steps with constant
 // twiddles). All threads of the CTA cooperate on `nb` transforms held in ONE shared
 // buffer: a pass reads its inputs to registers, synchronises, then writes the outputs
@@ -30,6 +30,9 @@ constexpr int kPlanThreads = 256;
 RBC_HD int pad(int i) { return i + (i >> 4); }
 RBC_HD int padded_len(int n) { return n + (n >> 4) + 1; }
 
+// Factorisation with few passes and large radices: 16s, then 8s, and a single leftover
+// radix (4, 2, 3, 6 -> 3 x 2, 12 -> 4 x 3 ...). Prefers 8 x 8 x 8 over 16 x 16 x 2 so
+// that the smallest radix, which limits how many transforms a CTA can batch, stays big.
 inline Plan make_plan(int n)
 {
     Plan p;
@@ -37,24 +40,35 @@ inline Plan make_plan(int n)
     p.stride = padded_len(n);
     p.npass = 0;
     int m = n;
-    if (m % 16 == 0) { p.radix[p.npass++] = 16; m /= 16; }
-    else if (m % 8 == 0) { p.radix[p.npass++] = 8; m /= 8; }
-    while (m % 16 == 0) { p.radix[p.npass++] = 16; m /= 16; }
-    while (m % 8 == 0) { p.radix[p.npass++] = 8; m /= 8; }
-    while (m % 4 == 0) { p.radix[p.npass++] = 4; m /= 4; }
-    while (m % 2 == 0) { p.radix[p.npass++] = 2; m /= 2; }
-    while (m % 3 == 0) { p.radix[p.npass++] = 3; m /= 3; }
-    if (m != 1 || n < 8) p.npass = -1; // unsupported length
-    // every pass must fit the CTA: radix >= 4 one butterfly per thread, radix 2 and 3
-    // up to two (MAXB in run()); the smallest such "butterfly width" sets the chunk
-    int eff = 1 << 30;
-    for (int s = 0; s < p.npass; ++s) {
-        const int r = p.radix[s];
-        const int e = r >= 4 ? r : 2 * r;
-        eff = e < eff ? e : eff;
+    int twos = 0, threes = 0;
+    while (m % 2 == 0) { m /= 2; ++twos; }
+    while (m % 3 == 0) { m /= 3; ++threes; }
+    if (m != 1 || n < 8) { p.npass = -1; p.chunk = 0; return p; }
+    // powers of two as 16s and 8s (4 or 2 only when twos < 3)
+    int n16 = 0, n8 = 0, rest2 = 0;
+    if (twos >= 3) {
+        switch (twos % 4) {
+        case 0: n16 = twos / 4; break;
+        case 1: n16 = (twos - 9) / 4; n8 = 3; if (twos < 9) { n16 = 0; n8 = 1; rest2 = twos - 3; } break; // 2^5 = 8 x 4
+        case 2: n16 = (twos - 6) / 4; n8 = 2; if (twos < 6) { n16 = 0; n8 = 1; rest2 = twos - 3; } break;
+        case 3: n16 = (twos - 3) / 4; n8 = 1; break;
+        }
+    } else {
+        rest2 = twos;
     }
-    p.chunk = p.npass > 0 ? (kPlanThreads * eff) / n : 0;
-    if (p.npass > 0 && p.chunk < 1) p.npass = -1;
+    for (int i = 0; i < n16; ++i) p.radix[p.npass++] = 16;
+    for (int i = 0; i < n8; ++i) p.radix[p.npass++] = 8;
+    if (rest2 == 2) p.radix[p.npass++] = 4;
+    else if (rest2 == 1) p.radix[p.npass++] = 2;
+    for (int i = 0; i < threes; ++i) p.radix[p.npass++] = 3;
+    // put the largest radix first (stride-R writes of the first pass are padded)
+    for (int a = 0; a < p.npass; ++a)
+        for (int b = a + 1; b < p.npass; ++b)
+            if (p.radix[b] > p.radix[a]) { int t = p.radix[a]; p.radix[a] = p.radix[b]; p.radix[b] = t; }
+    int rmin = 1 << 30;
+    for (int s2 = 0; s2 < p.npass; ++s2) rmin = p.radix[s2] < rmin ? p.radix[s2] : rmin;
+    p.chunk = (kPlanThreads * rmin) / n;
+    if (p.chunk < 1) p.npass = -1;
     return p;
 }
 
@@ -119,41 +133,42 @@ RBC_D void dft_small(typename cplx_t<R>::type* v, int sign)
         v[2] = e2 + o2; v[6] = e2 - o2;
         v[3] = e3 + o3; v[7] = e3 - o3;
     } else if constexpr (RAD == 16) {
-        // n = 4 m + q: four 4-point DFTs over m, twiddles W16^(q k1), then 4-point DFTs over q
-        C y[4][4];
+        // n = 4 m + q: 4-point DFTs over m in place (v[q], v[q+4], v[q+8], v[q+12] then
+        // hold Y_q[k1 = 0..3]), twiddles W16^(q k1), 4-point DFTs over q for each k1;
+        // X[k1 + 4 k2] ends up in v[4 k2 + k1] after the final register transpose.
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            y[q][0] = v[q]; y[q][1] = v[q + 4]; y[q][2] = v[q + 8]; y[q][3] = v[q + 12];
-            dft4<R>(y[q][0], y[q][1], y[q][2], y[q][3], sign);
-        }
+        for (int q = 0; q < 4; ++q) dft4<R>(v[q], v[q + 4], v[q + 8], v[q + 12], sign);
         const R c1 = (R)0.92387953251128675613, s1 = (R)0.38268343236508977173;
         const R h = (R)0.70710678118654752440;
-        // q = 1: W16^k1, k1 = 1..3
-        y[1][1] = rot<C, R>(y[1][1], c1, s * s1);
-        y[1][2] = rot<C, R>(y[1][2], h, s * h);
-        y[1][3] = rot<C, R>(y[1][3], s1, s * c1);
-        // q = 2: W16^(2 k1) = W8^k1
-        y[2][1] = rot<C, R>(y[2][1], h, s * h);
-        y[2][2] = cmul_is<C, R>(y[2][2], s);
-        y[2][3] = rot<C, R>(y[2][3], -h, s * h);
-        // q = 3: W16^(3 k1): e = 3, 6, 9
-        y[3][1] = rot<C, R>(y[3][1], s1, s * c1);
-        y[3][2] = rot<C, R>(y[3][2], -h, s * h);
-        y[3][3] = rot<C, R>(y[3][3], -c1, -s * s1);
+        v[5] = rot<C, R>(v[5], c1, s * s1);     // q=1 k1=1: W16^1
+        v[9] = rot<C, R>(v[9], h, s * h);       // q=1 k1=2: W16^2
+        v[13] = rot<C, R>(v[13], s1, s * c1);   // q=1 k1=3: W16^3
+        v[6] = rot<C, R>(v[6], h, s * h);       // q=2 k1=1: W16^2
+        v[10] = cmul_is<C, R>(v[10], s);        // q=2 k1=2: W16^4
+        v[14] = rot<C, R>(v[14], -h, s * h);    // q=2 k1=3: W16^6
+        v[7] = rot<C, R>(v[7], s1, s * c1);     // q=3 k1=1: W16^3
+        v[11] = rot<C, R>(v[11], -h, s * h);    // q=3 k1=2: W16^6
+        v[15] = rot<C, R>(v[15], -c1, -s * s1); // q=3 k1=3: W16^9
 #pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) {
-            C a = y[0][k1], b = y[1][k1], c = y[2][k1], d = y[3][k1];
-            dft4<R>(a, b, c, d, sign);
-            v[k1] = a; v[k1 + 4] = b; v[k1 + 8] = c; v[k1 + 12] = d;
-        }
+        for (int k1 = 0; k1 < 4; ++k1) dft4<R>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3], sign);
+        // v[4 k1 + k2] holds X[k1 + 4 k2]: transpose the 4 x 4 block
+        C t;
+        t = v[1]; v[1] = v[4]; v[4] = t;
+        t = v[2]; v[2] = v[8]; v[8] = t;
+        t = v[3]; v[3] = v[12]; v[12] = t;
+        t = v[6]; v[6] = v[9]; v[9] = t;
+        t = v[7]; v[7] = v[13]; v[13] = t;
+        t = v[11]; v[11] = v[14]; v[14] = t;
     }
 }
 
 // One Stockham pass over nb transforms (in place, see header); each thread handles up
 // to MAXB butterflies.
+// Not inlined: each radix gets its own register allocation instead of sharing the
+// union of all radices' live ranges inside run().
 template <int RAD, int MAXB, typename R>
-RBC_D void pass(typename cplx_t<R>::type* buf, const Plan& p, int ns, int nb,
-                const typename cplx_t<R>::type* tw, int sign)
+__device__ __noinline__ void pass(typename cplx_t<R>::type* buf, const Plan& p, int ns, int nb,
+                                  const typename cplx_t<R>::type* tw, int sign)
 {
     typedef typename cplx_t<R>::type C;
     const int n = p.n;
@@ -207,8 +222,8 @@ RBC_D void run(typename cplx_t<R>::type* buf, const Plan& p, int nb, const typen
         if (r == 16) pass<16, 1, R>(buf, p, ns, nb, tw, sign);
         else if (r == 8) pass<8, 1, R>(buf, p, ns, nb, tw, sign);
         else if (r == 4) pass<4, 1, R>(buf, p, ns, nb, tw, sign);
-        else if (r == 2) pass<2, 2, R>(buf, p, ns, nb, tw, sign);
-        else pass<3, 2, R>(buf, p, ns, nb, tw, sign);
+        else if (r == 2) pass<2, 1, R>(buf, p, ns, nb, tw, sign);
+        else pass<3, 1, R>(buf, p, ns, nb, tw, sign);
         ns *= r;
     }
 }

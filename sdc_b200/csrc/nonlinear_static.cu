@@ -12,7 +12,7 @@
 //
 // The kernels are the same as those of rbc_nonlinear (step_kernels.cuh,
 // contract_kernel.cuh); only the placement of their scratch differs.
-#include "../../include/rbc.h"
+#include "rbc.h"
 #include "common.cuh"
 #include "contract_kernel.cuh"
 #include "fft.cuh"

@@ -1,7 +1,7 @@
 // peak_fp64.cu -- measures the device's FP64 FMA throughput (roofline denominator for
 // the FP64 contraction kernel; the driver's measured peaks cover HBM and BF16 only).
 // Each thread runs 8 independent DFMA chains; grid = 4 CTAs of 256 threads per SM.
-#include "../../include/rbc.h"
+#include "rbc.h"
 #include <cuda_runtime.h>
 
 __global__ void __launch_bounds__(256) k_dfma_peak(double* out, int iters, double a, double b)

@@ -1,0 +1,154 @@
+// rbc_run.cpp -- command-line driver over the C ABI, mirroring the reference's main.cu.
+//
+// Options follow gpu_flow/code/main.cu:61-232 and code/README.txt (only the ones of the
+// solver path):
+//   -nmodes M N L        physical points in x, y and vertical modes (mandatory)
+//   -clength Lx Ly       box lengths (mandatory)
+//   -ra Ra  -pr Pr       Rayleigh and Prandtl numbers (mandatory)
+//   -dt dt  -t T         time step and final time (mandatory); iterations = ceil(T/dt)
+//   -nfiles n            state dumps during the run (theta_%08d.bin ... every iters/n)
+//   -files th f g F G    restart from reference dump files (FP32 or FP64)
+//   -history file        also restore the AB2 history (exact restart; the reference has none)
+//   -device d  -dir path -seed s  -particles n
+//   -init_amp a -init_kmax k   seeded initial condition (replaces init_random)
+//   -form fp64|mixed     precision form
+//   -diag n              print Nu_wall, Nu_vol, KE every n steps
+//   -real_bytes 4|8      element size of the written dumps (4 = the reference's default)
+// Writes simulation.log (main.cu:402-426) and returns non-zero on any library error.
+#include "rbc.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <sys/stat.h>
+
+namespace {
+
+struct Args {
+    int argc;
+    char** argv;
+    int find(const char* name) const
+    {
+        for (int i = 1; i < argc; ++i)
+            if (!std::strcmp(argv[i], name)) return i;
+        return -1;
+    }
+    bool has(const char* name) const { return find(name) >= 0; }
+    const char* str(const char* name, int k = 0) const
+    {
+        const int i = find(name);
+        return (i >= 0 && i + 1 + k < argc) ? argv[i + 1 + k] : nullptr;
+    }
+    double num(const char* name, double def, int k = 0, bool mandatory = false) const
+    {
+        const char* s = str(name, k);
+        if (!s) {
+            if (mandatory) {
+                std::fprintf(stderr, "missing mandatory option %s\n", name);
+                std::exit(2);
+            }
+            return def;
+        }
+        return std::atof(s);
+    }
+};
+
+int check(rbc_status s, rbc_handle* h, const char* what)
+{
+    if (s == RBC_OK) return 0;
+    std::fprintf(stderr, "%s: %s (%s)\n", what, rbc_status_string(s), h ? rbc_last_error(h) : "");
+    return 1;
+}
+
+} // namespace
+
+int main(int argc, char** argv)
+{
+    Args a{argc, argv};
+    if (argc < 2 || a.has("-h") || a.has("--help")) {
+        std::printf("usage: rbc_run -nmodes M N L -clength Lx Ly -ra Ra -pr Pr -dt dt -t T [options]\n");
+        return argc < 2 ? 2 : 0;
+    }
+    rbc_params p{};
+    p.nx = (int)a.num("-nmodes", 0, 0, true);
+    p.ny = (int)a.num("-nmodes", 0, 1, true);
+    p.nz = (int)a.num("-nmodes", 0, 2, true);
+    p.lx = a.num("-clength", 0, 0, true);
+    p.ly = a.num("-clength", 0, 1, true);
+    p.ra = a.num("-ra", 0, 0, true);
+    p.pr = a.num("-pr", 0, 0, true);
+    p.dt = a.num("-dt", 0, 0, true);
+    const double tfinal = a.num("-t", 0, 0, true);
+    p.device = (int)a.num("-device", 0);
+    p.n_tracers = (int)a.num("-particles", 0);
+    const char* form = a.str("-form");
+    p.form = (form && !std::strcmp(form, "mixed")) ? RBC_FORM_MIXED : RBC_FORM_FP64;
+    const int nfiles = (int)a.num("-nfiles", 1);
+    const unsigned long long seed = (unsigned long long)a.num("-seed", 1);
+    const int diag_every = (int)a.num("-diag", 0);
+    const int real_bytes = (int)a.num("-real_bytes", 4);
+    const char* dir = a.str("-dir");
+    std::string out = dir ? dir : ".";
+    if (dir) mkdir(dir, 0755);
+
+    // number of iterations as main.cu:275-280 (iCeil(final_t / delta_t))
+    const long long iters = (long long)std::ceil(tfinal / p.dt);
+    const long long write_every = nfiles > 0 ? iters / nfiles : 0;
+
+    rbc_handle* h = nullptr;
+    if (check(rbc_create(&p, &h), nullptr, "rbc_create")) return 1;
+    int rc = 0;
+    if (a.has("-files")) {
+        rc |= check(rbc_load_state(h, a.str("-files", 0), a.str("-files", 1), a.str("-files", 2), a.str("-files", 3),
+                                   a.str("-files", 4)),
+                    h, "rbc_load_state");
+        if (!rc && a.has("-history")) rc |= check(rbc_load_history(h, a.str("-history")), h, "rbc_load_history");
+    } else {
+        rc |= check(rbc_init_fields(h, seed, a.num("-init_amp", 1e-3), a.num("-init_kmax", 4.0)), h, "rbc_init_fields");
+    }
+    if (!rc && p.n_tracers > 0) rc |= check(rbc_tracers_seed(h, seed), h, "rbc_tracers_seed");
+    if (rc) {
+        rbc_destroy(h);
+        return 1;
+    }
+
+    {
+        FILE* log = std::fopen((out + "/simulation.log").c_str(), "w");
+        if (log) {
+            std::fprintf(log, "Simulation of Rayleigh-Benard convection (sm_100a)\nRayleigh-Number: %g\nPrandtl-Number: %g\n"
+                              "delta t: %g\nfinal t: %g\nnumber of files: %d\nnumber of iterations: %lld\n"
+                              "cube length x direction: %g\ncube length y direction: %g\ncube length z direction: 1\n"
+                              "number of x modes: %d\nnumber of y modes: %d\nnumber of z modes: %d\ncommand string: ",
+                         p.ra, p.pr, p.dt, tfinal, nfiles, iters, p.lx, p.ly, p.nx, p.ny, p.nz);
+            for (int i = 0; i < argc; ++i) std::fprintf(log, "%s ", argv[i]);
+            std::fprintf(log, "\n");
+            std::fclose(log);
+        }
+    }
+
+    long long done = 0;
+    while (done < iters && !rc) {
+        long long chunk = iters - done;
+        if (write_every > 0) chunk = std::min(chunk, write_every - done % write_every);
+        if (diag_every > 0) chunk = std::min(chunk, diag_every - done % diag_every);
+        rc |= check(rbc_step(h, (int)chunk), h, "rbc_step");
+        done += chunk;
+        if (rc) break;
+        if (diag_every > 0 && done % diag_every == 0) {
+            rbc_diag d;
+            rc |= check(rbc_diagnostics(h, &d), h, "rbc_diagnostics");
+            std::printf("step %lld t %.6f Nu_wall %.12f Nu_vol %.12f KE %.6e\n", done, done * p.dt, d.nu_wall, d.nu_vol, d.ke);
+        }
+        if (write_every > 0 && done % write_every == 0) {
+            rc |= check(rbc_save_state(h, out.c_str(), done, real_bytes), h, "rbc_save_state");
+            char path[4096];
+            std::snprintf(path, sizeof path, "%s/history_%08lld.bin", out.c_str(), done);
+            rc |= check(rbc_save_history(h, path), h, "rbc_save_history");
+        }
+    }
+    rbc_destroy(h);
+    return rc;
+}

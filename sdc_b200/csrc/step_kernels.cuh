@@ -71,7 +71,7 @@ struct Mult {
 // Reference: nonlinear_operator_rayleigh_noslip.cu:112-233 (u11 = d_x f, u21 = d_y f,
 // u31 = q^2 f, u12 = d_y g + F, u22 = -d_x g + G, theta, d_x theta, d_y theta).
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_synth_columns(
+__global__ void __launch_bounds__(kThreads, 2) k_synth_columns(
     Geom G, int W, rbcfft::Plan py, const double2* __restrict__ twy, const double2* __restrict__ th,
     const double2* __restrict__ f, const double2* __restrict__ g, const double2* __restrict__ FG,
     typename cplx_t<R>::type* __restrict__ H)
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kThreads) k_synth_columns(
 // parts of the DC entries are dropped, as a C2R does. NP pairs per CTA, all in one
 // plane (NP divides Ny/2).
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_rows_c2r(
+__global__ void __launch_bounds__(kThreads, 2) k_rows_c2r(
     Geom G, int NP, rbcfft::Plan px, const double2* __restrict__ twx,
     const typename cplx_t<R>::type* __restrict__ H, R* __restrict__ phys)
 {
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(kThreads) k_rows_c2r(
 // A[n] = (Z[n] + conj Z[-n]) / 2, B[n] = (Z[n] - conj Z[-n]) / 2i, columns n < ckw
 // (zero for n >= ckeep). Output CM.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_rows_r2c(
+__global__ void __launch_bounds__(kThreads, 2) k_rows_r2c(
     Geom G, int NP, rbcfft::Plan px, const double2* __restrict__ twx,
     const R* __restrict__ grp, typename cplx_t<R>::type* __restrict__ gh)
 {
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kThreads) k_rows_r2c(
 // F_k and G_k (reference :950-1003) are the q = 0 entries of the g-y group and of
 // the negated g-x group, scaled like f. Grid (ckw, L).
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_columns_combine(
+__global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
     Geom G, rbcfft::Plan py, const double2* __restrict__ twy,
     const typename cplx_t<R>::type* __restrict__ gh, typename cplx_t<R>::type* __restrict__ N,
     double* __restrict__ NFG)

@@ -26,14 +26,14 @@ struct TracerArgs {
     double lx, ly, dt, zmax;
 };
 
-// Velocity (u, v, w) at the grid node xy on the levels z0 and z1 from the node record.
+template <int L> struct NodeRecLen { static constexpr int value = (5 * L + 1) & ~1; };
+
+// Loads the node record of grid point xy into registers.
 template <typename R, int L>
-RBC_D void node_velocity(const R* __restrict__ nv, size_t xy, const double* zb0, const double* zb1,
-                         double (&u0)[3], double (&u1)[3])
+RBC_D void load_record(const R* __restrict__ nv, size_t xy, R (&rec)[NodeRecLen<L>::value])
 {
-    constexpr int NR = (5 * L + 1) & ~1;
+    constexpr int NR = NodeRecLen<L>::value;
     typedef typename cplx_t<R>::type R2;
-    R rec[NR];
     const R2* src = reinterpret_cast<const R2*>(nv + xy * NR);
 #pragma unroll
     for (int q = 0; q < NR / 2; ++q) {
@@ -41,6 +41,13 @@ RBC_D void node_velocity(const R* __restrict__ nv, size_t xy, const double* zb0,
         rec[2 * q] = v.x;
         rec[2 * q + 1] = v.y;
     }
+}
+
+// Velocity (u, v, w) of a node on the levels z0 and z1 from its record.
+template <typename R, int L>
+RBC_D void node_velocity(const R (&rec)[NodeRecLen<L>::value], const double* zb0, const double* zb1,
+                         double (&u0)[3], double (&u1)[3])
+{
     double a0 = 0, b0 = 0, c0 = 0, a1 = 0, b1 = 0, c1 = 0;
 #pragma unroll
     for (int i = 0; i < L; ++i) {
@@ -58,8 +65,14 @@ RBC_D void node_velocity(const R* __restrict__ nv, size_t xy, const double* zb0,
     u1[0] = a1; u1[1] = b1; u1[2] = c1;
 }
 
+// Velocity at (x, y, z) by trilinear interpolation of the node velocities (the
+// reference's vel_interpolate). A team of 4 consecutive lanes handles one particle: lane
+// q takes the xy corner (q & 1, q >> 1), evaluates its node at the two bracketing levels,
+// weights it, and the team adds the 4 contributions with two shuffle rounds; every lane
+// of the team returns the sum.
 template <typename R, int L>
-RBC_D void vel_interp(const TracerArgs& A, const double* zb, double x, double y, double z, double& rx, double& ry, double& rz)
+RBC_D void vel_interp_team(const TracerArgs& A, const double* zb, int q, double x, double y, double z,
+                           double& rx, double& ry, double& rz, R (&rec)[NodeRecLen<L>::value], int& cached)
 {
     const R* nv = reinterpret_cast<const R*>(A.nv);
     const int xs = A.nx, ys = A.ny;
@@ -77,35 +90,29 @@ RBC_D void vel_interp(const TracerArgs& A, const double* zb, double x, double y,
     const int ix1 = (ix0 + 1 >= xs) ? 0 : ix0 + 1;
     const int iy1 = (iy0 + 1 >= ys) ? 0 : iy0 + 1;
     const int iz1 = (iz0 + 1 >= kZNum) ? iz0 : iz0 + 1;
-    const double* zb0 = zb + (size_t)iz0 * 3 * L;
-    const double* zb1 = zb + (size_t)iz1 * 3 * L;
-    double v00[2][3], v10[2][3], v01[2][3], v11[2][3]; // [z level][component], corners (x, y)
-    node_velocity<R, L>(nv, (size_t)iy0 * xs + ix0, zb0, zb1, v00[0], v00[1]);
-    node_velocity<R, L>(nv, (size_t)iy0 * xs + ix1, zb0, zb1, v10[0], v10[1]);
-    node_velocity<R, L>(nv, (size_t)iy1 * xs + ix0, zb0, zb1, v01[0], v01[1]);
-    node_velocity<R, L>(nv, (size_t)iy1 * xs + ix1, zb0, zb1, v11[0], v11[1]);
-    double wR = xg - (double)ix0, wL = 1 - wR;
-    double cz0y0[3], cz0y1[3], cz1y0[3], cz1y1[3];
+    const double wx1 = xg - (double)ix0, wx0 = 1 - wx1;
+    const double wy1 = yg - (double)iy0, wy0 = 1 - wy1;
+    const double wz1 = zg - (double)iz0, wz0 = 1 - wz1;
+    const int ix = (q & 1) ? ix1 : ix0, iy = (q >> 1) ? iy1 : iy0;
+    const double w = ((q & 1) ? wx1 : wx0) * ((q >> 1) ? wy1 : wy0);
+    // RK stages rarely leave the cell: reload this corner's record only when it changed
+    const int node = iy * xs + ix;
+    if (node != cached) {
+        load_record<R, L>(nv, (size_t)node, rec);
+        cached = node;
+    }
+    double u0[3], u1[3];
+    node_velocity<R, L>(rec, zb + (size_t)iz0 * 3 * L, zb + (size_t)iz1 * 3 * L, u0, u1);
+    double v[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        cz0y0[d] = wL * v00[0][d] + wR * v10[0][d];
-        cz0y1[d] = wL * v01[0][d] + wR * v11[0][d];
-        cz1y0[d] = wL * v00[1][d] + wR * v10[1][d];
-        cz1y1[d] = wL * v01[1][d] + wR * v11[1][d];
+        v[d] = w * (wz0 * u0[d] + wz1 * u1[d]);
+        v[d] += __shfl_xor_sync(0xffffffffu, v[d], 1, 4);
+        v[d] += __shfl_xor_sync(0xffffffffu, v[d], 2, 4);
     }
-    wR = yg - (double)iy0;
-    wL = 1 - wR;
-    double c0[3], c1[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        c0[d] = wL * cz0y0[d] + wR * cz0y1[d];
-        c1[d] = wL * cz1y0[d] + wR * cz1y1[d];
-    }
-    wR = zg - (double)iz0;
-    wL = 1 - wR;
-    rx = wL * c0[0] + wR * c1[0];
-    ry = wL * c0[1] + wR * c1[1];
-    rz = wL * c0[2] + wR * c1[2];
+    rx = v[0];
+    ry = v[1];
+    rz = v[2];
 }
 
 template <typename R, int L>
@@ -114,18 +121,22 @@ __global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
     __shared__ double zb[kZNum * 3 * L];
     for (int e = threadIdx.x; e < kZNum * 3 * L; e += blockDim.x) zb[e] = A.zbasis[e];
     __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= A.n) return;
-    double x = A.pos[t], y = A.pos[A.n + t], z = A.pos[2 * A.n + t];
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = gt >> 2, q = gt & 3;               // particle, corner lane
+    const bool live = t < A.n;                       // whole teams are live or not
+    const int tt = live ? t : 0;
+    double x = A.pos[tt], y = A.pos[A.n + tt], z = A.pos[2 * A.n + tt];
     const double dt = A.dt;
     double vx, vy, vz;
-    vel_interp<R, L>(A, zb, x, y, z, vx, vy, vz);
+    R rec[NodeRecLen<L>::value];
+    int cached = -1;
+    vel_interp_team<R, L>(A, zb, q, x, y, z, vx, vy, vz, rec, cached);
     const double dx1 = dt * vx, dy1 = dt * vy, dz1 = dt * vz;
-    vel_interp<R, L>(A, zb, x + 0.5 * dx1, y + 0.5 * dy1, z + 0.5 * dz1, vx, vy, vz);
+    vel_interp_team<R, L>(A, zb, q, x + 0.5 * dx1, y + 0.5 * dy1, z + 0.5 * dz1, vx, vy, vz, rec, cached);
     const double dx2 = dt * vx, dy2 = dt * vy, dz2 = dt * vz;
-    vel_interp<R, L>(A, zb, x + 0.5 * dx2, y + 0.5 * dy2, z + 0.5 * dz2, vx, vy, vz);
+    vel_interp_team<R, L>(A, zb, q, x + 0.5 * dx2, y + 0.5 * dy2, z + 0.5 * dz2, vx, vy, vz, rec, cached);
     const double dx3 = dt * vx, dy3 = dt * vy, dz3 = dt * vz;
-    vel_interp<R, L>(A, zb, x + dx3, y + dy3, z + dz3, vx, vy, vz);
+    vel_interp_team<R, L>(A, zb, q, x + dx3, y + dy3, z + dz3, vx, vy, vz, rec, cached);
     const double dx4 = dt * vx, dy4 = dt * vy, dz4 = dt * vz;
     x += (dx1 + 2 * (dx2 + dx3) + dx4) / 6.;
     y += (dy1 + 2 * (dy2 + dy3) + dy4) / 6.;
@@ -133,9 +144,11 @@ __global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
     const double zm = A.zmax;
     if (!(z <= zm)) z = (z < 2 * zm) ? 2 * zm - z : zm;  // also sends NaN to the lid
     else if (z < -zm) z = (z > -2 * zm) ? -2 * zm - z : -zm;
-    A.pos[t] = x;
-    A.pos[A.n + t] = y;
-    A.pos[2 * A.n + t] = z;
+    if (live && q == 0) {
+        A.pos[t] = x;
+        A.pos[A.n + t] = y;
+        A.pos[2 * A.n + t] = z;
+    }
 }
 
 } // namespace rbck

@@ -1,7 +1,8 @@
 // update_kernel.cuh -- fused per-wavenumber update of the IMEX step (sm_100a, FP64).
 //
 // One team of T = next_pow2(L) lanes per kept wavenumber (c, r); lane k owns vertical
-// mode k and the team exchanges modes with warp shuffles. Per wavenumber it does:
+// mode k and the team exchanges its mode vectors through a per-warp shared-memory slot.
+// Per wavenumber it does:
 //   inverse B        (inverse_B_matrix.cu:199-328): theta x2, f by the L x L B_ff^-1 of
 //                    its q^2 class, g x (-2 Pr / q^2) (0 at q = 0), F, G x 2 Pr (Im = 0)
 //   AB2 / Euler      (implicit_explicit_stepping.cu:43-69): u += 1.5dt r - 0.5dt r_prev
@@ -52,115 +53,140 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
 {
     typedef typename cplx_t<R>::type C;
     constexpr int T = TeamSize<L>::value;
-    __shared__ double dtab[3 * L * L];
-    for (int e = threadIdx.x; e < 3 * L * L; e += blockDim.x) dtab[e] = A.diag_tab[e];
-    __syncthreads();
+    constexpr int TPW = 32 / T;                 // teams per warp
+    // per-warp staging of the team vectors: [team][mode] (instead of shuffles)
+    __shared__ double2 stg[kThreads / 32][2][TPW][T];
+    const double* dtab = A.diag_tab;            // [3][L*L], read through the L1 cache
     const Geom& G = A.G;
     const int ny = G.ny;
     const size_t plane = (size_t)G.ckp * ny;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int e = gt / T;            // wavenumber: c * ny + r
-    const int k = gt - e * T;        // this lane's vertical mode
-    const int c = e / ny, r = e - c * ny;
-    const int cl = (c < G.ckeep) ? A.cls[e] : -1;  // uniform over the team
-    const bool act = cl >= 0;
-    const bool kact = act && k < L;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int tm = lane / T;                    // team within the warp
+    const int k = lane - tm * T;                // this lane's vertical mode
     const C* Nc = reinterpret_cast<const C*>(A.N);
-    const size_t o = (size_t)e;
-    double esum = 0.0, wsum = 0.0;
-    const int ry = wrap_row(r, ny);
-    const double mx = (kPi + kPi) * (c / G.lx), my = (kPi + kPi) * (ry / G.ly);
-    const double q2d = mx * mx + my * my;           // device formula of the reference kernels
-    const bool mirror = (c == 0 && r > 0 && r < ny / 2);
     const double dt = G.dt, pr = G.pr;
     const double a1 = A.first ? dt : 1.5 * dt, a2 = -0.5 * dt;
-    // ---------------- inverse B
-    double2 nt = make_double2(0, 0), nf = nt, ng = nt;
-    if (kact) {
-        const C t0 = Nc[(0 * L + k) * plane + o], t1 = Nc[(1 * L + k) * plane + o], t2 = Nc[(2 * L + k) * plane + o];
-        nt = make_double2(t0.x, t0.y);
-        nf = make_double2(t1.x, t1.y);
-        ng = make_double2(t2.x, t2.y);
-    }
-    const double2 bt = nt * 2.0;
-    double2 bf = make_double2(0, 0);
-    const double* bi = A.binv + (size_t)(act ? cl : 0) * L * L + (size_t)(k < L ? k : 0) * L;
-#pragma unroll
-    for (int m = 0; m < L; ++m) {
-        const double2 v = shfl2(nf, m, T);
-        const double op = kact ? bi[m] : 0.0;
-        bf = make_double2(bf.x + op * v.x, bf.y + op * v.y);
-    }
-    const double2 bg = (q2d != 0.0) ? ng * ((-2.0) * pr / q2d) : make_double2(0, 0);
-    // ---------------- AB2 and history
-    double2 ut = make_double2(0, 0), uf = ut, ug = ut;
-    if (kact) {
-        double2* hp = A.hist + o;
-        if (!mirror) {
-            ut = A.th[k * plane + o];
-            uf = A.f[k * plane + o];
-            ug = A.g[k * plane + o];
-            ut = make_double2(fma(bt.x, a1, ut.x), fma(bt.y, a1, ut.y));
-            uf = make_double2(fma(bf.x, a1, uf.x), fma(bf.y, a1, uf.y));
-            ug = make_double2(fma(bg.x, a1, ug.x), fma(bg.y, a1, ug.y));
-            if (!A.first) {
-                const double2 ht = hp[(0 * L + k) * plane], hf = hp[(1 * L + k) * plane], hg = hp[(2 * L + k) * plane];
-                ut = make_double2(fma(ht.x, a2, ut.x), fma(ht.y, a2, ut.y));
-                uf = make_double2(fma(hf.x, a2, uf.x), fma(hf.y, a2, uf.y));
-                ug = make_double2(fma(hg.x, a2, ug.x), fma(hg.y, a2, ug.y));
-            }
-        }
-        hp[(0 * L + k) * plane] = bt;
-        hp[(1 * L + k) * plane] = bf;
-        hp[(2 * L + k) * plane] = bg;
-    }
-    // ---------------- implicit solve
-    double2 to = make_double2(0, 0), fo = to;
-    const double* M = A.imp + (size_t)(act ? cl : 0) * 4 * L * L + (size_t)(k < L ? k : 0) * L;
-#pragma unroll
-    for (int m = 0; m < L; ++m) {
-        const double2 vt = shfl2(ut, m, T), vf = shfl2(uf, m, T);
-        if (kact) {
-            const double tt = M[m], tf = M[L * L + m], ft = M[2 * L * L + m], ff = M[3 * L * L + m];
-            to = make_double2(to.x + (tt * vt.x + tf * vf.x), to.y + (tt * vt.y + tf * vf.y));
-            fo = make_double2(fo.x + (ft * vt.x + ff * vf.x), fo.y + (ft * vt.y + ff * vf.y));
-        }
-    }
     const double mpi = (k + 1) * kPi;
-    double2 go = (q2d != 0.0) ? ug * (1.0 / (1.0 + dt * pr * (q2d + mpi * mpi))) : make_double2(0, 0);
-    if (c == 0 && r == 0) { to.y = 0; fo.y = 0; go.y = 0; }
-    if (kact && !mirror) {
-        A.th[k * plane + o] = to;
-        A.f[k * plane + o] = fo;
-        A.g[k * plane + o] = go;
-        if (c == 0 && r > ny / 2) {
-            const size_t om = (size_t)(ny - r);
-            A.th[k * plane + om] = cconj(to);
-            A.f[k * plane + om] = cconj(fo);
-            A.g[k * plane + om] = cconj(go);
-        }
-        if (!isfinite(to.x + to.y + fo.x + fo.y + go.x + go.y)) atomicOr(A.err, RBC_DEVERR_NAN);
-    }
-    // ---------------- diagnostics: Parseval over the full spectrum; columns c > 0 stand
-    // for +-kx (weight 2), the kx = 0 team of row Ny - r also for its mirror row r.
+    double esum = 0.0, wsum = 0.0;
+    const long long nwave = (long long)G.ckeep * ny;
     {
-        const double wq = (c > 0 || r > ny / 2) ? 2.0 : 1.0;
-        const double qx = 2 * kPi * c / G.lx, qy = 2 * kPi * ry / G.ly, q2 = qx * qx + qy * qy;
-        double eff = 0, ecc = 0, wt = 0;
+        const long long e = (long long)blockIdx.x * (blockDim.x / T) + threadIdx.x / T; // wavenumber c * ny + r
+        const int c = (int)(e / ny), r = (int)(e - (long long)c * ny);
+        const int cl = (e < nwave) ? A.cls[e] : -1;          // uniform over the team
+        const bool act = cl >= 0;
+        const bool kact = act && k < L;
+        const size_t o = (size_t)e;
+        const int ry = wrap_row(r, ny);
+        const double mx = (kPi + kPi) * (c / G.lx), my = (kPi + kPi) * (ry / G.ly);
+        const double q2d = mx * mx + my * my;       // device formula of the reference kernels
+        const bool mirror = (c == 0 && r > 0 && r < ny / 2);
+        double2 nt = make_double2(0, 0), nf = nt, ng = nt, ut = nt, uf = nt, ug = nt, ht = nt, hf = nt, hg = nt;
+        double bi[L], M[4][L];
+        if (kact) {
+            const C t0 = Nc[(0 * L + k) * plane + o], t1 = Nc[(1 * L + k) * plane + o], t2 = Nc[(2 * L + k) * plane + o];
+            nt = make_double2(t0.x, t0.y);
+            nf = make_double2(t1.x, t1.y);
+            ng = make_double2(t2.x, t2.y);
+            const double* brow = A.binv + (size_t)cl * L * L + (size_t)k * L;
+            const double* mrow = A.imp + (size_t)cl * 4 * L * L + (size_t)k * L;
 #pragma unroll
-        for (int j = 0; j < L; ++j) {
-            const double2 fj = shfl2(fo, j, T), tj = shfl2(to, j, T);
-            if (kact) {
-                const double ff = fo.x * fj.x + fo.y * fj.y;
-                eff += dtab[k + j * L] * ff;
-                ecc += dtab[L * L + k + j * L] * ff;
-                wt += dtab[2 * L * L + k + j * L] * (fo.x * tj.x + fo.y * tj.y);
+            for (int m = 0; m < L; ++m) {
+                bi[m] = brow[m];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) M[b][m] = mrow[b * L * L + m];
+            }
+            if (!mirror) {
+                ut = A.th[k * plane + o];
+                uf = A.f[k * plane + o];
+                ug = A.g[k * plane + o];
+                if (!A.first) {
+                    ht = A.hist[(0 * L + k) * plane + o];
+                    hf = A.hist[(1 * L + k) * plane + o];
+                    hg = A.hist[(2 * L + k) * plane + o];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < L; ++m) {
+                bi[m] = 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) M[b][m] = 0;
             }
         }
+        // ---------------- inverse B (f needs the team's N_f)
+        stg[wid][0][tm][k] = nf;
+        __syncwarp();
+        const double2 bt = nt * 2.0;
+        double2 bf = make_double2(0, 0);
+#pragma unroll
+        for (int m = 0; m < L; ++m) {
+            const double2 v = stg[wid][0][tm][m];
+            bf = make_double2(bf.x + bi[m] * v.x, bf.y + bi[m] * v.y);
+        }
+        const double2 bg = (q2d != 0.0) ? ng * ((-2.0) * pr / q2d) : make_double2(0, 0);
+        // ---------------- AB2 and history
+        if (kact) {
+            if (!mirror) {
+                ut = make_double2(fma(bt.x, a1, ut.x), fma(bt.y, a1, ut.y));
+                uf = make_double2(fma(bf.x, a1, uf.x), fma(bf.y, a1, uf.y));
+                ug = make_double2(fma(bg.x, a1, ug.x), fma(bg.y, a1, ug.y));
+                if (!A.first) {
+                    ut = make_double2(fma(ht.x, a2, ut.x), fma(ht.y, a2, ut.y));
+                    uf = make_double2(fma(hf.x, a2, uf.x), fma(hf.y, a2, uf.y));
+                    ug = make_double2(fma(hg.x, a2, ug.x), fma(hg.y, a2, ug.y));
+                }
+            }
+            A.hist[(0 * L + k) * plane + o] = bt;
+            A.hist[(1 * L + k) * plane + o] = bf;
+            A.hist[(2 * L + k) * plane + o] = bg;
+        }
+        // ---------------- implicit solve
+        __syncwarp();
+        stg[wid][0][tm][k] = ut;
+        stg[wid][1][tm][k] = uf;
+        __syncwarp();
+        double2 to = make_double2(0, 0), fo = to;
+#pragma unroll
+        for (int m = 0; m < L; ++m) {
+            const double2 vt = stg[wid][0][tm][m], vf = stg[wid][1][tm][m];
+            to = make_double2(to.x + (M[0][m] * vt.x + M[1][m] * vf.x), to.y + (M[0][m] * vt.y + M[1][m] * vf.y));
+            fo = make_double2(fo.x + (M[2][m] * vt.x + M[3][m] * vf.x), fo.y + (M[2][m] * vt.y + M[3][m] * vf.y));
+        }
+        double2 go = (q2d != 0.0) ? ug * (1.0 / (1.0 + dt * pr * (q2d + mpi * mpi))) : make_double2(0, 0);
+        if (c == 0 && r == 0) { to.y = 0; fo.y = 0; go.y = 0; }
         if (kact && !mirror) {
+            A.th[k * plane + o] = to;
+            A.f[k * plane + o] = fo;
+            A.g[k * plane + o] = go;
+            if (c == 0 && r > ny / 2) {
+                const size_t om = (size_t)(ny - r);
+                A.th[k * plane + om] = cconj(to);
+                A.f[k * plane + om] = cconj(fo);
+                A.g[k * plane + om] = cconj(go);
+            }
+            if (!isfinite(to.x + to.y + fo.x + fo.y + go.x + go.y)) atomicOr(A.err, RBC_DEVERR_NAN);
+        }
+        // ---------------- diagnostics: Parseval over the full spectrum; columns c > 0
+        // stand for +-kx (weight 2), the kx = 0 team of row Ny - r also for row r.
+        __syncwarp();
+        stg[wid][0][tm][k] = to;
+        stg[wid][1][tm][k] = fo;
+        __syncwarp();
+        if (kact && !mirror) {
+            const double wq = (c > 0 || r > ny / 2) ? 2.0 : 1.0;
+            const double qx = 2 * kPi * c / G.lx, qy = 2 * kPi * ry / G.ly, q2 = qx * qx + qy * qy;
+            double eff = 0, ecc = 0, wt = 0;
+#pragma unroll
+            for (int j = 0; j < L; ++j) {
+                const double2 tj = stg[wid][0][tm][j], fj = stg[wid][1][tm][j];
+                const double ff = fo.x * fj.x + fo.y * fj.y;
+                eff += __ldg(dtab + k + j * L) * ff;
+                ecc += __ldg(dtab + L * L + k + j * L) * ff;
+                wt += __ldg(dtab + 2 * L * L + k + j * L) * (fo.x * tj.x + fo.y * tj.y);
+            }
             const double egg = go.x * go.x + go.y * go.y;
-            esum = wq * (q2 * eff + 0.5 * q2 * egg + q2 * q2 * ecc);
-            wsum = wq * q2 * wt;
+            esum += wq * (q2 * eff + 0.5 * q2 * egg + q2 * q2 * ecc);
+            wsum += wq * q2 * wt;
             if (c == 0 && r == 0) {
                 const double fac = 1.0 / (1.0 + dt * pr * mpi * mpi);
 #pragma unroll
@@ -186,7 +212,6 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
     }
     __shared__ double red[2][kThreads / 32];
     __shared__ bool last;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) { red[0][wid] = esum; red[1][wid] = wsum; }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -219,6 +244,7 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
     }
 }
 
+// One team per kept-column wavenumber.
 template <int L> inline int update_blocks(int ckeep, int ny)
 {
     const long long threads = (long long)ckeep * ny * TeamSize<L>::value;
