@@ -198,6 +198,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", type=int, default=1, help="1: autotune the FFT launch tiling at creation")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -217,7 +218,8 @@ def main():
     import numpy as np
     import sdc_b200
 
-    s = sdc_b200.Solver(**WORK, form=args.form, n_tracers=NTRACERS, device=local)
+    s = sdc_b200.Solver(**WORK, form=args.form, n_tracers=NTRACERS, device=local, tune=bool(args.tune))
+    W, NP = s.launch_config
     # one dedicated stream for the library and the timing events
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
@@ -300,6 +302,7 @@ def main():
                 "config": {"workload": f"plain {args.form.upper()} RBC step 256x256x8, Lx=Ly=32, Ra=5000, "
                                        f"Pr=0.9, dt=5e-4, +65536 tracers (RK4, 128 z levels)",
                            "form": args.form, "parallelism": f"replicas x{world}",
+                           "launch": {"autotuned": bool(args.tune), "column_block": W, "row_pairs": NP},
                            "l2": "working set > 126 MB L2 (state, history, scratch ~300 MB); no flush",
                            "alg_bytes_per_step": step_b + tr_b},
                 "roofline": roof, "gpu_launches": launches,

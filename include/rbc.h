@@ -60,6 +60,12 @@ typedef struct {
     int diag_capacity; /* per-step diagnostics ring entries (0: 4096) */
     int tune;        /* 1: time the launch tilings of the FFT kernels at creation and keep
                         the fastest (project autotuner); 0: built-in heuristic */
+    double tracer_diffusivity; /* D, the reference's -le value: after every RK4 advance each
+                        coordinate moves by sqrt(2 D dt) N(0,1) (diffuse_particles,
+                        gpu_flow/code/particle/particle_tracer.cu:194-199, 690-716); 0: none */
+    unsigned long long noise_seed; /* seed of that noise (see rbc_tracers_advance) */
+    int track_frames;  /* device ring of recorded tracer positions, in frames (0: no tracks) */
+    int track_period;  /* steps between recorded frames (0 or 1: every step) */
 } rbc_params;
 
 /* Diagnostics of the state after a step (no reference counterpart). */
@@ -149,10 +155,53 @@ rbc_status rbc_tracers_set(rbc_handle* h, const double* xyz, int n);
 rbc_status rbc_tracers_get(rbc_handle* h, double* xyz, int n);
 /* Uniform seeded positions in [0,Lx) x [0,Ly) x (-1/2,1/2) (SplitMix64). */
 rbc_status rbc_tracers_seed(rbc_handle* h, unsigned long long seed);
+/* Initial positions by pattern, as particle_tracer::init_positions
+ * (particle_tracer.cu:58-137, 376-450). Uniform and normal draws come from the
+ * SplitMix64 stream of `seed` (uniform ((u >> 11) + 1/2) 2^-53, normal by Box-Muller
+ * cos(2 pi u2) sqrt(-2 ln u1)):
+ *   RANDOM        x = Lx u, y = Ly u, z = u - 1/2 per particle (= rbc_tracers_seed)
+ *   CENTER        all at (Lx/2, Ly/2, 0)
+ *   CENTER_SIGMA  (Lx/2, Ly/2, 0) + sigma N(0,1) per coordinate
+ *   DIAGONAL      x = Lx i / n, y = Ly i / n, z = 0
+ *   PAIRS         particles 2i and 2i+1 at the same (Lx u, Ly u, 0); n even
+ *   COORD_SIGMA   (cx, cy, cz) + sigma N(0,1) per coordinate
+ * Like the reference, the sigma spread is not reflected at the lids. */
+typedef enum {
+    RBC_TRACERS_RANDOM = 0, RBC_TRACERS_CENTER = 1, RBC_TRACERS_CENTER_SIGMA = 2,
+    RBC_TRACERS_DIAGONAL = 3, RBC_TRACERS_PAIRS = 4, RBC_TRACERS_COORD_SIGMA = 5
+} rbc_tracer_init;
+rbc_status rbc_tracers_init(rbc_handle* h, int type, unsigned long long seed, double cx, double cy,
+                            double cz, double sigma);
 /* One tracer step with the current velocity field (particle_tracer::step_particles,
  * particle_tracer.cu:141-212: RK4, trilinear interpolation on 128 z levels, periodic x/y,
- * reflection at z = +-(1/2 - 1e-3)); rbc_step calls it after every fluid step. */
+ * then the diffusion step when tracer_diffusivity > 0, then reflection at
+ * z = +-(1/2 - 1e-3)); rbc_step calls it after every fluid step. The diffusion normals
+ * are counter-based: for the positions of step m, particle t and coordinate d, the
+ * uniforms are elements 2j and 2j+1 (0-based) of the SplitMix64 stream of noise_seed
+ * with j = 3 (m n + t) + d, and the normal is cos(2 pi u2) sqrt(-2 ln u1). */
 rbc_status rbc_tracers_advance(rbc_handle* h);
+/* Moments of the current positions in FP64 (particle_tracer::calc_secondmoment and
+ * calc_pair_secondmoment, particle_tracer.cu:217-259, 771-870):
+ *   out[0] = <x>, out[1] = <y>, out[2] = <x^2 + y^2> - <x>^2 - <y>^2,
+ *   out[3] = sum over pairs (2i, 2i+1) of dx^2 + dy^2, each |d| above half the box
+ *            replaced by box - |d| (PERIODIC), divided by n/2 (integer division). */
+rbc_status rbc_tracer_moments(rbc_handle* h, double* out);
+/* Recorded tracks (the reference's position buffer, get_particle_positions and
+ * track_writer::append, particle_tracer.cu:273-309, output/track_writer.cu:21-70).
+ * With track_frames > 0 the positions of every step m with m % track_period == 0 are
+ * kept as FP32 frames (the reference's TRACK_FLOAT_REAL) in a device ring; the frame of
+ * the initial positions is recorded when tracers are set on such a step. This call moves
+ * the unread frames, oldest first, to xyz[frame][3][n] (x, y, z blocks) and their step
+ * numbers to times; *nframes receives the count (at most max_frames; the rest stay
+ * unread). rbc_step refuses (RBC_ERR_INVALID_ARG) to run steps whose frames would not
+ * fit in the ring, as step_particles stops on a full buffer. */
+rbc_status rbc_tracks_read(rbc_handle* h, float* xyz, unsigned int* times, int max_frames, int* nframes);
+/* Writes frames as a TRKSS track file, version 'a' (track_movie::Write,
+ * gpu_flow/code/output/track_movie.cpp:256-325): "TRKSS", 'a', uint32 tracks, uint32
+ * frame rate 1, uint32 length + description, uint32 first and last frame time, uint32
+ * frame count, then per frame uint32 time and x, y, z float32 per track. Host only. */
+rbc_status rbc_track_write(const char* path, const char* description, const float* xyz,
+                           const unsigned int* times, int nframes, int n);
 
 /* --- diagnostics --------------------------------------------------------------- */
 /* Diagnostics of the latest step (or of the initial state before any step). */

@@ -69,6 +69,11 @@ def lib():
         L.oracle_init_theta.restype = None
         L.oracle_tracer_positions.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp]
         L.oracle_tracer_positions.restype = None
+        L.oracle_set_diffusion.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64]
+        L.oracle_set_diffusion.restype = None
+        L.oracle_tracer_pattern.argtypes = ([ctypes.c_int, ctypes.c_uint64, ctypes.c_int] + [ctypes.c_double] * 6 +
+                                            [_dp])
+        L.oracle_tracer_pattern.restype = None
         _LIB = L
     return _LIB
 
@@ -117,6 +122,55 @@ def tracer_positions(seed, n, lx, ly):
     out = np.zeros(3 * n)
     lib().oracle_tracer_positions(seed, n, lx, ly, _ptr(out))
     return out
+
+
+def tracer_pattern(kind, seed, n, lx, ly, coord=(0.0, 0.0, 0.0), sigma=0.0):
+    """Start positions of particle_tracer::init_positions (0 random ... 5 coord_sigma)."""
+    out = np.zeros(3 * n)
+    lib().oracle_tracer_pattern(kind, seed, n, lx, ly, *coord, sigma, _ptr(out))
+    return out
+
+
+def tracer_moments(xyz, lx, ly):
+    """calc_moments_on_GPU and calc_pair_secondmoment_on_GPU (particle_tracer.cu:771-870)
+    restated in FP64: <x>, <y>, <x^2+y^2> - <x>^2 - <y>^2, and the mean over pairs
+    (2i, 2i+1) of the squared separation with the PERIODIC minimum image, divided by n/2."""
+    n = xyz.size // 3
+    x, y = xyz[:n], xyz[n:2 * n]
+    mx, my = x.mean(), y.mean()
+    m2 = (x * x + y * y).mean() - mx * mx - my * my
+    m = (n // 2) * 2 if n % 2 == 0 else n - 1
+    dx = np.abs(x[1:m:2] - x[0:m:2])
+    dy = np.abs(y[1:m:2] - y[0:m:2])
+    dx = np.where(dx > 0.5 * lx, lx - dx, dx)
+    dy = np.where(dy > 0.5 * ly, ly - dy, dy)
+    return np.array([mx, my, m2, (dx * dx + dy * dy).sum() / (n // 2)])
+
+
+def read_trkss(path):
+    """Parses a TRKSS version 'a' track file (track_movie::Write,
+    gpu_flow/code/output/track_movie.cpp:256-325) into a dict."""
+    import struct
+    b = open(path, "rb").read()
+    assert b[:5] == b"TRKSS"
+    version = b[5:6]
+    ntr, fs, dl = struct.unpack_from("<3I", b, 6)
+    o = 18
+    desc = b[o:o + dl].decode()
+    o += dl
+    tmin, tmax, nfr = struct.unpack_from("<3I", b, o)
+    o += 12
+    times, frames = [], []
+    for _ in range(nfr):
+        times.append(struct.unpack_from("<I", b, o)[0])
+        o += 4
+        xyz = np.frombuffer(b, "<f4", 3 * ntr, o).reshape(ntr, 3)
+        o += 12 * ntr
+        frames.append(xyz.T.copy())
+    assert o == len(b)
+    return {"version": version, "tracks": ntr, "fs": fs, "description": desc, "time_min": tmin,
+            "time_max": tmax, "times": np.array(times, np.uint32),
+            "frames": np.array(frames, np.float32).reshape(nfr, 3, ntr)}
 
 
 class Oracle:
@@ -180,6 +234,9 @@ class Oracle:
 
     def tracers_advance(self):
         lib().oracle_tracers_advance(self.h)
+
+    def set_diffusion(self, D, seed):
+        lib().oracle_set_diffusion(self.h, D, seed)
 
     def velocity_grid(self):
         shp = (128, self.ny, self.nx)

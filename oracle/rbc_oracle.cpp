@@ -364,6 +364,27 @@ struct FFT2 {
     }
 };
 
+// ---------------------------------------------------------------- tracer diffusion noise
+// diffuse_particles (particle_tracer.cu:690-716) adds sigma N(0,1) to every coordinate
+// after the RK4 advance, sigma = sqrt(2 D dt) (:194-199). The reference draws from cuRAND;
+// the build's normal for the positions of step m, particle t of n and coordinate d is
+// Box-Muller on elements 2j and 2j+1 (0-based) of the SplitMix64 stream of the seed,
+// j = 3 (m n + t) + d. Element i is the generator's output after i + 1 increments.
+static inline uint64_t splitmix64_at(uint64_t seed, uint64_t i)
+{
+    uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+static inline double diffusion_normal(uint64_t seed, long long m, long long n, long long t, int d)
+{
+    const uint64_t j = 3ULL * ((uint64_t)m * (uint64_t)n + (uint64_t)t) + (uint64_t)d;
+    const double u1 = ((splitmix64_at(seed, 2 * j) >> 11) + 0.5) / 9007199254740992.0;
+    const double u2 = ((splitmix64_at(seed, 2 * j + 1) >> 11) + 0.5) / 9007199254740992.0;
+    return std::cos(2.0 * PI * u2) * std::sqrt(-2.0 * std::log(u1));
+}
+
 // ---------------------------------------------------------------- solver
 struct Params {
     int nx, ny, L;
@@ -1024,9 +1045,15 @@ struct Solver {
 
     // particle_tracer::step_particles (:141-212) with step_particle_on_GPU (RK4) and
     // periodic_boundaries (PERIODIC: only the z reflection).
-    void step_tracers()
+    // Tracer diffusion (D, the reference's -le value) and the seed of its noise.
+    double tr_diff = 0.0;
+    uint64_t noise_seed = 0;
+
+    // particle_tracer::step_particles for the positions of step m.
+    void step_tracers(long long m)
     {
         if (tx.empty()) return;
+        const double sig = tr_diff > 0 ? std::sqrt(2.0 * tr_diff * p.dt) : 0.0;
         std::vector<double> ux, uy, uz;
         velocity_grid(ux, uy, uz);
         const double dt = p.dt;
@@ -1047,6 +1074,11 @@ struct Solver {
             x += (dx1 + 2 * (dx2 + dx3) + dx4) / 6.;
             y += (dy1 + 2 * (dy2 + dy3) + dy4) / 6.;
             z += (dz1 + 2 * (dz2 + dz3) + dz4) / 6.;
+            if (sig > 0) {
+                x += sig * diffusion_normal(noise_seed, m, n, t, 0);
+                y += sig * diffusion_normal(noise_seed, m, n, t, 1);
+                z += sig * diffusion_normal(noise_seed, m, n, t, 2);
+            }
             if (!(z <= zm)) {
                 if (z < 2 * zm) z = 2 * zm - z;
                 else z = zm;
@@ -1067,7 +1099,7 @@ struct Solver {
         make_real(th);
         make_real(f);
         make_real(g);
-        step_tracers();
+        step_tracers(steps + 1);
         ++steps;
     }
 
@@ -1250,7 +1282,12 @@ void oracle_tracers_get(oracle_handle* h, double* xyz)
     std::memcpy(xyz + 2 * n, s.tz.data(), n * sizeof(double));
 }
 // Advances tracers with the current velocity field only (no fluid step).
-void oracle_tracers_advance(oracle_handle* h) { h->s.step_tracers(); }
+void oracle_tracers_advance(oracle_handle* h) { h->s.step_tracers(h->s.steps); }
+void oracle_set_diffusion(oracle_handle* h, double D, uint64_t seed)
+{
+    h->s.tr_diff = D;
+    h->s.noise_seed = seed;
+}
 void oracle_velocity_grid(oracle_handle* h, double* ux, double* uy, double* uz)
 {
     Solver& s = h->s;
@@ -1372,6 +1409,54 @@ void oracle_tracer_positions(uint64_t seed, int n, double lx, double ly, double*
         xyz[i] = lx * u01(st);
         xyz[n + i] = ly * u01(st);
         xyz[2 * n + i] = u01(st) - 0.5;
+    }
+}
+
+// Start patterns of particle_tracer::init_positions (particle_tracer.cu:58-137, 376-450)
+// with SplitMix64 draws in place of cuRAND: 0 random, 1 center, 2 center_sigma,
+// 3 diagonal, 4 pairs, 5 coord_sigma.
+void oracle_tracer_pattern(int type, uint64_t seed, int n, double lx, double ly, double cx, double cy, double cz,
+                           double sigma, double* xyz)
+{
+    double *x = xyz, *y = xyz + n, *z = xyz + 2 * (size_t)n;
+    uint64_t st = seed;
+    if (type == 0) {
+        oracle_tracer_positions(seed, n, lx, ly, xyz);
+        return;
+    }
+    if (type == 3) {
+        for (int i = 0; i < n; ++i) {
+            x[i] = (lx * i) / (double)n;
+            y[i] = (ly * i) / (double)n;
+            z[i] = 0.0;
+        }
+        return;
+    }
+    if (type == 4) {
+        for (int i = 0; 2 * i + 1 < n; ++i) {
+            const double px = lx * u01(st), py = ly * u01(st);
+            x[2 * i] = x[2 * i + 1] = px;
+            y[2 * i] = y[2 * i + 1] = py;
+            z[2 * i] = z[2 * i + 1] = 0.0;
+        }
+        return;
+    }
+    if (type == 1 || type == 2) {
+        cx = 0.5 * lx;
+        cy = 0.5 * ly;
+        cz = 0.0;
+    }
+    if (type == 1) sigma = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double v[3] = {cx, cy, cz};
+        if (sigma > 0)
+            for (int d = 0; d < 3; ++d) {
+                const double u1 = u01(st), u2 = u01(st);
+                v[d] += sigma * (std::cos(2.0 * PI * u2) * std::sqrt(-2.0 * std::log(u1)));
+            }
+        x[i] = v[0];
+        y[i] = v[1];
+        z[i] = v[2];
     }
 }
 

@@ -30,7 +30,8 @@ class _Params(ctypes.Structure):
                 ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("ra", ctypes.c_double),
                 ("pr", ctypes.c_double), ("dt", ctypes.c_double), ("form", ctypes.c_int),
                 ("n_tracers", ctypes.c_int), ("device", ctypes.c_int), ("diag_capacity", ctypes.c_int),
-                ("tune", ctypes.c_int)]
+                ("tune", ctypes.c_int), ("tracer_diffusivity", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong),
+                ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int)]
 
 
 class _Diag(ctypes.Structure):
@@ -51,7 +52,8 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_measure_fp64_peak", "rbc_nonlinear_noalloc", "rbc_dump_read", "rbc_dump_write",
            "rbc_save_state", "rbc_load_state", "rbc_save_history", "rbc_load_history", "rbc_ensemble_create",
            "rbc_ensemble_destroy", "rbc_ensemble_member", "rbc_ensemble_step", "rbc_ensemble_last_error", "rbc_launch_config",
-           "rbc_kernel_launches"]
+           "rbc_kernel_launches", "rbc_tracers_init", "rbc_tracer_moments", "rbc_tracks_read", "rbc_track_write"]
+TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
 
 def lib():
@@ -82,6 +84,12 @@ def lib():
     L.rbc_tracers_get.argtypes = [vp, _dp, ctypes.c_int]
     L.rbc_tracers_seed.argtypes = [vp, ctypes.c_ulonglong]
     L.rbc_tracers_advance.argtypes = [vp]
+    L.rbc_tracers_init.argtypes = [vp, ctypes.c_int, ctypes.c_ulonglong] + [ctypes.c_double] * 4
+    L.rbc_tracer_moments.argtypes = [vp, _dp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    up = ctypes.POINTER(ctypes.c_uint)
+    L.rbc_tracks_read.argtypes = [vp, fp, up, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.rbc_track_write.argtypes = [ctypes.c_char_p, ctypes.c_char_p, fp, up, ctypes.c_int, ctypes.c_int]
     L.rbc_diagnostics.argtypes = [vp, ctypes.POINTER(_Diag)]
     L.rbc_diag_history.argtypes = [vp, ctypes.POINTER(_Diag), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.rbc_spectrum.argtypes = [vp, ctypes.c_double, _dp, ctypes.c_int]
@@ -159,8 +167,23 @@ def dump_write(path, arr, real_bytes=8):
         raise RBCError(st, f"rbc_dump_write({path})")
 
 
-def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False):
-    return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)))
+def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False,
+                tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1):
+    return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)),
+                   tracer_diffusivity, noise_seed, track_frames, track_period)
+
+
+def track_write(path, frames, times, description=""):
+    """Writes FP32 frames [nframes][3][n] with their step numbers as a TRKSS track file."""
+    fr = np.ascontiguousarray(frames, dtype=np.float32)
+    tm = np.ascontiguousarray(times, dtype=np.uint32)
+    nf = fr.shape[0]
+    n = fr.shape[2] if nf else 0
+    st = lib().rbc_track_write(os.fsencode(path), description.encode(),
+                               fr.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                               tm.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), nf, n)
+    if st != RBC_OK:
+        raise RBCError(st, f"rbc_track_write({path})")
 
 
 class Ensemble:
@@ -201,16 +224,18 @@ class Solver:
     """One RBC run on one GPU (mirrors the reference's operator set, see include/rbc.h)."""
 
     def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0,
-                 tune=False, _handle=None):
+                 tune=False, tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, _handle=None):
         self.nx, self.ny, self.L = nx, ny, nz
         self.mox = nx // 2 + 1
         self.n_tracers = n_tracers
+        self.track_frames = track_frames
         self.params = dict(nx=nx, ny=ny, nz=nz, lx=lx, ly=ly, ra=ra, pr=pr, dt=dt, form=form)
         self._owned = _handle is None
         if _handle is not None:
             self.h = _handle
             return
-        p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune)
+        p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune,
+                        tracer_diffusivity, noise_seed, track_frames, track_period)
         h = ctypes.c_void_p()
         st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
         if st != RBC_OK:
@@ -319,6 +344,35 @@ class Solver:
 
     def tracers_advance(self):
         self._check(lib().rbc_tracers_advance(self.h))
+
+    def tracers_init(self, pattern, seed=0, coord=(0.0, 0.0, 0.0), sigma=0.0):
+        """Start positions by pattern (random, center, center_sigma, diagonal, pairs, coord_sigma)."""
+        self._check(lib().rbc_tracers_init(self.h, TRACER_PATTERNS[pattern], seed, *coord, sigma))
+
+    def tracer_moments(self):
+        """(<x>, <y>, second moment, pair second moment) of the current positions."""
+        out = np.zeros(4)
+        self._check(lib().rbc_tracer_moments(self.h, _p(out)))
+        return out
+
+    def tracks_read(self, max_frames=1 << 30):
+        """Unread recorded frames as (FP32 [nframes][3][n], step numbers)."""
+        k = ctypes.c_int(0)
+        ring = max(1, self.track_frames)
+        cap = min(max_frames, ring)
+        frames, times = [], []
+        while True:
+            fr = np.zeros((cap, 3, self.n_tracers), np.float32)
+            tm = np.zeros(cap, np.uint32)
+            self._check(lib().rbc_tracks_read(self.h, fr.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                              tm.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), cap, ctypes.byref(k)))
+            frames.append(fr[:k.value])
+            times.append(tm[:k.value])
+            max_frames -= k.value
+            if k.value < cap or max_frames <= 0:
+                break
+            cap = min(max_frames, ring)
+        return np.concatenate(frames), np.concatenate(times)
 
     # diagnostics
     def diagnostics(self):

@@ -94,6 +94,16 @@ struct rbc_handle {
     double* zbasis = nullptr;     // [128][3][L]
     void* nv = nullptr;           // [Ny*Nx][NodeRec] node records for the tracers (R)
     bool tracer_pending = false;  // a fluid step ran whose tracer advance is not done yet
+    double tr_sigma = 0.0;        // sqrt(2 D dt) of the diffusion step
+    float* trk = nullptr;         // [trk_cap][3][ntr] recorded frames
+    int trk_cap = 0, trk_period = 1;
+    long long trk_next = 0;       // step of the oldest unread frame (a multiple of trk_period)
+    double* trsums = nullptr;     // [4] moment sums
+    // the tracer advance runs on a side stream, forked after the contraction and joined
+    // after the update, so that it overlaps the analysis FFTs and the update
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool join_pending = false;
     long long launches = 0;
     int contract_grid = 0, contract_smem = 0;
     // CUDA graphs of one steady-state (AB2) step: [0] without, [1] with the pending
@@ -320,11 +330,35 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
 }
 
 // Nonlinear operator from phys into N / NFG: K3 + K4 + K5 over the columns of G.
-template <typename R> static void run_analysis(rbc_handle* h, const Geom& G)
+static void join_tracer(rbc_handle* h)
+{
+    if (!h->join_pending) return;
+    RBC_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    h->join_pending = false;
+}
+
+// Forward x and y transforms of the contracted groups (after the contraction). With a
+// pending tracer advance the tracer kernel is forked onto the side stream right after
+// the contraction that wrote its node records; defer_join leaves the join to the caller
+// (run_step joins after the update), otherwise it is joined here.
+template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, bool defer_join = false)
 {
     typedef typename cplx_t<R>::type C;
     RBC_DISPATCH_L(launch_contract, R, G.L, h);
-    if (h->tracer_pending) launch_tracer_from_synthesis<R>(h);
+    if (h->tracer_pending) {
+        if (h->side && !h->profiling) {
+            RBC_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+            RBC_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+            cudaStream_t main_stream = h->stream;
+            h->stream = h->side;
+            launch_tracer_from_synthesis<R>(h);
+            h->stream = main_stream;
+            RBC_CUDA(cudaEventRecord(h->ev_join, h->side));
+            h->join_pending = true;
+        } else {
+            launch_tracer_from_synthesis<R>(h);
+        }
+    }
     const int rows = 13 * G.L * G.ny;
     {
     StageScope sc(h, ST_R2C);
@@ -332,10 +366,13 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G)
     RBC_CUDA(cudaGetLastError());
     }
     dim3 g5(G.ckw, G.L);
+    {
     StageScope sc(h, ST_COMBINE);
     k_columns_combine<R><<<g5, kThreads, smem_combine<R>(h), h->stream>>>(G, h->py, h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
     RBC_CUDA(cudaGetLastError());
+    }
     h->launches += 2;
+    if (!defer_join) join_tracer(h);
 }
 
 
@@ -377,7 +414,49 @@ static void tracer_setup(rbc_handle* h)
     const size_t rsz = h->mixed ? sizeof(float) : sizeof(double);
     h->nv = dalloc<unsigned char>((size_t)h->G.P * ((5 * L + 1) & ~1) * rsz, h->owned);
     RBC_CUDA(cudaMemset(h->trpos, 0, 3 * (size_t)h->ntr * sizeof(double)));
+    h->trsums = dalloc<double>(4, h->owned);
+    RBC_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    RBC_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    RBC_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    const double D = h->prm.tracer_diffusivity;
+    h->tr_sigma = D > 0 ? std::sqrt(2.0 * D * h->G.dt) : 0.0;
+    h->trk_period = h->prm.track_period > 1 ? h->prm.track_period : 1;
+    h->trk_cap = h->prm.track_frames;
+    if (h->trk_cap > 0) {
+        h->trk = dalloc<float>((size_t)h->trk_cap * 3 * h->ntr, h->owned);
+        RBC_CUDA(cudaMemset(h->trk, 0, (size_t)h->trk_cap * 3 * h->ntr * sizeof(float)));
+    }
 }
+
+// Step of the newest tracer positions: the fluid steps taken, minus a pending advance.
+static long long tracer_time(const rbc_handle* h) { return h->host_steps - (h->tracer_pending ? 1 : 0); }
+
+// Unread track frames if the tracer positions were at step `upto`.
+static long long track_frames_until(const rbc_handle* h, long long upto)
+{
+    if (upto < h->trk_next) return 0;
+    return upto / h->trk_period - h->trk_next / h->trk_period + 1;
+}
+
+// New positions were set at the current step: the track restarts there.
+static void track_reset(rbc_handle* h)
+{
+    if (!h->trk) return;
+    const long long m = h->host_steps, P = h->trk_period;
+    h->trk_next = ((m + P - 1) / P) * P;
+    if (m % P == 0) {
+        float* fr = h->trk + (size_t)((m / P) % h->trk_cap) * 3 * h->ntr;
+        k_track_frame<<<(3 * h->ntr + 255) / 256, 256, 0, h->stream>>>(h->trpos, fr, h->ntr);
+        RBC_CUDA(cudaGetLastError());
+    }
+}
+
+// Steps whose frames would overrun the ring are refused (particle_tracer.cu:145-147).
+static bool track_room(const rbc_handle* h, long long nsteps)
+{
+    return !h->trk || track_frames_until(h, h->host_steps + nsteps) <= h->trk_cap;
+}
+static const char* kTrackFull = "track ring full: read the recorded frames (rbc_tracks_read) before stepping on";
 
 template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
 {
@@ -393,6 +472,12 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.ly = h->G.ly;
     A.dt = h->G.dt;
     A.zmax = 0.5f - 1e-3;
+    A.sigma = h->tr_sigma;
+    A.noise_seed = h->prm.noise_seed;
+    A.step_counter = h->step_counter;
+    A.track = h->trk;
+    A.track_cap = h->trk_cap;
+    A.track_period = h->trk_period;
     StageScope sc(h, ST_TRACER);
     k_tracers<R, L><<<(4 * h->ntr + 127) / 128, 128, 0, h->stream>>>(A); // 4 lanes per tracer
     RBC_CUDA(cudaGetLastError());
@@ -412,9 +497,10 @@ template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h)
 template <typename R> static void run_step(rbc_handle* h)
 {
     run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
-    run_analysis<R>(h, h->G); // the contraction also writes the tracers' node records
+    run_analysis<R>(h, h->G, true); // the contraction also writes the tracers' node records
     h->tracer_pending = false;
     RBC_DISPATCH_L(launch_update, R, h->G.L, h);
+    join_tracer(h);
     h->have_hist = true;
     h->tracer_pending = h->ntr > 0;
     ++h->host_steps;
@@ -529,6 +615,11 @@ static void free_all(rbc_handle* h)
     h->owned.clear();
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     h->own_stream = nullptr;
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    h->side = nullptr;
+    h->ev_fork = h->ev_join = nullptr;
 }
 
 void rbc_destroy(rbc_handle* h)
@@ -538,6 +629,7 @@ void rbc_destroy(rbc_handle* h)
     cudaGetDevice(&cur);
     cudaSetDevice(h->prm.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->side) cudaStreamSynchronize(h->side);
     free_all(h);
     cudaSetDevice(cur);
     delete h;
@@ -558,6 +650,9 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
     *out = nullptr;
     if (!fft_len_ok(p->nx) || !fft_len_ok(p->ny)) return RBC_ERR_INVALID_ARG;
     if (!(p->lx > 0 && p->ly > 0 && p->pr > 0 && p->dt > 0) || p->n_tracers < 0) return RBC_ERR_INVALID_ARG;
+    if (!(p->tracer_diffusivity >= 0 && std::isfinite(p->tracer_diffusivity)) || p->track_frames < 0 ||
+        p->track_period < 0 || (p->track_frames > 0 && p->n_tracers == 0))
+        return RBC_ERR_INVALID_ARG;
     if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED) return RBC_ERR_INVALID_ARG;
     if (!L_supported(p->nz, p->form == RBC_FORM_MIXED)) return RBC_ERR_UNSUPPORTED;
     rbc_handle* h = new rbc_handle;
@@ -832,6 +927,7 @@ static void capture_step(rbc_handle* h, int variant)
 rbc_status rbc_step_async(rbc_handle* h, int nsteps)
 {
     if (nsteps < 0) return fail(h, RBC_ERR_INVALID_ARG, "negative step count");
+    if (h && !track_room(h, nsteps)) return fail(h, RBC_ERR_INVALID_ARG, kTrackFull);
     RBC_GUARD(h)
     h->launches = 0;
     for (int s = 0; s < nsteps; ++s) {
@@ -1220,6 +1316,7 @@ rbc_status rbc_tracers_set(rbc_handle* h, const double* xyz, int n)
     RBC_GUARD(h)
     h->tracer_pending = false;
     RBC_CUDA(cudaMemcpyAsync(h->trpos, xyz, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    track_reset(h);
     RBC_CUDA(cudaStreamSynchronize(h->stream));
     return RBC_OK;
     RBC_GUARD_END(h)
@@ -1243,6 +1340,63 @@ rbc_status rbc_tracers_seed(rbc_handle* h, unsigned long long seed)
     std::vector<double> xyz(3 * (size_t)h->ntr);
     rbchost::seeded_positions(seed, h->ntr, h->prm.lx, h->prm.ly, xyz.data());
     return rbc_tracers_set(h, xyz.data(), h->ntr);
+}
+
+rbc_status rbc_tracers_init(rbc_handle* h, int type, unsigned long long seed, double cx, double cy, double cz,
+                            double sigma)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (type < RBC_TRACERS_RANDOM || type > RBC_TRACERS_COORD_SIGMA || !(sigma >= 0))
+        return fail(h, RBC_ERR_INVALID_ARG, "unknown tracer pattern or negative sigma");
+    if (type == RBC_TRACERS_PAIRS && (h->ntr & 1))
+        return fail(h, RBC_ERR_INVALID_ARG, "position pairs need an even number of tracers");
+    std::vector<double> xyz(3 * (size_t)h->ntr);
+    rbchost::tracer_pattern(type, seed, h->ntr, h->prm.lx, h->prm.ly, cx, cy, cz, sigma, xyz.data());
+    return rbc_tracers_set(h, xyz.data(), h->ntr);
+}
+
+rbc_status rbc_tracer_moments(rbc_handle* h, double* out)
+{
+    if (!out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
+    RBC_GUARD(h)
+    if (h->ntr == 0) return fail(h, RBC_ERR_INVALID_ARG, "no tracers");
+    flush_tracers(h);
+    k_tracer_sums<<<1, 1024, 0, h->stream>>>(h->trpos, h->ntr, h->prm.lx, h->prm.ly, h->trsums);
+    RBC_CUDA(cudaGetLastError());
+    double s[4];
+    RBC_CUDA(cudaMemcpyAsync(s, h->trsums, sizeof s, cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    const double n = h->ntr;
+    out[0] = s[0] / n;
+    out[1] = s[1] / n;
+    out[2] = s[2] / n - out[0] * out[0] - out[1] * out[1];
+    out[3] = s[3] / (double)(h->ntr / 2);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_tracks_read(rbc_handle* h, float* xyz, unsigned int* times, int max_frames, int* nframes)
+{
+    if (!nframes || max_frames < 0 || (max_frames > 0 && (!xyz || !times)))
+        return fail(h, RBC_ERR_INVALID_ARG, "bad output buffers");
+    RBC_GUARD(h)
+    *nframes = 0;
+    if (!h->trk) return fail(h, RBC_ERR_INVALID_ARG, "no track ring (params.track_frames = 0)");
+    flush_tracers(h);
+    const long long avail = track_frames_until(h, tracer_time(h));
+    const int k = (int)std::min<long long>(avail, max_frames);
+    const size_t fsz = 3 * (size_t)h->ntr;
+    for (int i = 0; i < k; ++i) {
+        const long long t = h->trk_next + (long long)i * h->trk_period;
+        const float* fr = h->trk + (size_t)((t / h->trk_period) % h->trk_cap) * fsz;
+        RBC_CUDA(cudaMemcpyAsync(xyz + (size_t)i * fsz, fr, fsz * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        times[i] = (unsigned int)t;
+    }
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    h->trk_next += (long long)k * h->trk_period;
+    *nframes = k;
+    return RBC_OK;
+    RBC_GUARD_END(h)
 }
 
 rbc_status rbc_tracers_advance(rbc_handle* h)
@@ -1360,6 +1514,11 @@ rbc_status rbc_ensemble_step(rbc_ensemble* e, int nsteps)
     if (!e || nsteps < 0) return RBC_ERR_INVALID_ARG;
     if (cudaSetDevice(e->device) != cudaSuccess) return RBC_ERR_CUDA;
     e->last_error.clear();
+    for (auto* h : e->members)
+        if (!track_room(h, nsteps)) {
+            e->last_error = kTrackFull;
+            return RBC_ERR_INVALID_ARG;
+        }
     try {
         const int n = (int)e->members.size();
         int s = 0;

@@ -25,3 +25,18 @@ template <typename C, typename R> RBC_HD C cmul_is(C a, R s) { C r; r.x = -s * a
 
 // Error word written by kernels that detect a violated precondition (never traps).
 enum rbc_dev_error { RBC_DEVERR_NONE = 0, RBC_DEVERR_BOUNDS = 1, RBC_DEVERR_NAN = 2, RBC_DEVERR_TIMEOUT = 4 };
+
+// Asynchronous global -> shared copies (cp.async, sm_80+): every copy of a load phase
+// is in flight at once and no registers stage the data. Element sizes 4, 8 or 16 bytes;
+// both addresses aligned to the size. cp_async_wait_all() + __syncthreads() publishes
+// the data to the CTA.
+template <int BYTES> RBC_D void cp_async(void* smem_dst, const void* gmem_src)
+{
+    static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async copies 4, 8 or 16 bytes");
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem_src), "n"(BYTES) : "memory");
+}
+RBC_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }

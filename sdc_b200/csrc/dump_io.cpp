@@ -145,4 +145,43 @@ rbc_status rbc_dump_write(const char* path, const int* dims, int ndims, const do
     return write_container(path, {&M}, real_bytes) ? RBC_OK : RBC_ERR_IO;
 }
 
+// TRKSS track file, version 'a' (gpu_flow/code/output/track_movie.cpp:256-325): header
+// "TRKSS", 'a', uint32 tracks, uint32 frame rate (1, track_writer.cu:15), uint32 length
+// and the description, uint32 first and last frame time, uint32 frame count; then per
+// frame uint32 time and x, y, z float32 per track.
+rbc_status rbc_track_write(const char* path, const char* description, const float* xyz, const unsigned int* times,
+                           int nframes, int n)
+{
+    if (!path || nframes < 0 || n < 0 || (nframes > 0 && (!xyz || !times))) return RBC_ERR_INVALID_ARG;
+    const std::string desc = description ? description : "";
+    std::vector<unsigned char> out;
+    auto put = [&out](const void* p, size_t k) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        out.insert(out.end(), b, b + k);
+    };
+    auto put32 = [&put](uint32_t v) { put(&v, 4); };
+    put("TRKSS", 5);
+    put("a", 1);
+    put32((uint32_t)n);
+    put32(1u);
+    put32((uint32_t)desc.size());
+    put(desc.data(), desc.size());
+    put32(nframes > 0 ? times[0] : 0u);
+    put32(nframes > 0 ? times[nframes - 1] : 0u);
+    put32((uint32_t)nframes);
+    for (int f = 0; f < nframes; ++f) {
+        put32(times[f]);
+        const float* fx = xyz + (size_t)f * 3 * n;
+        for (int j = 0; j < n; ++j) {
+            put(fx + j, 4);
+            put(fx + n + j, 4);
+            put(fx + 2 * (size_t)n + j, 4);
+        }
+    }
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return RBC_ERR_IO;
+    const bool ok = std::fwrite(out.data(), 1, out.size(), fp) == out.size();
+    return (std::fclose(fp) == 0 && ok) ? RBC_OK : RBC_ERR_IO;
+}
+
 } // extern "C"

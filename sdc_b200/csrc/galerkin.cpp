@@ -414,4 +414,53 @@ void seeded_positions(uint64_t seed, int n, double lx, double ly, double* xyz)
     }
 }
 
+// particle_tracer.cu:58-137 (patterns) and 376-450 (device initialisers); the reference's
+// cuRAND draws are replaced by the SplitMix64 stream of `seed`.
+void tracer_pattern(int type, uint64_t seed, int n, double lx, double ly, double cx, double cy, double cz,
+                    double sigma, double* xyz)
+{
+    double* x = xyz;
+    double* y = xyz + n;
+    double* z = xyz + 2 * (size_t)n;
+    uint64_t s = seed;
+    auto normal = [&s]() {
+        const double u1 = unit_open(s), u2 = unit_open(s);
+        return std::cos(2.0 * kPi * u2) * std::sqrt(-2.0 * std::log(u1));
+    };
+    switch (type) {
+    case 0: // random
+        seeded_positions(seed, n, lx, ly, xyz);
+        return;
+    case 3: // diagonal
+        for (int i = 0; i < n; ++i) {
+            x[i] = (lx * i) / (double)n;
+            y[i] = (ly * i) / (double)n;
+            z[i] = 0.0;
+        }
+        return;
+    case 4: // pairs
+        for (int i = 0; i + 1 < n; i += 2) {
+            const double px = lx * unit_open(s), py = ly * unit_open(s);
+            x[i] = x[i + 1] = px;
+            y[i] = y[i + 1] = py;
+            z[i] = z[i + 1] = 0.0;
+        }
+        return;
+    default: break;
+    }
+    // center, center_sigma, coord_sigma: a point, then sigma N(0,1) per coordinate
+    if (type == 1 || type == 2) { cx = 0.5 * lx; cy = 0.5 * ly; cz = 0.0; }
+    if (type == 1) sigma = 0.0;
+    for (int i = 0; i < n; ++i) {
+        x[i] = cx;
+        y[i] = cy;
+        z[i] = cz;
+        if (sigma > 0.0) {
+            x[i] += sigma * normal();
+            y[i] += sigma * normal();
+            z[i] += sigma * normal();
+        }
+    }
+}
+
 } // namespace rbchost

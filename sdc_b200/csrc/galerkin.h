@@ -53,5 +53,8 @@ void build_operator_tables(const GridInfo& g, const Tables& T, OperatorTables& o
 // (interleaved complex), followed by the Hermitian fix on the kx = 0 column.
 void seeded_theta(const GridInfo& g, uint64_t seed, double amp, double kmax, double* theta);
 void seeded_positions(uint64_t seed, int n, double lx, double ly, double* xyz);
+// Tracer start patterns of particle_tracer::init_positions (rbc_tracer_init types).
+void tracer_pattern(int type, uint64_t seed, int n, double lx, double ly, double cx, double cy, double cz,
+                    double sigma, double* xyz);
 
 } // namespace rbchost

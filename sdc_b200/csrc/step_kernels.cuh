@@ -85,13 +85,35 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns(
     const int st = py.stride;
     load_twiddles<R>(tw, twy, G.ny);
     const size_t base = ((size_t)k * G.ckp + c0) * G.ny;
+    constexpr bool kStage = sizeof(C) == sizeof(double2);
+    if constexpr (kStage) {
+        // FP64: theta, f and g land in the slots of fields 5, 0 and 3 of their own
+        // (column, row); the same thread reads them back below, so no barrier is needed.
+        for (int e = threadIdx.x; e < W * G.ny; e += blockDim.x) {
+            const int cc = e / G.ny, r = e - cc * G.ny, c = c0 + cc;
+            if (c < G.ckeep && row_kept(r, G.ny)) {
+                cp_async<16>(buf + (5 * W + cc) * st + rbcfft::pad(r), th + base + e);
+                cp_async<16>(buf + (0 * W + cc) * st + rbcfft::pad(r), f + base + e);
+                cp_async<16>(buf + (3 * W + cc) * st + rbcfft::pad(r), g + base + e);
+            }
+        }
+        cp_async_wait_all();
+    }
     for (int e = threadIdx.x; e < W * G.ny; e += blockDim.x) {
         const int cc = e / G.ny, r = e - cc * G.ny, c = c0 + cc;
         double2 vt = make_double2(0, 0), vf = vt, vg = vt;
         if (c < G.ckeep && row_kept(r, G.ny)) {
-            vt = th[base + e];
-            vf = f[base + e];
-            vg = g[base + e];
+            if constexpr (kStage) {
+                const C a = buf[(5 * W + cc) * st + rbcfft::pad(r)], b = buf[(0 * W + cc) * st + rbcfft::pad(r)],
+                        d = buf[(3 * W + cc) * st + rbcfft::pad(r)];
+                vt = make_double2(a.x, a.y);
+                vf = make_double2(b.x, b.y);
+                vg = make_double2(d.x, d.y);
+            } else {
+                vt = th[base + e];
+                vf = f[base + e];
+                vg = g[base + e];
+            }
         }
         const Mult m(c, r, G);
         double2 u12 = cmul_is<double2, double>(vg, m.fy);
@@ -134,20 +156,32 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r(
     const int nx = G.nx, st = px.stride;
     const int row0 = 2 * NP * blockIdx.x;           // first row (plane * Ny + y)
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
+    // A[n] lands at n and B[n] at nx - n, where the Hermitian extension puts its values;
+    // B[0] goes to the spare last slot of the padded row (st - 1 > pad(nx - 1)).
+    const C* src = H + (size_t)plane * G.ckp * G.ny + y0;
+    for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
+        const int n = e / NP, pp = e - n * NP;
+        C* row = buf + pp * st;
+        cp_async<sizeof(C)>(row + rbcfft::pad(n), src + (size_t)n * G.ny + 2 * pp);
+        cp_async<sizeof(C)>(row + (n ? rbcfft::pad(nx - n) : st - 1), src + (size_t)n * G.ny + 2 * pp + 1);
+    }
     for (int e = threadIdx.x; e < NP * nx; e += blockDim.x) {
         const int pp = e / nx, n = e - pp * nx;
         if (n >= G.ckeep && n <= nx - G.ckeep) buf[pp * st + rbcfft::pad(n)] = cmk<C>(0, 0);
     }
-    const C* src = H + (size_t)plane * G.ckp * G.ny + y0;
+    cp_async_wait_all();
+    __syncthreads();
     for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
         const int n = e / NP, pp = e - n * NP;
-        C A = src[(size_t)n * G.ny + 2 * pp], B = src[(size_t)n * G.ny + 2 * pp + 1];
+        C* row = buf + pp * st;
+        C* pb = row + (n ? rbcfft::pad(nx - n) : st - 1);
+        C A = row[rbcfft::pad(n)], B = *pb;
         if (n == 0) { A.y = 0; B.y = 0; }
         C z; z.x = A.x - B.y; z.y = A.y + B.x;       // A + iB
-        buf[pp * st + rbcfft::pad(n)] = z;
+        row[rbcfft::pad(n)] = z;
         if (n > 0) {
             C zm; zm.x = A.x + B.y; zm.y = B.x - A.y; // conj(A) + i conj(B)
-            buf[pp * st + rbcfft::pad(nx - n)] = zm;
+            *pb = zm;
         }
     }
     __syncthreads();
@@ -181,8 +215,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c(
     const R* src = grp + (size_t)row0 * nx;
     for (int e = threadIdx.x; e < NP * nx; e += blockDim.x) {
         const int pp = e / nx, x = e - pp * nx;
-        buf[pp * st + rbcfft::pad(x)] = cmk<C>(src[(size_t)(2 * pp) * nx + x], src[(size_t)(2 * pp + 1) * nx + x]);
+        R* d = reinterpret_cast<R*>(buf + pp * st + rbcfft::pad(x));
+        cp_async<sizeof(R)>(d, src + (size_t)(2 * pp) * nx + x);
+        cp_async<sizeof(R)>(d + 1, src + (size_t)(2 * pp + 1) * nx + x);
     }
+    cp_async_wait_all();
     __syncthreads();
     fft_batched<R>(buf, px, NP, tw, -1);
     const R half = (R)0.5;
@@ -226,8 +263,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
     const C* src = gh + ((size_t)k * G.ckp + c) * ny;
     for (int e = threadIdx.x; e < 13 * ny; e += blockDim.x) {
         const int grpi = e / ny, r = e - grpi * ny;
-        buf[grpi * py.stride + rbcfft::pad(r)] = src[grpi * cstride + r];
+        cp_async<sizeof(C)>(buf + grpi * py.stride + rbcfft::pad(r), src + grpi * cstride + r);
     }
+    cp_async_wait_all();
     __syncthreads();
     fft_batched<R>(buf, py, 13, tw, -1);
     const double invP = 1.0 / ((double)G.nx * ny);

@@ -13,6 +13,7 @@
 //   w = sum_i C_i(z_l) u31_i.
 #pragma once
 #include "common.cuh"
+#include "splitmix.h"
 
 namespace rbck {
 
@@ -24,6 +25,11 @@ struct TracerArgs {
     double* pos;          // [3][n] x, y, z
     int n, nx, ny, L;
     double lx, ly, dt, zmax;
+    double sigma;                     // sqrt(2 D dt) of the diffusion step (0: none)
+    unsigned long long noise_seed;
+    const long long* step_counter;    // completed fluid steps = step m of the new positions
+    float* track;                     // [track_cap][3][n] FP32 frames, or null
+    int track_cap, track_period;
 };
 
 template <int L> struct NodeRecLen { static constexpr int value = (5 * L + 1) & ~1; };
@@ -141,14 +147,66 @@ __global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
     x += (dx1 + 2 * (dx2 + dx3) + dx4) / 6.;
     y += (dy1 + 2 * (dy2 + dy3) + dy4) / 6.;
     z += (dz1 + 2 * (dz2 + dz3) + dz4) / 6.;
+    if (!(live && q == 0)) return;
+    const long long m = *A.step_counter;
+    if (A.sigma > 0.0) {
+        // diffuse_particles (particle_tracer.cu:690-716) before the lid reflection
+        x += A.sigma * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 0);
+        y += A.sigma * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 1);
+        z += A.sigma * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 2);
+    }
     const double zm = A.zmax;
     if (!(z <= zm)) z = (z < 2 * zm) ? 2 * zm - z : zm;  // also sends NaN to the lid
     else if (z < -zm) z = (z > -2 * zm) ? -2 * zm - z : -zm;
-    if (live && q == 0) {
-        A.pos[t] = x;
-        A.pos[A.n + t] = y;
-        A.pos[2 * A.n + t] = z;
+    A.pos[t] = x;
+    A.pos[A.n + t] = y;
+    A.pos[2 * A.n + t] = z;
+    if (A.track && m % A.track_period == 0) {
+        float* fr = A.track + (size_t)((m / A.track_period) % A.track_cap) * 3 * A.n;
+        fr[t] = (float)x;
+        fr[A.n + t] = (float)y;
+        fr[2 * A.n + t] = (float)z;
     }
+}
+
+// Copies positions into one FP32 track frame (the frame of freshly set positions).
+__global__ void k_track_frame(const double* __restrict__ pos, float* __restrict__ frame, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x)
+        frame[i] = (float)pos[i];
+}
+
+// Sums for the tracer moments in FP64, one CTA of 1024 threads: thread i sums particles
+// i, i + 1024, ... (and pairs likewise), then a fixed shared-memory tree; deterministic.
+// out[0..3] = sum x, sum y, sum x^2 + y^2, sum over pairs of the squared periodic separation.
+__global__ void __launch_bounds__(1024) k_tracer_sums(const double* __restrict__ pos, int n, double lx, double ly,
+                                                      double* __restrict__ out)
+{
+    __shared__ double red[4][1024];
+    double sx = 0, sy = 0, s2 = 0, sp = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = pos[i], y = pos[n + i];
+        sx += x;
+        sy += y;
+        s2 += x * x + y * y;
+    }
+    for (int i = 2 * threadIdx.x; i < n - 1; i += 2 * blockDim.x) {
+        double dx = fabs(pos[i + 1] - pos[i]), dy = fabs(pos[n + i + 1] - pos[n + i]);
+        if (dx > 0.5 * lx) dx = lx - dx;
+        if (dy > 0.5 * ly) dy = ly - dy;
+        sp += dx * dx + dy * dy;
+    }
+    red[0][threadIdx.x] = sx;
+    red[1][threadIdx.x] = sy;
+    red[2][threadIdx.x] = s2;
+    red[3][threadIdx.x] = sp;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[threadIdx.x] = red[threadIdx.x][0];
 }
 
 } // namespace rbck

@@ -211,26 +211,34 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
         wsum += __shfl_down_sync(0xffffffffu, wsum, s);
     }
     __shared__ double red[2][kThreads / 32];
-    __shared__ bool last;
     if (lane == 0) { red[0][wid] = esum; red[1][wid] = wsum; }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (wid != 0) return; // warp 0 publishes the block partial and, in the last block, reduces
+    bool last = false;
+    if (lane == 0) {
         double a = 0, b = 0;
         for (int w = 0; w < (int)(blockDim.x / 32); ++w) { a += red[0][w]; b += red[1][w]; }
         A.partial[2 * blockIdx.x] = a;
         A.partial[2 * blockIdx.x + 1] = b;
         __threadfence();
-        const unsigned int t = atomicAdd(A.ticket, 1u);
-        last = (t == gridDim.x - 1);
+        last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
     }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        double a = 0, b = 0;
-        for (int i = 0; i < (int)gridDim.x; ++i) {
-            a += ((volatile double*)A.partial)[2 * i];
-            b += ((volatile double*)A.partial)[2 * i + 1];
-        }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    // fixed partition (lane l sums blocks l, l + 32, ...) and a fixed shuffle tree:
+    // the result does not depend on the order in which blocks finished
+    double a = 0, b = 0;
+    for (int i = lane; i < (int)gridDim.x; i += 32) {
+        a += ((volatile double*)A.partial)[2 * i];
+        b += ((volatile double*)A.partial)[2 * i + 1];
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, s);
+        b += __shfl_down_sync(0xffffffffu, b, s);
+    }
+    if (lane == 0) {
         double nuw = 1.0;
         for (int kk = 0; kk < L; ++kk) nuw -= (kk + 1) * kPi * ((volatile double*)A.th00)[kk];
         const long long s = *A.step_counter + 1;
