@@ -98,6 +98,31 @@ rbc_status rbc_set_stream(rbc_handle* h, void* stream);
  * matrix_device_init::init_random (gpu_flow/code/util/init.cu:9-20) and main.cu:300-396.
  * The next step is an Euler step. */
 rbc_status rbc_init_fields(rbc_handle* h, unsigned long long seed, double amplitude, double kmax);
+/* Pattern initial conditions of matrix_device_init (gpu_flow/code/util/init.cu:22-310),
+ * selected in the reference by main.cu's -init_* options (main.cu:88-98, 326-352). The
+ * pattern is evaluated in FP64 on the Nx x Ny grid of the unit square and its unnormalised
+ * R2C transform becomes theta's lowest vertical mode; every other entry of theta gets
+ * uniform noise in [-noise, noise) (the reference's init_random left its +-1e-6 noise
+ * there); f = g = F = G = 0; then the Hermitian fix. `mode` is the reference's -init_mode
+ * (default Lx/2), truncated to an integer as its int parameters do; `amplitude` is
+ * max_amplitude (1e-6 in the reference).
+ *   ISR          amp cos(2 pi (mode x) + phase), phase uniform in [0, 2 pi)
+ *   DISLOCATION  amp cos(2 pi mode x - phi_1 + phi_2), defects at (1/2, 1/4), (1/2, 3/4)
+ *   RECTANGLE    amp cos(2 pi x_m x) with x_m = (Lx / (Nx - 1)) (Nx - 5) / 2, and a strip
+ *                x < 1/8 of uniform noise in [-amp, amp)
+ *   SV           amp cos(2 pi (mode y + phase(x, y))), x_frac 0.2
+ *   CR           amp cos(2 pi mode y - phi_1 + phi_2), x_frac 0.8
+ *   GIANTSPIRAL  amp cos(2 pi mode r - phi_1 + phi_2), centre (1/2, 1/2), defect (0.8, 1/2)
+ *   TEST         init_test: theta and f = amp sin(c) on row 0, columns c > 0, every mode;
+ *                F_k = amp cos(k); no noise
+ * The random draws (isr phase, rectangle strip, noise) come from the SplitMix64 stream of
+ * `seed` in that order. The next step is an Euler step. */
+typedef enum {
+    RBC_INIT_ISR = 1, RBC_INIT_DISLOCATION = 2, RBC_INIT_RECTANGLE = 3, RBC_INIT_SV = 4,
+    RBC_INIT_CR = 5, RBC_INIT_GIANTSPIRAL = 6, RBC_INIT_TEST = 7
+} rbc_init_pattern_type;
+rbc_status rbc_init_pattern(rbc_handle* h, int pattern, double mode, double amplitude, unsigned long long seed,
+                            double noise);
 /* Upload / download the state (host buffers, reference layout). rbc_set_state applies
  * the 2/3 dealiasing of the reference's first dealias_data call and resets the AB2
  * history, as a restart from dump files does (main.cu:290-385,

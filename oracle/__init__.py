@@ -69,6 +69,9 @@ def lib():
         L.oracle_init_theta.restype = None
         L.oracle_tracer_positions.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp]
         L.oracle_tracer_positions.restype = None
+        L.oracle_init_pattern.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_uint64, ctypes.c_double]
+        L.oracle_init_pattern.restype = None
         L.oracle_set_diffusion.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_uint64]
         L.oracle_set_diffusion.restype = None
         L.oracle_tracer_pattern.argtypes = ([ctypes.c_int, ctypes.c_uint64, ctypes.c_int] + [ctypes.c_double] * 6 +
@@ -234,6 +237,10 @@ class Oracle:
 
     def tracers_advance(self):
         lib().oracle_tracers_advance(self.h)
+
+    def init_pattern(self, kind, mode, amp=1e-6, seed=0, noise=0.0):
+        """Pattern initial condition (1 isr ... 6 giantspiral, 7 test), see oracle_init_pattern."""
+        lib().oracle_init_pattern(self.h, kind, mode, amp, seed, noise)
 
     def set_diffusion(self, D, seed):
         lib().oracle_set_diffusion(self.h, D, seed)

@@ -1412,6 +1412,91 @@ void oracle_tracer_positions(uint64_t seed, int n, double lx, double ly, double*
     }
 }
 
+// Pattern initial conditions of matrix_device_init (gpu_flow/code/util/init.cu:22-310)
+// as main.cu:326-352 applies them: the real-space pattern (FP64, unit square, Nx x Ny
+// points) is R2C-transformed without normalisation into theta's mode 0, the other theta
+// entries get uniform noise (the reference's init_random), f = g = F = G = 0, then
+// make_real. The reference's int mode parameters truncate `mode`; rectangle takes
+// x_mode = (int)((Lx/(Nx-1)) (Nx-5)/2) (main.cu:330); sv and cr use x_frac 0.2 and 0.8.
+// rand() is replaced by SplitMix64 draws in the order: isr phase, rectangle strip, noise.
+// Type 7 is init_test (init.cu:250-310).
+void oracle_init_pattern(oracle_handle* h, int type, double mode, double amp, uint64_t seed, double noise)
+{
+    Solver& s = h->s;
+    const int nx = s.p.nx, ny = s.p.ny, mox = s.mox;
+    std::fill(s.th.begin(), s.th.end(), cd(0));
+    std::fill(s.f.begin(), s.f.end(), cd(0));
+    std::fill(s.g.begin(), s.g.end(), cd(0));
+    std::fill(s.F.begin(), s.F.end(), cd(0));
+    std::fill(s.G.begin(), s.G.end(), cd(0));
+    uint64_t st = seed;
+    if (type == 7) {
+        for (int k = 0; k < s.p.L; ++k) {
+            for (int c = 1; c < mox; ++c) {
+                s.th[s.sidx(c, 0, k)] = cd(amp * std::sin((double)c), 0.0);
+                s.f[s.sidx(c, 0, k)] = cd(amp * std::sin((double)c), 0.0);
+            }
+            s.F[k] = cd(amp * std::cos((double)k), 0.0);
+        }
+    } else {
+        const int m = (int)mode;
+        std::vector<double> T((size_t)nx * ny);
+        double phase = 0.0;
+        if (type == 1) phase = 2 * PI * u01(st);
+        const int xm_rect = (int)((s.p.lx / (nx - 1.0)) * (nx - 5.0) / 2.0);
+        for (int j = 0; j < ny; ++j) {
+            for (int i = 0; i < nx; ++i) {
+                const double X = (double)i / nx, Y = (double)j / ny;  // grid point in the unit square
+                double v = 0.0;
+                if (type == 1) {
+                    v = amp * std::cos(2.0 * PI * (i * (double(m) / nx) + j * (0.0 / ny)) + phase);
+                } else if (type == 2) {
+                    const double h1x = (nx / 2.0) / nx + 0.5 / nx, h1y = (ny / 4.0) / ny + 0.5 / ny;
+                    const double h2x = h1x, h2y = (3.0 * ny / 4.0) / ny + 0.5 / ny;
+                    const double xx = i * (1.0 / nx), yy = j * (1.0 / ny);
+                    v = amp * std::cos(m * 2.0 * PI * xx + 0 * 2.0 * PI * yy - std::atan2(yy - h1y, xx - h1x) +
+                                       std::atan2(yy - h2y, xx - h2x));
+                } else if (type == 3) {
+                    if (i < nx / 8) v = (2.0 * u01(st) - 1.0) * amp;
+                    else v = amp * std::cos(2.0 * PI * (i * (double(xm_rect) / nx) + j * 0.0));
+                } else if (type == 4) {
+                    const double xf = 0.2, lo = 0.5 * (1.0 - xf), hi = 1.0 - lo;
+                    double ph = -0.5 * std::sin(2 * PI * Y) - X * X;
+                    if (X > hi) ph += 1.0;
+                    else if (X > lo) ph += 0.5 * (1.0 - std::cos(PI * (X - lo) / xf));
+                    v = amp * std::cos(2.0 * PI * (j * (double(m) / ny) + ph));
+                } else if (type == 5) {
+                    const double xf = 0.8;
+                    const double c1x = 0.5 * ((1.0 - xf) * nx + 1) * (1.0 / nx), c2x = 1.0 - c1x;
+                    const double cy = 0.5 * (ny + 1) * (1.0 / ny);
+                    const double xx = i * (1.0 / nx), yy = j * (1.0 / ny);
+                    v = amp * std::cos(m * 2.0 * PI * yy - std::atan2(yy - cy, xx - c1x) + std::atan2(yy - cy, xx - c2x));
+                } else if (type == 6) {
+                    const double xx = i * (1.0 / nx), yy = j * (1.0 / ny);
+                    const double rr = std::sqrt((xx - 0.5) * (xx - 0.5) + (yy - 0.5) * (yy - 0.5));
+                    v = amp * std::cos(2.0 * PI * m * rr - std::atan2(yy - 0.5, xx - 0.5) + std::atan2(yy - 0.5, xx - 0.8));
+                }
+                T[(size_t)j * nx + i] = v;
+            }
+        }
+        std::vector<cd> plane((size_t)ny * mox);
+        s.fft.r2c(T.data(), plane.data());
+        for (int r = 0; r < ny; ++r)
+            for (int c = 0; c < mox; ++c) s.th[s.sidx(c, r, 0)] = plane[(size_t)r * mox + c];
+        if (noise > 0)
+            for (int k = 1; k < s.p.L; ++k)
+                for (int r = 0; r < ny; ++r)
+                    for (int c = 0; c < mox; ++c) {
+                        const double re = noise * (2.0 * u01(st) - 1.0);
+                        const double im = noise * (2.0 * u01(st) - 1.0);
+                        s.th[s.sidx(c, r, k)] = cd(re, im);
+                    }
+    }
+    s.make_real(s.th);
+    s.make_real(s.f);
+    s.have_hist = false;
+}
+
 // Start patterns of particle_tracer::init_positions (particle_tracer.cu:58-137, 376-450)
 // with SplitMix64 draws in place of cuRAND: 0 random, 1 center, 2 center_sigma,
 // 3 diagonal, 4 pairs, 5 coord_sigma.

@@ -52,7 +52,9 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_measure_fp64_peak", "rbc_nonlinear_noalloc", "rbc_dump_read", "rbc_dump_write",
            "rbc_save_state", "rbc_load_state", "rbc_save_history", "rbc_load_history", "rbc_ensemble_create",
            "rbc_ensemble_destroy", "rbc_ensemble_member", "rbc_ensemble_step", "rbc_ensemble_last_error", "rbc_launch_config",
-           "rbc_kernel_launches", "rbc_tracers_init", "rbc_tracer_moments", "rbc_tracks_read", "rbc_track_write"]
+           "rbc_kernel_launches", "rbc_tracers_init", "rbc_tracer_moments", "rbc_tracks_read", "rbc_track_write",
+           "rbc_init_pattern"]
+INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
 TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
 
@@ -84,6 +86,8 @@ def lib():
     L.rbc_tracers_get.argtypes = [vp, _dp, ctypes.c_int]
     L.rbc_tracers_seed.argtypes = [vp, ctypes.c_ulonglong]
     L.rbc_tracers_advance.argtypes = [vp]
+    L.rbc_init_pattern.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong,
+                                   ctypes.c_double]
     L.rbc_tracers_init.argtypes = [vp, ctypes.c_int, ctypes.c_ulonglong] + [ctypes.c_double] * 4
     L.rbc_tracer_moments.argtypes = [vp, _dp]
     fp = ctypes.POINTER(ctypes.c_float)
@@ -266,6 +270,13 @@ class Solver:
     # fields
     def init_fields(self, seed, amplitude=1e-3, kmax=4.0):
         self._check(lib().rbc_init_fields(self.h, seed, amplitude, kmax))
+
+    def init_pattern(self, pattern, mode=None, amplitude=1e-6, seed=0, noise=0.0):
+        """Pattern initial condition of the reference (-init_isr, -init_sv, ...); mode defaults
+        to Lx/2 as main.cu's -init_mode does."""
+        if mode is None:
+            mode = self.params["lx"] / 2.0
+        self._check(lib().rbc_init_pattern(self.h, INIT_PATTERNS[pattern], mode, amplitude, seed, noise))
 
     def set_state(self, theta, f, g, F, G):
         a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (theta, f, g, F, G)]

@@ -295,17 +295,27 @@ static bool L_supported(int L, bool mixed)
     return L == 2 || L == 3 || L == 4 || L == 5 || L == 6 || L == 8 || L == 12;
 }
 
+// Radix of the two-pass register FFT for the x and y lengths (0: Stockham passes).
+static int rx_x(const rbc_handle* h) { return rbcfft::two_pass_radix(h->G.nx); }
+static int rx_y(const rbc_handle* h) { return rbcfft::two_pass_radix(h->G.ny); }
+
 template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
 {
-    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + (size_t)nfield * h->W * h->py.stride);
+    const size_t c = sizeof(typename cplx_t<R>::type);
+    if (const int rx = rx_y(h))
+        return c * ((size_t)h->G.ny + (size_t)nfield * h->W * tp_stride(h->G.ny, rx)) +
+               sizeof(double2) * 3 * (size_t)h->W * h->G.ny;
+    return c * ((size_t)h->G.ny + (size_t)nfield * h->W * h->py.stride);
 }
 template <typename R> static size_t smem_combine(const rbc_handle* h)
 {
-    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + 13 * (size_t)h->py.stride);
+    const int rx = rx_y(h);
+    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + 13 * (size_t)(rx ? tp_stride(h->G.ny, rx) : h->py.stride));
 }
 template <typename R> static size_t smem_rows(const rbc_handle* h)
 {
-    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.nx + (size_t)h->NP * h->px.stride);
+    const int rx = rx_x(h);
+    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.nx + (size_t)h->NP * (rx ? tp_stride(h->G.nx, rx) : h->px.stride));
 }
 
 template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h);
@@ -319,12 +329,23 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     dim3 g1(G.ckw / h->W, G.L);
     {
     StageScope sc(h, ST_SYNTH);
-    k_synth_columns<R><<<g1, kThreads, smem_cols<R>(h, 8), h->stream>>>(G, h->W, h->py, h->twy, th, f, g, FG, (C*)h->H);
+    const size_t sm = smem_cols<R>(h, 8);
+    switch (rx_y(h)) {
+    case 16: k_synth_columns_tp<R, 16><<<g1, 8 * h->W * 16, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H); break;
+    case 8: k_synth_columns_tp<R, 8><<<g1, 8 * h->W * 8, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H); break;
+    default: k_synth_columns<R><<<g1, kThreads, sm, h->stream>>>(G, h->W, h->py, h->twy, th, f, g, FG, (C*)h->H);
+    }
     RBC_CUDA(cudaGetLastError());
     }
     const int rows = 8 * G.L * G.ny;
     StageScope sc(h, ST_C2R);
-    k_rows_c2r<R><<<rows / (2 * h->NP), kThreads, smem_rows<R>(h), h->stream>>>(G, h->NP, h->px, h->twx, (const C*)h->H, (R*)h->phys);
+    const int nb = rows / (2 * h->NP);
+    const size_t sm = smem_rows<R>(h);
+    switch (rx_x(h)) {
+    case 16: k_rows_c2r_tp<R, 16><<<nb, h->NP * 16, sm, h->stream>>>(G, h->NP, h->twx, (const C*)h->H, (R*)h->phys); break;
+    case 8: k_rows_c2r_tp<R, 8><<<nb, h->NP * 8, sm, h->stream>>>(G, h->NP, h->twx, (const C*)h->H, (R*)h->phys); break;
+    default: k_rows_c2r<R><<<nb, kThreads, sm, h->stream>>>(G, h->NP, h->px, h->twx, (const C*)h->H, (R*)h->phys);
+    }
     RBC_CUDA(cudaGetLastError());
     h->launches += 2;
 }
@@ -362,13 +383,24 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     const int rows = 13 * G.L * G.ny;
     {
     StageScope sc(h, ST_R2C);
-    k_rows_r2c<R><<<rows / (2 * h->NP), kThreads, smem_rows<R>(h), h->stream>>>(G, h->NP, h->px, h->twx, (const R*)h->grp, (C*)h->gh);
+    const int nb = rows / (2 * h->NP);
+    const size_t sm = smem_rows<R>(h);
+    switch (rx_x(h)) {
+    case 16: k_rows_r2c_tp<R, 16><<<nb, h->NP * 16, sm, h->stream>>>(G, h->NP, h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 8: k_rows_r2c_tp<R, 8><<<nb, h->NP * 8, sm, h->stream>>>(G, h->NP, h->twx, (const R*)h->grp, (C*)h->gh); break;
+    default: k_rows_r2c<R><<<nb, kThreads, sm, h->stream>>>(G, h->NP, h->px, h->twx, (const R*)h->grp, (C*)h->gh);
+    }
     RBC_CUDA(cudaGetLastError());
     }
     dim3 g5(G.ckw, G.L);
     {
     StageScope sc(h, ST_COMBINE);
-    k_columns_combine<R><<<g5, kThreads, smem_combine<R>(h), h->stream>>>(G, h->py, h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
+    const size_t sm = smem_combine<R>(h);
+    switch (rx_y(h)) {
+    case 16: k_columns_combine_tp<R, 16><<<g5, 13 * 16, sm, h->stream>>>(G, h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    case 8: k_columns_combine_tp<R, 8><<<g5, 13 * 8, sm, h->stream>>>(G, h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    default: k_columns_combine<R><<<g5, kThreads, sm, h->stream>>>(G, h->py, h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
+    }
     RBC_CUDA(cudaGetLastError());
     }
     h->launches += 2;
@@ -534,6 +566,14 @@ template <typename R> static void set_attributes(rbc_handle* h)
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
 }
 
 // ------------------------------------------------------------------ autotuner
@@ -550,14 +590,26 @@ static void autotune(rbc_handle* h)
     cudaEvent_t a, b;
     RBC_CUDA(cudaEventCreate(&a));
     RBC_CUDA(cudaEventCreate(&b));
+    int dev = 0, optin = 0;
+    RBC_CUDA(cudaGetDevice(&dev));
+    RBC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    (void)csz;
     for (int W = 1; W <= 4; W *= 2) {
         if (8 * W > h->py.chunk && W > 1) continue;
-        if (csz * ((size_t)G.ny + 8 * (size_t)W * h->py.stride) > 200 * 1024) continue;
+        if (rx_y(h) && 8 * W * rx_y(h) > kThreads) continue;
         for (int NP = 1; NP <= 32 && NP <= h->px.chunk; ++NP) {
             if ((G.ny / 2) % NP) continue;
-            if (csz * ((size_t)G.nx + (size_t)NP * h->px.stride) > 200 * 1024) continue;
+            if (rx_x(h) && NP * rx_x(h) > kThreads) continue;
+            const int W0 = h->W, NP0 = h->NP;
             h->W = W;
             h->NP = NP;
+            const size_t need = mixed ? std::max({smem_cols<float>(h, 8), smem_combine<float>(h), smem_rows<float>(h)})
+                                      : std::max({smem_cols<double>(h, 8), smem_combine<double>(h), smem_rows<double>(h)});
+            if (need > (size_t)optin) {
+                h->W = W0;
+                h->NP = NP0;
+                continue;
+            }
             G.ckw = ((G.ckeep + W - 1) / W) * W;
             if (mixed) set_attributes<float>(h);
             else set_attributes<double>(h);
@@ -877,6 +929,20 @@ rbc_status rbc_init_fields(rbc_handle* h, unsigned long long seed, double amplit
     std::vector<double> th(2 * n), zero(2 * n, 0.0), fg(2 * L, 0.0);
     rbchost::seeded_theta(h->gi, seed, amplitude, kmax, th.data());
     return rbc_set_state(h, th.data(), zero.data(), zero.data(), fg.data(), fg.data());
+}
+
+rbc_status rbc_init_pattern(rbc_handle* h, int pattern, double mode, double amplitude, unsigned long long seed,
+                            double noise)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (pattern < RBC_INIT_ISR || pattern > RBC_INIT_TEST || !std::isfinite(mode) || !std::isfinite(amplitude) ||
+        !(noise >= 0))
+        return fail(h, RBC_ERR_INVALID_ARG, "unknown pattern or bad amplitude");
+    const int L = h->G.L;
+    const size_t n = (size_t)h->G.ny * h->G.mox * L;
+    std::vector<double> th(2 * n), f(2 * n, 0.0), g(2 * n, 0.0), F(2 * L, 0.0), G(2 * L, 0.0);
+    rbchost::pattern_theta(h->gi, pattern, mode, amplitude, seed, noise, th.data(), f.data(), F.data());
+    return rbc_set_state(h, th.data(), f.data(), g.data(), F.data(), G.data());
 }
 
 static rbc_status check_err(rbc_handle* h)

@@ -11,6 +11,7 @@
 #include "contract_prog.h"
 
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <map>
 #include <algorithm>
@@ -461,6 +462,183 @@ void tracer_pattern(int type, uint64_t seed, int n, double lx, double ly, double
             z[i] += sigma * normal();
         }
     }
+}
+
+// ------------------------------------------------------------------ pattern init
+typedef std::complex<double> cplx;
+
+// Recursive mixed-radix (2, 3) DFT, y[k] = sum_j x[j s] exp(-2 pi i j k / n); twiddles
+// from long double.
+static void dft23(const cplx* x, int s, int n, cplx* y)
+{
+    if (n == 1) {
+        y[0] = x[0];
+        return;
+    }
+    const int r = (n % 2 == 0) ? 2 : 3, m = n / r;
+    for (int p = 0; p < r; ++p) dft23(x + (size_t)p * s, s * r, m, y + (size_t)p * m);
+    cplx t[3], u[3];
+    for (int k = 0; k < m; ++k) {
+        for (int p = 0; p < r; ++p) {
+            const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)(p * k) / n;
+            t[p] = y[(size_t)p * m + k] * cplx((double)std::cos(a), (double)std::sin(a));
+        }
+        for (int q = 0; q < r; ++q) {
+            cplx acc = 0;
+            for (int p = 0; p < r; ++p) {
+                const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)(p * q) / r;
+                acc += t[p] * cplx((double)std::cos(a), (double)std::sin(a));
+            }
+            u[q] = acc;
+        }
+        for (int q = 0; q < r; ++q) y[k + (size_t)q * m] = u[q];
+    }
+}
+
+void rfft2(int nx, int ny, const double* real, double* out)
+{
+    const int mox = nx / 2 + 1;
+    std::vector<cplx> row(nx), rowo(nx), half((size_t)ny * mox), col(ny), colo(ny);
+    for (int y = 0; y < ny; ++y) {
+        for (int x = 0; x < nx; ++x) row[x] = real[(size_t)y * nx + x];
+        dft23(row.data(), 1, nx, rowo.data());
+        for (int c = 0; c < mox; ++c) half[(size_t)y * mox + c] = rowo[c];
+    }
+    for (int c = 0; c < mox; ++c) {
+        for (int y = 0; y < ny; ++y) col[y] = half[(size_t)y * mox + c];
+        dft23(col.data(), 1, ny, colo.data());
+        for (int y = 0; y < ny; ++y) {
+            out[2 * ((size_t)y * mox + c)] = colo[y].real();
+            out[2 * ((size_t)y * mox + c) + 1] = colo[y].imag();
+        }
+    }
+}
+
+// Real-space patterns of matrix_device_init (gpu_flow/code/util/init.cu:22-261) on the
+// Nx x Ny grid of the unit square, in FP64. `mode` is passed to the reference's int
+// parameter, so it is truncated; the rectangle pattern takes x_mode from Lx and Nx as
+// main.cu:330 does; sv and cr use x_frac 0.2 and 0.8 (main.cu:339-342). The reference's
+// rand() draws (rectangle noise strip, isr phase) come from the SplitMix64 stream.
+static void pattern_real(const GridInfo& g, int type, double mode, double amp, uint64_t& s, std::vector<double>& v)
+{
+    const int nx = g.nx, ny = g.ny;
+    const double PI = kPi;
+    v.assign((size_t)nx * ny, 0.0);
+    const int im = (int)mode;
+    auto at = [&](int i, int j) -> double& { return v[(size_t)j * nx + i]; };
+    switch (type) {
+    case 1: { // isr (init.cu:102-128)
+        const double phase = 2 * PI * unit_open(s);
+        const double dx = double(im) / nx, dy = 0.0 / ny;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) at(i, j) = amp * std::cos(2.0 * PI * (i * dx + j * dy) + phase);
+        break;
+    }
+    case 2: { // dislocation (init.cu:22-67), y_mode 0
+        const double dx = 1.0 / nx, dy = 1.0 / ny;
+        const double x1 = (nx / 2.0) * dx + dx / 2.0, x2 = x1;
+        const double y1 = (ny / 4.0) * dy + dy / 2.0, y2 = (3.0 * ny / 4.0) * dy + dy / 2.0;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double p1 = std::atan2(j * dy - y1, i * dx - x1), p2 = std::atan2(j * dy - y2, i * dx - x2);
+                at(i, j) = amp * std::cos(im * 2.0 * PI * (i * dx) + 0 * 2.0 * PI * (j * dy) - p1 + p2);
+            }
+        break;
+    }
+    case 3: { // rectangle (init.cu:69-100) with x_mode = (Lx / (Nx - 1)) (Nx - 5) / 2 (main.cu:330)
+        const int xm = (int)((g.lx / (nx - 1.0)) * (nx - 5.0) / 2.0);
+        const double dx = double(xm) / nx, dy = 0.0;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                at(i, j) = (i < nx / 8) ? (2.0 * unit_open(s) - 1.0) * amp : amp * std::cos(2.0 * PI * (i * dx + j * dy));
+        break;
+    }
+    case 4: { // sv (init.cu:130-163), x_frac 0.2
+        const double x_frac = 0.2, dy = double(im) / ny;
+        const double xl = 0.5 * (1.0 - x_frac), xr = 1.0 - xl;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double x = i / double(nx), y = j / double(ny);
+                double ph = -0.5 * std::sin(2 * PI * y) - x * x;
+                if (x > xr) ph += 1.0;
+                else if (x > xl) ph += 0.5 * (1.0 - std::cos(PI * (x - xl) / x_frac));
+                at(i, j) = amp * std::cos(2.0 * PI * (j * dy + ph));
+            }
+        break;
+    }
+    case 5: { // cr (init.cu:165-207), x_frac 0.8
+        const double x_frac = 0.8, dx = 1.0 / nx, dy = 1.0 / ny;
+        const double x1 = 0.5 * ((1.0 - x_frac) * nx + 1) * dx, x2 = 1.0 - x1;
+        const double y1 = 0.5 * (ny + 1) * dy, y2 = y1;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double p1 = std::atan2(j * dy - y1, i * dx - x1), p2 = std::atan2(j * dy - y2, i * dx - x2);
+                at(i, j) = amp * std::cos(im * 2.0 * PI * (j * dy) - p1 + p2);
+            }
+        break;
+    }
+    case 6: { // giantspiral (init.cu:209-248)
+        const double dx = 1.0 / nx, dy = 1.0 / ny;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double ax = i * dx - 0.5, ay = j * dy - 0.5, bx = i * dx - 0.8, by = j * dy - 0.5;
+                const double r = std::sqrt(ax * ax + ay * ay);
+                at(i, j) = amp * std::cos(2.0 * PI * im * r - std::atan2(ay, ax) + std::atan2(by, bx));
+            }
+        break;
+    }
+    default: break;
+    }
+}
+
+void pattern_theta(const GridInfo& g, int type, double mode, double amp, uint64_t seed, double noise, double* theta,
+                   double* f, double* F)
+{
+    const int mox = g.mox, ny = g.ny, L = g.L;
+    const size_t plane = (size_t)mox * ny;
+    std::memset(theta, 0, sizeof(double) * 2 * plane * L);
+    uint64_t s = seed;
+    if (type == 7) {
+        // init_test (init.cu:250-310): row 0, columns c > 0 of every mode get amp sin(c)
+        // in f and theta; F_k = amp cos(k)
+        std::memset(f, 0, sizeof(double) * 2 * plane * L);
+        for (int k = 0; k < L; ++k) {
+            for (int c = 1; c < mox; ++c) {
+                theta[2 * ((size_t)k * plane + c)] = amp * std::sin((double)c);
+                f[2 * ((size_t)k * plane + c)] = amp * std::sin((double)c);
+            }
+            F[2 * k] = amp * std::cos((double)k);
+            F[2 * k + 1] = 0.0;
+        }
+    } else {
+        std::vector<double> v;
+        pattern_real(g, type, mode, amp, s, v);
+        rfft2(g.nx, ny, v.data(), theta);
+        // modes k >= 1: uniform noise in [-noise, noise) (init_random, init.cu:350-365)
+        if (noise > 0)
+            for (int k = 1; k < L; ++k)
+                for (size_t e = 0; e < plane; ++e) {
+                    theta[2 * ((size_t)k * plane + e)] = noise * (2.0 * unit_open(s) - 1.0);
+                    theta[2 * ((size_t)k * plane + e) + 1] = noise * (2.0 * unit_open(s) - 1.0);
+                }
+    }
+    // Hermitian fix on the kx = 0 column (make_real_signal, util.cu:184-224)
+    auto fix = [&](double* a) {
+        for (int k = 0; k < L; ++k) {
+            double* b = a + 2 * (size_t)k * plane;
+            for (int r = 0; r < ny; ++r) {
+                double* e = b + 2 * (size_t)r * mox;
+                if (r == 0 || r == ny / 2) e[1] = 0.0;
+                else if (r < ny / 2) {
+                    const double* src = b + 2 * (size_t)(ny - r) * mox;
+                    e[0] = src[0];
+                    e[1] = -src[1];
+                }
+            }
+        }
+    };
+    fix(theta);
+    if (type == 7) fix(f);
 }
 
 } // namespace rbchost

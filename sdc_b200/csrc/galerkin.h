@@ -53,6 +53,15 @@ void build_operator_tables(const GridInfo& g, const Tables& T, OperatorTables& o
 // (interleaved complex), followed by the Hermitian fix on the kx = 0 column.
 void seeded_theta(const GridInfo& g, uint64_t seed, double amp, double kmax, double* theta);
 void seeded_positions(uint64_t seed, int n, double lx, double ly, double* xyz);
+// Pattern initial temperature (rbc_init_pattern types) into theta [L][Ny][mox]
+// (interleaved complex): the reference's real-space pattern R2C-transformed into the
+// lowest vertical mode, uniform noise in the others, the Hermitian fix. For the TEST
+// pattern f and F are filled too (f [L][Ny][mox], F [L] interleaved complex).
+void pattern_theta(const GridInfo& g, int type, double mode, double amp, uint64_t seed, double noise, double* theta,
+                   double* f, double* F);
+// Forward real 2-D FFT (unnormalised, e^{-i}) of real[ny][nx] into out[ny][nx/2+1]
+// (interleaved complex); nx, ny = 2^a 3^b.
+void rfft2(int nx, int ny, const double* real, double* out);
 // Tracer start patterns of particle_tracer::init_positions (rbc_tracer_init types).
 void tracer_pattern(int type, uint64_t seed, int n, double lx, double ly, double cx, double cy, double cz,
                     double sigma, double* xyz);

@@ -11,6 +11,10 @@
 //   -history file        also restore the AB2 history (exact restart; the reference has none)
 //   -device d  -dir path -seed s  -particles n
 //   -init_amp a -init_kmax k   seeded initial condition (replaces init_random)
+//   -init_isr | -init_dislocation | -init_rectangle | -init_sv | -init_cr |
+//   -init_giantspiral | -init_test   pattern initial conditions (main.cu:88-98, 326-352)
+//   -init_mode m  -init_noise a      their mode (default Lx/2) and the noise of the other
+//                                    modes (default 1e-6, init_random's amplitude)
 //   -form fp64|mixed     precision form
 //   -diag n              print Nu_wall, Nu_vol, KE every n steps
 //   -real_bytes 4|8      element size of the written dumps (4 = the reference's default)
@@ -107,7 +111,18 @@ int main(int argc, char** argv)
                     h, "rbc_load_state");
         if (!rc && a.has("-history")) rc |= check(rbc_load_history(h, a.str("-history")), h, "rbc_load_history");
     } else {
-        rc |= check(rbc_init_fields(h, seed, a.num("-init_amp", 1e-3), a.num("-init_kmax", 4.0)), h, "rbc_init_fields");
+        static const char* kPatterns[] = {"-init_isr", "-init_dislocation", "-init_rectangle", "-init_sv",
+                                          "-init_cr", "-init_giantspiral", "-init_test"};
+        int pattern = 0;
+        for (int i = 0; i < 7; ++i)
+            if (a.has(kPatterns[i])) pattern = i + 1;
+        if (pattern)
+            rc |= check(rbc_init_pattern(h, pattern, a.num("-init_mode", p.lx / 2.0), a.num("-init_amp", 1e-6), seed,
+                                         pattern == RBC_INIT_TEST ? 0.0 : a.num("-init_noise", 1e-6)),
+                        h, "rbc_init_pattern");
+        else
+            rc |= check(rbc_init_fields(h, seed, a.num("-init_amp", 1e-3), a.num("-init_kmax", 4.0)), h,
+                        "rbc_init_fields");
     }
     if (!rc && p.n_tracers > 0) rc |= check(rbc_tracers_seed(h, seed), h, "rbc_tracers_seed");
     if (rc) {

@@ -17,6 +17,7 @@
 #pragma once
 #include "common.cuh"
 #include "fft.cuh"
+#include "fft2p.cuh"
 
 namespace rbck {
 
@@ -295,6 +296,241 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
         N[o] = cmk<C>(at.x, at.y);
         N[pl + o] = cmk<C>(af.x, af.y);
         N[2 * pl + o] = cmk<C>(ag.x, ag.y);
+    }
+}
+
+// =================================================================================
+// Two-pass forms of K1, K2, K4 and K5 for transform lengths N = RX * RX (64, 256), see
+// fft2p.cuh. The CTA holds the same transforms as the Stockham forms; each transform
+// is done by RX consecutive lanes, so the block has (transforms x RX) threads. A
+// transform's shared region has tp_stride(N) elements (the padded row of the Stockham
+// forms, or the RX (RX + 1) transpose tile if that is longer).
+RBC_HD int tp_stride(int n, int rx) { return rbcfft::padded_len(n) > rx * (rx + 1) ? rbcfft::padded_len(n) : rx * (rx + 1); }
+
+// Synthesis field fld (order of k_synth_columns) at (c, r) from theta, f, g.
+RBC_D double2 synth_value(int fld, double2 vt, double2 vf, double2 vg, const Mult& m)
+{
+    switch (fld) {
+    case 0: return cmul_is<double2, double>(vf, m.fx);
+    case 1: return cmul_is<double2, double>(vf, m.fy);
+    case 2: return vf * (-m.lap);
+    case 3: return cmul_is<double2, double>(vg, m.fy);
+    case 4: return cmul_is<double2, double>(vg, m.fx) * (-1.0);
+    case 5: return vt;
+    case 6: return cmul_is<double2, double>(vt, m.fx);
+    default: return cmul_is<double2, double>(vt, m.fy);
+    }
+}
+
+// K1, two-pass: grid (ckw / W, L), block 8 W RX threads (transform q = fld W + cc).
+template <typename R, int RX>
+__global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
+    Geom G, int W, const double2* __restrict__ twy, const double2* __restrict__ th,
+    const double2* __restrict__ f, const double2* __restrict__ g, const double2* __restrict__ FG,
+    typename cplx_t<R>::type* __restrict__ H)
+{
+    typedef typename cplx_t<R>::type C;
+    constexpr int N = RX * RX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    const int st = tp_stride(N, RX);
+    C* buf = tw + N;
+    double2* stg = reinterpret_cast<double2*>(buf + 8 * W * st); // [3][W][N]: theta, f, g
+    const int k = blockIdx.y;
+    const int c0 = blockIdx.x * W;
+    const size_t base = ((size_t)k * G.ckp + c0) * N;
+    for (int e = threadIdx.x; e < W * N; e += blockDim.x) {
+        const int cc = e / N, r = e - cc * N;
+        if (c0 + cc < G.ckeep && row_kept(r, N)) {
+            cp_async<16>(stg + e, th + base + e);
+            cp_async<16>(stg + W * N + e, f + base + e);
+            cp_async<16>(stg + 2 * W * N + e, g + base + e);
+        }
+    }
+    load_twiddles<R>(tw, twy, N);
+    cp_async_wait_all();
+    __syncthreads();
+    const int q = threadIdx.x / RX, t = threadIdx.x - q * RX;
+    const int fld = q / W, cc = q - fld * W, c = c0 + cc;
+    C v[RX];
+#pragma unroll
+    for (int a = 0; a < RX; ++a) {
+        const int r = t + RX * a;
+        double2 val = make_double2(0, 0);
+        if (c < G.ckeep && row_kept(r, N)) {
+            const int e = cc * N + r;
+            val = synth_value(fld, stg[e], stg[W * N + e], stg[2 * W * N + e], Mult(c, r, G));
+        }
+        if (c == 0 && r == 0) {
+            if (fld == 3) val = val + FG[k];
+            else if (fld == 4) val = val + FG[G.L + k];
+        }
+        v[a] = cmk<C>(val.x, val.y);
+    }
+    rbcfft::two_pass<RX, R>(v, t, buf + q * st, tw, +1);
+    C* dst = H + (((size_t)fld * G.L + k) * G.ckp + c) * N;
+#pragma unroll
+    for (int k2 = 0; k2 < RX; ++k2) dst[t + RX * k2] = v[k2];
+}
+
+// K2, two-pass: block NP RX threads, transform pp = row pair.
+template <typename R, int RX>
+__global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
+    Geom G, int NP, const double2* __restrict__ twx, const typename cplx_t<R>::type* __restrict__ H,
+    R* __restrict__ phys)
+{
+    typedef typename cplx_t<R>::type C;
+    constexpr int N = RX * RX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* buf = tw + N;
+    const int st = tp_stride(N, RX);
+    const int row0 = 2 * NP * blockIdx.x;
+    const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
+    // A[n] to slot n, B[n] to slot N - n (B[0] to the spare last slot st - 1 > pad(N - 1))
+    const C* src = H + (size_t)plane * G.ckp * G.ny + y0;
+    for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
+        const int n = e / NP, pp = e - n * NP;
+        C* row = buf + pp * st;
+        cp_async<sizeof(C)>(row + rbcfft::pad(n), src + (size_t)n * G.ny + 2 * pp);
+        cp_async<sizeof(C)>(row + (n ? rbcfft::pad(N - n) : st - 1), src + (size_t)n * G.ny + 2 * pp + 1);
+    }
+    for (int e = threadIdx.x; e < NP * N; e += blockDim.x) {
+        const int pp = e / N, n = e - pp * N;
+        if (n >= G.ckeep && n <= N - G.ckeep) buf[pp * st + rbcfft::pad(n)] = cmk<C>(0, 0);
+    }
+    load_twiddles<R>(tw, twx, N);
+    cp_async_wait_all();
+    __syncthreads();
+    for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
+        const int n = e / NP, pp = e - n * NP;
+        C* row = buf + pp * st;
+        C* pb = row + (n ? rbcfft::pad(N - n) : st - 1);
+        C A = row[rbcfft::pad(n)], B = *pb;
+        if (n == 0) { A.y = 0; B.y = 0; }
+        C z; z.x = A.x - B.y; z.y = A.y + B.x;       // A + iB
+        row[rbcfft::pad(n)] = z;
+        if (n > 0) {
+            C zm; zm.x = A.x + B.y; zm.y = B.x - A.y; // conj(A) + i conj(B)
+            *pb = zm;
+        }
+    }
+    __syncthreads();
+    const int pp = threadIdx.x / RX, t = threadIdx.x - pp * RX;
+    C* S = buf + pp * st;
+    C v[RX];
+#pragma unroll
+    for (int a = 0; a < RX; ++a) v[a] = S[rbcfft::pad(t + RX * a)];
+    __syncwarp(rbcfft::team_mask<RX>()); // every lane has read before the tile is overwritten
+    rbcfft::two_pass<RX, R>(v, t, S, tw, +1);
+    R* dst = phys + (size_t)(row0 + 2 * pp) * N;
+#pragma unroll
+    for (int k2 = 0; k2 < RX; ++k2) {
+        dst[t + RX * k2] = v[k2].x;
+        dst[N + t + RX * k2] = v[k2].y;
+    }
+}
+
+// K4, two-pass: block NP RX threads.
+template <typename R, int RX>
+__global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
+    Geom G, int NP, const double2* __restrict__ twx, const R* __restrict__ grp,
+    typename cplx_t<R>::type* __restrict__ gh)
+{
+    typedef typename cplx_t<R>::type C;
+    constexpr int N = RX * RX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* buf = tw + N;
+    const int st = tp_stride(N, RX);
+    const int row0 = 2 * NP * blockIdx.x;
+    const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
+    const int pp = threadIdx.x / RX, t = threadIdx.x - pp * RX;
+    const R* src = grp + (size_t)(row0 + 2 * pp) * N;
+    C v[RX];
+#pragma unroll
+    for (int a = 0; a < RX; ++a) {
+        v[a].x = src[t + RX * a];
+        v[a].y = src[N + t + RX * a];
+    }
+    load_twiddles<R>(tw, twx, N);
+    __syncthreads();
+    C* S = buf + pp * st;
+    rbcfft::two_pass<RX, R>(v, t, S, tw, -1);
+#pragma unroll
+    for (int k2 = 0; k2 < RX; ++k2) S[rbcfft::pad(t + RX * k2)] = v[k2];
+    __syncthreads();
+    const R half = (R)0.5;
+    C* dst = gh + (size_t)plane * G.ckp * G.ny + y0;
+    for (int e = threadIdx.x; e < NP * G.ckw; e += blockDim.x) {
+        const int n = e / NP, q = e - n * NP;
+        C A = cmk<C>(0, 0), B = A;
+        if (n < G.ckeep) {
+            const C z = buf[q * st + rbcfft::pad(n)];
+            const C zm = buf[q * st + rbcfft::pad(n == 0 ? 0 : N - n)];
+            A.x = half * (z.x + zm.x);
+            A.y = half * (z.y - zm.y);
+            B.x = half * (z.y + zm.y);
+            B.y = half * (zm.x - z.x);
+        }
+        dst[(size_t)n * G.ny + 2 * q] = A;
+        dst[(size_t)n * G.ny + 2 * q + 1] = B;
+    }
+}
+
+// K5, two-pass: grid (ckw, L), block 13 RX threads (transform = group).
+template <typename R, int RX>
+__global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
+    Geom G, const double2* __restrict__ twy, const typename cplx_t<R>::type* __restrict__ gh,
+    typename cplx_t<R>::type* __restrict__ N_out, double* __restrict__ NFG)
+{
+    typedef typename cplx_t<R>::type C;
+    constexpr int N = RX * RX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* buf = tw + N;
+    const int st = tp_stride(N, RX);
+    const int c = blockIdx.x, k = blockIdx.y;
+    const size_t cstride = (size_t)G.L * G.ckp * N; // between groups
+    const int gq = threadIdx.x / RX, t = threadIdx.x - gq * RX;
+    const C* src = gh + ((size_t)k * G.ckp + c) * N + gq * cstride;
+    C v[RX];
+#pragma unroll
+    for (int a = 0; a < RX; ++a) v[a] = src[t + RX * a];
+    load_twiddles<R>(tw, twy, N);
+    __syncthreads();
+    C* S = buf + gq * st;
+    rbcfft::two_pass<RX, R>(v, t, S, tw, -1);
+#pragma unroll
+    for (int k2 = 0; k2 < RX; ++k2) S[rbcfft::pad(t + RX * k2)] = v[k2];
+    __syncthreads();
+    const double invP = 1.0 / ((double)G.nx * N);
+    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        double2 vv[13];
+#pragma unroll
+        for (int gi = 0; gi < 13; ++gi) {
+            const C z = buf[gi * st + rbcfft::pad(r)];
+            vv[gi] = make_double2(z.x, z.y);
+        }
+        if (c == 0 && r == 0) {
+            NFG[k] = vv[10].x * (-invP / G.pr);          // F: mean of the g-y group
+            NFG[G.L + k] = -vv[11].x * (-invP / G.pr);   // G: minus mean of the g-x group
+        }
+        const Mult m(c, r, G);
+        const double xx = -(m.fx * m.fx), yy = -(m.fy * m.fy);
+        double2 af = vv[0] * xx + vv[1] * m.xy + vv[2] * yy + cmul_is<double2, double>(vv[3], m.fx) +
+                     cmul_is<double2, double>(vv[4], m.fy) + cmul_is<double2, double>(vv[5], m.fx) * m.lap +
+                     cmul_is<double2, double>(vv[6], m.fy) * m.lap + vv[7] * m.lap;
+        double2 ag = vv[8] * m.xy + vv[9] * (yy - xx) + cmul_is<double2, double>(vv[10], m.fy) +
+                     cmul_is<double2, double>(vv[11], m.fx);
+        const double2 at = vv[12] * (-invP);
+        af = af * (-invP / G.pr);
+        ag = ag * (-invP / G.pr);
+        const size_t o = ((size_t)k * G.ckp + c) * N + r;
+        const size_t pl = (size_t)G.L * G.ckp * N;
+        N_out[o] = cmk<C>(at.x, at.y);
+        N_out[pl + o] = cmk<C>(af.x, af.y);
+        N_out[2 * pl + o] = cmk<C>(ag.x, ag.y);
     }
 }
 

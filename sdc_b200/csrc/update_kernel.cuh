@@ -72,29 +72,22 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
     {
         const long long e = (long long)blockIdx.x * (blockDim.x / T) + threadIdx.x / T; // wavenumber c * ny + r
         const int c = (int)(e / ny), r = (int)(e - (long long)c * ny);
-        const int cl = (e < nwave) ? A.cls[e] : -1;          // uniform over the team
-        const bool act = cl >= 0;
-        const bool kact = act && k < L;
+        // the class index and the vectors are fetched together: the vector loads are
+        // predicated on the kept band by its formula (always in bounds), the tables wait
+        // for the class index
+        const int cl = (e < nwave) ? __ldg(A.cls + e) : -1;   // uniform over the team
+        const bool geo = e < nwave && k < L && c < G.ckeep && row_kept(r, ny);
         const size_t o = (size_t)e;
         const int ry = wrap_row(r, ny);
         const double mx = (kPi + kPi) * (c / G.lx), my = (kPi + kPi) * (ry / G.ly);
         const double q2d = mx * mx + my * my;       // device formula of the reference kernels
         const bool mirror = (c == 0 && r > 0 && r < ny / 2);
         double2 nt = make_double2(0, 0), nf = nt, ng = nt, ut = nt, uf = nt, ug = nt, ht = nt, hf = nt, hg = nt;
-        double bi[L], M[4][L];
-        if (kact) {
+        if (geo) {
             const C t0 = Nc[(0 * L + k) * plane + o], t1 = Nc[(1 * L + k) * plane + o], t2 = Nc[(2 * L + k) * plane + o];
             nt = make_double2(t0.x, t0.y);
             nf = make_double2(t1.x, t1.y);
             ng = make_double2(t2.x, t2.y);
-            const double* brow = A.binv + (size_t)cl * L * L + (size_t)k * L;
-            const double* mrow = A.imp + (size_t)cl * 4 * L * L + (size_t)k * L;
-#pragma unroll
-            for (int m = 0; m < L; ++m) {
-                bi[m] = brow[m];
-#pragma unroll
-                for (int b = 0; b < 4; ++b) M[b][m] = mrow[b * L * L + m];
-            }
             if (!mirror) {
                 ut = A.th[k * plane + o];
                 uf = A.f[k * plane + o];
@@ -103,6 +96,35 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
                     ht = A.hist[(0 * L + k) * plane + o];
                     hf = A.hist[(1 * L + k) * plane + o];
                     hg = A.hist[(2 * L + k) * plane + o];
+                }
+            }
+        }
+        const bool act = cl >= 0;
+        const bool kact = act && k < L;
+        double bi[L], M[4][L];
+        if (kact) {
+            const double* brow = A.binv + (size_t)cl * L * L + (size_t)k * L;
+            const double* mrow = A.imp + (size_t)cl * 4 * L * L + (size_t)k * L;
+            if constexpr (L % 2 == 0) {
+                // rows start on even doubles: 16-byte loads
+#pragma unroll
+                for (int m = 0; m < L; m += 2) {
+                    const double2 v = __ldg(reinterpret_cast<const double2*>(brow + m));
+                    bi[m] = v.x;
+                    bi[m + 1] = v.y;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const double2 w = __ldg(reinterpret_cast<const double2*>(mrow + b * L * L + m));
+                        M[b][m] = w.x;
+                        M[b][m + 1] = w.y;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < L; ++m) {
+                    bi[m] = __ldg(brow + m);
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) M[b][m] = __ldg(mrow + b * L * L + m);
                 }
             }
         } else {
