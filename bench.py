@@ -190,6 +190,44 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def mixed_form(s64, stream, args, local, world):
+    """Mixed form (FP32 synthesis, products and FFTs; FP64 implicit solve and reductions)
+    on the same workload: sim-time/s over the same timed step count from the given state,
+    and the relative error of Nu_wall, Nu_vol and KE against the FP64 form after 2000
+    steps from that state (equal sim time)."""
+    import torch
+    import sdc_b200
+    state = s64.get_state()
+    tr = s64.tracers_get()
+    m = sdc_b200.Solver(**WORK, form="mixed", n_tracers=NTRACERS, device=local, tune=bool(args.tune))
+    m.set_stream(stream.cuda_stream)
+    m.set_state(*state)
+    m.tracers_set(tr)
+    m.step(args.warmup)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step_async(args.steps)
+    e1.record(stream)
+    m.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, device="cuda")
+    value = weak_scaling_value(world, args.steps, WORK["dt"], ms)
+    # accuracy at equal sim time
+    n_cmp = 2000
+    for sv in (s64, m):
+        sv.set_state(*state)
+        sv.tracers_set(tr)
+        sv.step(n_cmp)
+    d64, dm = s64.diagnostics(), m.diagnostics()
+    err = {k: abs(dm[k] - d64[k]) / abs(d64[k]) for k in ("nu_wall", "nu_vol", "ke")}
+    m.close()
+    return {"value": value, "unit": "sim-time/s", "ms_per_step": ms / args.steps,
+            "dtype": "f32 synthesis/products/FFTs + f64 implicit solve, mean flow, diagnostics",
+            "rel_err_vs_fp64": err, "compared_after_steps": n_cmp,
+            "fp64_nu_wall": d64["nu_wall"], "nu_err_le_1e-3": err["nu_wall"] <= 1e-3}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,6 +237,7 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", type=int, default=1, help="1: autotune the FFT launch tiling at creation")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed-form leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -289,6 +328,13 @@ def main():
     d = s.diagnostics()
     assert np.isfinite(d["ke"]) and np.all(np.isfinite(out_tr)) and all(np.all(np.isfinite(a)) for a in out_state)
 
+    # ---- the mixed form on the same workload (north_star form 1): throughput from the
+    # convective FP64 state reached above, and its diagnostics error against the FP64 form
+    # over the same 2000 steps from that state
+    forms = None
+    if args.form == "fp64" and not args.no_forms:
+        forms = {"mixed": mixed_form(s, stream, args, local, world)}
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(8)
@@ -307,7 +353,7 @@ def main():
                            "alg_bytes_per_step": step_b + tr_b},
                 "roofline": roof, "gpu_launches": launches,
                 "hbm_gbs_step_alg": (step_b + tr_b) / (ms_max / args.steps * 1e-3) / 1e9,
-                "clocks": clocks, "e2e": e2e, "cpu_baseline": cb,
+                "clocks": clocks, "e2e": e2e, "cpu_baseline": cb, "forms": forms,
                 "diag": {"nu_wall": d["nu_wall"], "ke": d["ke"], "step": d["step"]}}
         print(json.dumps(line), flush=True)
     s.close()

@@ -352,14 +352,27 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
     __syncthreads();
     const int q = threadIdx.x / RX, t = threadIdx.x - q * RX;
     const int fld = q / W, cc = q - fld * W, c = c0 + cc;
+    // the multipliers of Mult, evaluated with the same expressions, only where a field
+    // needs them (fx per column; fy and the Laplacian per row)
+    const double fx = c * (2 * kPi / G.lx), ac = c / G.lx;
+    const bool ckept = c < G.ckeep;
+    const double2* in = stg + (fld < 3 ? W * N : fld < 5 ? 2 * W * N : 0) + cc * N; // f, g or theta
     C v[RX];
 #pragma unroll
     for (int a = 0; a < RX; ++a) {
         const int r = t + RX * a;
-        double2 val = make_double2(0, 0);
-        if (c < G.ckeep && row_kept(r, N)) {
-            const int e = cc * N + r;
-            val = synth_value(fld, stg[e], stg[W * N + e], stg[2 * W * N + e], Mult(c, r, G));
+        const double2 u = (ckept && row_kept(r, N)) ? in[r] : make_double2(0, 0);
+        const int ry = wrap_row(r, N);
+        double2 val;
+        switch (fld) {
+        case 0: case 4: case 6: val = cmul_is<double2, double>(u, fx); if (fld == 4) val = val * (-1.0); break;
+        case 1: case 3: case 7: val = cmul_is<double2, double>(u, ry * (2 * kPi / G.ly)); break;
+        case 2: {
+            const double b = ry / G.ly;
+            val = u * (-((-4 * kPi * kPi) * (ac * ac + b * b)));
+            break;
+        }
+        default: val = u;
         }
         if (c == 0 && r == 0) {
             if (fld == 3) val = val + FG[k];
