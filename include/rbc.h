@@ -307,6 +307,81 @@ rbc_status rbc_nonlinear_noalloc(int device, int nx, int ny, int nz, double lx, 
 /* Device kernel launches issued by the last rbc_step call (for launch accounting). */
 long long rbc_kernel_launches(const rbc_handle* h);
 
+/* --- learned surrogate ----------------------------------------------------------- */
+/* No counterpart in the reference (jceyy/sdc has no learned component). A Fourier neural
+ * operator over the horizontal plane advances a solver's state by one surrogate interval
+ * (steps_per_interval plain steps) at a time. Its input and output are the collocation
+ * fields theta, u, v, w at the nq Gauss-Legendre levels z_q of (-1/2, 1/2): FP32
+ * [ny][nx][4 nq], channel = field * nq + q. The network predicts their normalized
+ * increment; the increment is projected back onto (theta, f, g, F, G) by least squares
+ * in z (exact for fields in the span of the basis) and added to the FP64 state. BF16
+ * GEMMs with FP32 accumulation, FP32 loss and Adam. Layout of the parameter vector:
+ * sdc_b200/csrc/fno.cu. One surrogate serves solvers of one grid (nx, ny, nz). */
+typedef struct rbc_fno rbc_fno;
+typedef struct {
+    int nx, ny;        /* horizontal grid of the solvers it serves */
+    int nz;            /* their vertical Galerkin modes */
+    int nq;            /* collocation levels (nq >= nz; channels C = 4 nq <= 256) */
+    int width;         /* channels of the spectral layers (8..64, a multiple of 8) */
+    int modes;         /* retained Fourier modes per direction: kx < m, |ky| < m (+ ky = -m) */
+    int layers;        /* spectral layers */
+    int hidden;        /* hidden width of the projection (8..256) */
+    int max_batch;     /* largest training batch */
+    int device;
+    unsigned long long seed; /* weight initialisation (SplitMix64) */
+} rbc_fno_params;
+rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out);
+void rbc_fno_destroy(rbc_fno* m);
+const char* rbc_fno_last_error(const rbc_fno* m);
+long long rbc_fno_num_params(const rbc_fno* m);
+rbc_status rbc_fno_get_params(rbc_fno* m, float* out, long long n);
+rbc_status rbc_fno_set_params(rbc_fno* m, const float* in, long long n); /* resets Adam */
+/* Normalization [4][C]: input mean, input std, increment mean, increment std. */
+rbc_status rbc_fno_get_norm(rbc_fno* m, float* out);
+rbc_status rbc_fno_set_norm(rbc_fno* m, const float* in);
+/* The bare network on host buffers x, y [batch][ny][nx][C] (already normalized). */
+rbc_status rbc_fno_forward(rbc_fno* m, const float* x, int batch, float* y);
+/* Mean-squared-error loss of the network on (x, target) and its gradient with respect to
+ * the parameter vector (n = rbc_fno_num_params). */
+rbc_status rbc_fno_loss_grad(rbc_fno* m, const float* x, const float* target, int batch, double* loss,
+                             float* grad);
+/* Collocation fields of a solver's state (out [ny][nx][4 nq]), and the increment form:
+ * state += projection of delta [ny][nx][4 nq] (the next step is an Euler step). */
+rbc_status rbc_fno_colloc_get(rbc_fno* m, rbc_handle* h, float* out);
+rbc_status rbc_fno_colloc_add(rbc_fno* m, rbc_handle* h, const float* delta);
+/* Snapshot store on the device (nslots collocation snapshots), filled from solvers. */
+rbc_status rbc_fno_dataset_reserve(rbc_fno* m, int nslots);
+rbc_status rbc_fno_dataset_capture(rbc_fno* m, rbc_handle* h, int slot);
+/* Trains on the pairs (src[i] -> dst[i]) of the store: `epochs` passes in shuffled
+ * batches (seeded), Adam with a cosine decay from lr to lr / 50; fit_norm = 1 first sets
+ * the normalization from these pairs. epoch_loss[e] = mean loss of epoch e. */
+rbc_status rbc_fno_train(rbc_fno* m, const int* src, const int* dst, int npairs, int epochs, int batch, double lr,
+                         unsigned long long seed, int fit_norm, double* epoch_loss);
+/* n surrogate intervals of the solver's state. */
+rbc_status rbc_fno_advance(rbc_fno* m, rbc_handle* h, int n);
+
+/* Rollout with the plain step as judge: every judge_every-th interval the surrogate and
+ * the plain step (steps_per_interval steps) each advance the same state; the rollout
+ * keeps the plain result and compares Nu_wall (relative error) and the theta spectrum at
+ * z = 0 (relative L2 error over spec_bins bins; 0 bins or spec_tol <= 0: not checked).
+ * When an error exceeds its tolerance the plain step takes over for fallback_intervals
+ * intervals (-1: the rest of the run). */
+typedef struct {
+    int intervals;
+    int steps_per_interval;
+    int judge_every;
+    double nu_tol;
+    double spec_tol;
+    int spec_bins;
+    int fallback_intervals;
+} rbc_surrogate_params;
+typedef struct {
+    int surrogate_intervals, plain_intervals, checks, fallbacks;
+    double max_nu_err, max_spec_err, last_nu_err, last_spec_err;
+    double ms;         /* device time of the rollout (CUDA events on the solver's stream) */
+} rbc_surrogate_report;
+rbc_status rbc_surrogate_run(rbc_fno* m, rbc_handle* h, const rbc_surrogate_params* p, rbc_surrogate_report* rep);
+
 #ifdef __cplusplus
 }
 #endif

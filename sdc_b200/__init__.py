@@ -39,6 +39,25 @@ class _Diag(ctypes.Structure):
                 ("step", ctypes.c_longlong)]
 
 
+class _FnoParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nq", ctypes.c_int),
+                ("width", ctypes.c_int), ("modes", ctypes.c_int), ("layers", ctypes.c_int),
+                ("hidden", ctypes.c_int), ("max_batch", ctypes.c_int), ("device", ctypes.c_int),
+                ("seed", ctypes.c_ulonglong)]
+
+
+class _SurrogateParams(ctypes.Structure):
+    _fields_ = [("intervals", ctypes.c_int), ("steps_per_interval", ctypes.c_int), ("judge_every", ctypes.c_int),
+                ("nu_tol", ctypes.c_double), ("spec_tol", ctypes.c_double), ("spec_bins", ctypes.c_int),
+                ("fallback_intervals", ctypes.c_int)]
+
+
+class _SurrogateReport(ctypes.Structure):
+    _fields_ = [("surrogate_intervals", ctypes.c_int), ("plain_intervals", ctypes.c_int), ("checks", ctypes.c_int),
+                ("fallbacks", ctypes.c_int), ("max_nu_err", ctypes.c_double), ("max_spec_err", ctypes.c_double),
+                ("last_nu_err", ctypes.c_double), ("last_spec_err", ctypes.c_double), ("ms", ctypes.c_double)]
+
+
 class _State(ctypes.Structure):
     _fields_ = [("theta", ctypes.c_void_p), ("f", ctypes.c_void_p), ("g", ctypes.c_void_p),
                 ("F", ctypes.c_void_p), ("G", ctypes.c_void_p)]
@@ -53,7 +72,10 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_save_state", "rbc_load_state", "rbc_save_history", "rbc_load_history", "rbc_ensemble_create",
            "rbc_ensemble_destroy", "rbc_ensemble_member", "rbc_ensemble_step", "rbc_ensemble_last_error", "rbc_launch_config",
            "rbc_kernel_launches", "rbc_tracers_init", "rbc_tracer_moments", "rbc_tracks_read", "rbc_track_write",
-           "rbc_init_pattern"]
+           "rbc_init_pattern", "rbc_fno_create", "rbc_fno_destroy", "rbc_fno_last_error", "rbc_fno_num_params",
+           "rbc_fno_get_params", "rbc_fno_set_params", "rbc_fno_get_norm", "rbc_fno_set_norm", "rbc_fno_forward",
+           "rbc_fno_loss_grad", "rbc_fno_colloc_get", "rbc_fno_colloc_add", "rbc_fno_dataset_reserve",
+           "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run"]
 INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
 TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
@@ -123,6 +145,27 @@ def lib():
     L.rbc_launch_config.argtypes = [vp, ip, ip]
     L.rbc_kernel_launches.argtypes = [vp]
     L.rbc_kernel_launches.restype = ctypes.c_longlong
+    L.rbc_fno_create.argtypes = [ctypes.POINTER(_FnoParams), ctypes.POINTER(vp)]
+    L.rbc_fno_destroy.argtypes = [vp]
+    L.rbc_fno_destroy.restype = None
+    L.rbc_fno_last_error.argtypes = [vp]
+    L.rbc_fno_last_error.restype = ctypes.c_char_p
+    L.rbc_fno_num_params.argtypes = [vp]
+    L.rbc_fno_num_params.restype = ctypes.c_longlong
+    L.rbc_fno_get_params.argtypes = [vp, fp, ctypes.c_longlong]
+    L.rbc_fno_set_params.argtypes = [vp, fp, ctypes.c_longlong]
+    L.rbc_fno_get_norm.argtypes = [vp, fp]
+    L.rbc_fno_set_norm.argtypes = [vp, fp]
+    L.rbc_fno_forward.argtypes = [vp, fp, ctypes.c_int, fp]
+    L.rbc_fno_loss_grad.argtypes = [vp, fp, fp, ctypes.c_int, _dp, fp]
+    L.rbc_fno_colloc_get.argtypes = [vp, vp, fp]
+    L.rbc_fno_colloc_add.argtypes = [vp, vp, fp]
+    L.rbc_fno_dataset_reserve.argtypes = [vp, ctypes.c_int]
+    L.rbc_fno_dataset_capture.argtypes = [vp, vp, ctypes.c_int]
+    L.rbc_fno_train.argtypes = [vp, ip, ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                ctypes.c_ulonglong, ctypes.c_int, _dp]
+    L.rbc_fno_advance.argtypes = [vp, vp, ctypes.c_int]
+    L.rbc_surrogate_run.argtypes = [vp, vp, ctypes.POINTER(_SurrogateParams), ctypes.POINTER(_SurrogateReport)]
     _LIB = L
     return L
 
@@ -408,3 +451,108 @@ class Solver:
         cnt = ctypes.c_int(0)
         self._check(lib().rbc_table(self.h, name.encode(), _p(out), ctypes.byref(cnt)))
         return out[:cnt.value]
+
+
+def _f32(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class FNO:
+    """Fourier neural operator surrogate of a solver grid (rbc_fno_*, include/rbc.h).
+
+    Channels are theta, u, v, w at nq collocation levels (C = 4 nq); arrays are float32
+    [batch][ny][nx][C]."""
+
+    def __init__(self, nx, ny, nz, nq, width=32, modes=16, layers=4, hidden=128, max_batch=8, device=0, seed=0):
+        self.nx, self.ny, self.nz, self.nq = nx, ny, nz, nq
+        self.C = 4 * nq
+        p = _FnoParams(nx, ny, nz, nq, width, modes, layers, hidden, max_batch, device, seed)
+        m = ctypes.c_void_p()
+        st = lib().rbc_fno_create(ctypes.byref(p), ctypes.byref(m))
+        if st != RBC_OK:
+            raise RBCError(st, "rbc_fno_create failed")
+        self.m = m
+
+    def close(self):
+        if getattr(self, "m", None):
+            lib().rbc_fno_destroy(self.m)
+        self.m = None
+
+    __del__ = close
+
+    def _check(self, st):
+        if st != RBC_OK:
+            raise RBCError(st, lib().rbc_fno_last_error(self.m).decode())
+
+    @property
+    def num_params(self):
+        return lib().rbc_fno_num_params(self.m)
+
+    def get_params(self):
+        out = np.empty(self.num_params, np.float32)
+        self._check(lib().rbc_fno_get_params(self.m, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), out.size))
+        return out
+
+    def set_params(self, v):
+        v, ptr = _f32(v)
+        self._check(lib().rbc_fno_set_params(self.m, ptr, v.size))
+
+    def get_norm(self):
+        out = np.empty((4, self.C), np.float32)
+        self._check(lib().rbc_fno_get_norm(self.m, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def set_norm(self, v):
+        v, ptr = _f32(v)
+        self._check(lib().rbc_fno_set_norm(self.m, ptr))
+
+    def forward(self, x):
+        x, px = _f32(x)
+        y = np.empty_like(x)
+        self._check(lib().rbc_fno_forward(self.m, px, x.shape[0], y.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return y
+
+    def loss_grad(self, x, target):
+        x, px = _f32(x)
+        t, pt = _f32(target)
+        loss = ctypes.c_double(0)
+        g = np.empty(self.num_params, np.float32)
+        self._check(lib().rbc_fno_loss_grad(self.m, px, pt, x.shape[0], ctypes.byref(loss),
+                                            g.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return loss.value, g
+
+    def colloc_get(self, solver):
+        out = np.empty((self.ny, self.nx, self.C), np.float32)
+        self._check(lib().rbc_fno_colloc_get(self.m, solver.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def colloc_add(self, solver, delta):
+        d, pd = _f32(delta)
+        self._check(lib().rbc_fno_colloc_add(self.m, solver.h, pd))
+
+    def reserve(self, nslots):
+        self._check(lib().rbc_fno_dataset_reserve(self.m, nslots))
+
+    def capture(self, solver, slot):
+        self._check(lib().rbc_fno_dataset_capture(self.m, solver.h, slot))
+
+    def train(self, src, dst, epochs, batch, lr=1e-3, seed=0, fit_norm=True):
+        src = np.ascontiguousarray(src, np.int32)
+        dst = np.ascontiguousarray(dst, np.int32)
+        loss = np.zeros(max(epochs, 1), np.float64)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self._check(lib().rbc_fno_train(self.m, src.ctypes.data_as(ip), dst.ctypes.data_as(ip), len(src), epochs,
+                                        batch, lr, seed, int(fit_norm), loss.ctypes.data_as(_dp)))
+        return loss[:epochs]
+
+    def advance(self, solver, n=1):
+        self._check(lib().rbc_fno_advance(self.m, solver.h, n))
+
+    def run(self, solver, intervals, steps_per_interval, judge_every=10, nu_tol=1e-3, spec_tol=0.0, spec_bins=0,
+            fallback_intervals=-1):
+        p = _SurrogateParams(intervals, steps_per_interval, judge_every, nu_tol, spec_tol, spec_bins,
+                             fallback_intervals)
+        r = _SurrogateReport()
+        self._check(lib().rbc_surrogate_run(self.m, solver.h, ctypes.byref(p), ctypes.byref(r)))
+        return {k: getattr(r, k) for k, _ in _SurrogateReport._fields_}

@@ -22,7 +22,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
            "-I" + INCLUDE, "-I" + CSRC]
 CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-I" + INCLUDE, "-I" + CSRC, "-I/usr/local/cuda/include"]
 
-CU_SOURCES = ["api.cu", "peak_fp64.cu", "nonlinear_static.cu"]
+CU_SOURCES = ["api.cu", "peak_fp64.cu", "nonlinear_static.cu", "fno.cu"]
 CPP_SOURCES = ["galerkin.cpp", "dump_io.cpp"]
 
 

@@ -8,6 +8,8 @@
 #include "step_kernels.cuh"
 #include "tracer_kernel.cuh"
 #include "update_kernel.cuh"
+#include "colloc_kernels.cuh"
+#include "solver_internal.h"
 
 #include <algorithm>
 #include <cmath>
@@ -1657,3 +1659,161 @@ rbc_status rbc_ensemble_step(rbc_ensemble* e, int nsteps)
 }
 
 } // extern "C"
+
+// ------------------------------------------------------------------ surrogate access
+// Library-internal functions of solver_internal.h (used by fno.cu).
+namespace rbcint {
+
+GridDesc grid(const rbc_handle* h)
+{
+    GridDesc d;
+    d.nx = h->G.nx;
+    d.ny = h->G.ny;
+    d.L = h->G.L;
+    d.ckeep = h->G.ckeep;
+    d.device = h->prm.device;
+    d.lx = h->G.lx;
+    d.ly = h->G.ly;
+    d.dt = h->G.dt;
+    d.ra = h->prm.ra;
+    d.pr = h->prm.pr;
+    d.mixed = h->mixed;
+    return d;
+}
+
+cudaStream_t stream(const rbc_handle* h) { return h->stream; }
+
+void set_error(rbc_handle* h, const char* msg)
+{
+    if (h) h->last_error = msg;
+}
+
+template <typename R, int L> static void encode_L(rbc_handle* h, int nq, const double* basis, float* out)
+{
+    const int P = h->G.P;
+    k_colloc_encode<R, L><<<(P + 255) / 256, 256, 0, h->stream>>>((const R*)h->phys, P, nq, basis, out);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+template <typename R> static void encode_t(rbc_handle* h, int nq, const double* basis, float* out)
+{
+    run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
+    switch (h->G.L) {
+    case 2: encode_L<R, 2>(h, nq, basis, out); break;
+    case 3: encode_L<R, 3>(h, nq, basis, out); break;
+    case 4: encode_L<R, 4>(h, nq, basis, out); break;
+    case 5: encode_L<R, 5>(h, nq, basis, out); break;
+    case 6: encode_L<R, 6>(h, nq, basis, out); break;
+    case 8: encode_L<R, 8>(h, nq, basis, out); break;
+    case 12: encode_L<R, 12>(h, nq, basis, out); break;
+    default: throw ArgError{"unsupported number of vertical modes"};
+    }
+}
+
+rbc_status colloc_encode(rbc_handle* h, int nq, const double* d_basis, float* d_out)
+{
+    if (!d_basis || !d_out || !h || nq < h->G.L) return fail(h, RBC_ERR_INVALID_ARG, "bad collocation arguments");
+    RBC_GUARD(h)
+    if (h->mixed) encode_t<float>(h, nq, d_basis, d_out);
+    else encode_t<double>(h, nq, d_basis, d_out);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+size_t colloc_scratch_bytes(const rbc_handle* h)
+{
+    const Geom& G = h->G;
+    return (size_t)4 * G.L * G.P * sizeof(double) + (size_t)4 * G.L * G.ckeep * G.ny * sizeof(double2);
+}
+
+template <int L> static void add_L(rbc_handle* h, int nq, const double* proj, const float* delta, void* scratch)
+{
+    const Geom& G = h->G;
+    double* planes = static_cast<double*>(scratch);
+    double2* rows = reinterpret_cast<double2*>(planes + (size_t)4 * L * G.P);
+    k_colloc_project<L><<<(G.P + 255) / 256, 256, 0, h->stream>>>(delta, G.P, nq, proj, planes);
+    RBC_CUDA(cudaGetLastError());
+    const size_t sm_row = (size_t)G.nx * (sizeof(double2) + sizeof(double));
+    k_colloc_row_dft<<<4 * L * G.ny, 128, sm_row, h->stream>>>(planes, G.nx, G.ny, G.ckeep, h->twx, rows);
+    RBC_CUDA(cudaGetLastError());
+    const size_t sm_col = (size_t)5 * G.ny * sizeof(double2);
+    if (sm_col > 48 * 1024)
+        RBC_CUDA(cudaFuncSetAttribute(k_colloc_assemble<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_col));
+    k_colloc_assemble<L><<<dim3(G.ckeep, L), 256, sm_col, h->stream>>>(rows, G, h->twy, h->th, h->f, h->g, h->FG);
+    RBC_CUDA(cudaGetLastError());
+    h->launches += 3;
+}
+
+rbc_status colloc_add(rbc_handle* h, int nq, const double* d_proj, const float* d_delta, void* d_scratch)
+{
+    if (!h || !d_proj || !d_delta || !d_scratch || nq < h->G.L)
+        return fail(h, RBC_ERR_INVALID_ARG, "bad collocation arguments");
+    RBC_GUARD(h)
+    flush_tracers(h); // a pending tracer advance uses the velocity of the state before the change
+    switch (h->G.L) {
+    case 2: add_L<2>(h, nq, d_proj, d_delta, d_scratch); break;
+    case 3: add_L<3>(h, nq, d_proj, d_delta, d_scratch); break;
+    case 4: add_L<4>(h, nq, d_proj, d_delta, d_scratch); break;
+    case 5: add_L<5>(h, nq, d_proj, d_delta, d_scratch); break;
+    case 6: add_L<6>(h, nq, d_proj, d_delta, d_scratch); break;
+    case 8: add_L<8>(h, nq, d_proj, d_delta, d_scratch); break;
+    case 12: add_L<12>(h, nq, d_proj, d_delta, d_scratch); break;
+    default: throw ArgError{"unsupported number of vertical modes"};
+    }
+    h->have_hist = false;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+size_t state_bytes(const rbc_handle* h)
+{
+    return ((size_t)3 * h->G.L * h->G.ckp * h->G.ny + 2 * (size_t)h->G.L) * sizeof(double2);
+}
+
+rbc_status state_save(rbc_handle* h, void* d_dst)
+{
+    if (!h || !d_dst) return fail(h, RBC_ERR_INVALID_ARG, "null buffer");
+    RBC_GUARD(h)
+    const size_t pl = (size_t)h->G.L * h->G.ckp * h->G.ny;
+    double2* d = static_cast<double2*>(d_dst);
+    RBC_CUDA(cudaMemcpyAsync(d, h->th, pl * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    RBC_CUDA(cudaMemcpyAsync(d + pl, h->f, pl * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    RBC_CUDA(cudaMemcpyAsync(d + 2 * pl, h->g, pl * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    RBC_CUDA(cudaMemcpyAsync(d + 3 * pl, h->FG, 2 * h->G.L * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status state_load(rbc_handle* h, const void* d_src)
+{
+    if (!h || !d_src) return fail(h, RBC_ERR_INVALID_ARG, "null buffer");
+    RBC_GUARD(h)
+    flush_tracers(h);
+    const size_t pl = (size_t)h->G.L * h->G.ckp * h->G.ny;
+    const double2* s = static_cast<const double2*>(d_src);
+    RBC_CUDA(cudaMemcpyAsync(h->th, s, pl * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    RBC_CUDA(cudaMemcpyAsync(h->f, s + pl, pl * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    RBC_CUDA(cudaMemcpyAsync(h->g, s + 2 * pl, pl * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    RBC_CUDA(cudaMemcpyAsync(h->FG, s + 3 * pl, 2 * h->G.L * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    h->have_hist = false;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status nu_wall(rbc_handle* h, double* nu)
+{
+    if (!h || !nu) return fail(h, RBC_ERR_INVALID_ARG, "null output");
+    RBC_GUARD(h)
+    const int L = h->G.L;
+    std::vector<double2> t(L);
+    RBC_CUDA(cudaMemcpy2DAsync(t.data(), sizeof(double2), h->th, (size_t)h->G.ckp * h->G.ny * sizeof(double2),
+                               sizeof(double2), L, cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    double v = 1.0;
+    for (int k = 0; k < L; ++k) v -= (k + 1) * kPi * t[k].x;
+    *nu = v;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+} // namespace rbcint

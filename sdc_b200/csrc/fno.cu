@@ -1,0 +1,923 @@
+// fno.cu -- learned surrogate of the RBC step: a Fourier neural operator (FNO) that
+// advances the solver state by one surrogate interval (many plain steps) at a time, its
+// training on snapshot pairs the solver generates, and a rollout in which the plain IMEX
+// step checks the surrogate's Nusselt number and spectrum and takes over when they drift.
+// No reference counterpart (jceyy/sdc has no learned component).
+//
+// Network (FNO-2d over the horizontal plane; the nq collocation levels of the four
+// fields theta, u, v, w are its C = 4 nq channels, channel = field * nq + level):
+//   h0 = x P^T + p                                   lift C -> W
+//   h_{l+1} = act(h_l W_l^T + b_l + K_l(h_l))         l = 0 .. nl-1, act = GELU except last
+//   K_l(h) = irfft2(R_l * rfft2(h) on kx < m, ky in [0, m) U [-m, 0))
+//   y = GELU(h_nl Q1^T + q1) Q2^T + q2                project W -> H -> C
+// y is the normalized increment of the collocation fields over one interval. The
+// truncated transforms are products with fixed DFT matrices (Fx, Fy forward, Gy, Gx
+// inverse), so every contraction runs as a BF16 GEMM with FP32 accumulation; activations
+// are stored in BF16, pre-activations, the loss and the optimizer in FP32.
+//
+// Parameter vector (FP32, this order): P [W][C], p [W]; per layer W_l [W][W], b_l [W],
+// R_l [2m][m][2][W][W] (ky index, kx, re/im, in, out); Q1 [H][W], q1 [H]; Q2 [C][H], q2 [C].
+#include "rbc.h"
+#include "fno_kernels.cuh"
+#include "galerkin.h"
+#include "solver_internal.h"
+#include "splitmix.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace rbcfno;
+
+namespace {
+
+struct CudaErr {
+    cudaError_t e;
+    const char* what;
+};
+struct ArgErr {
+    std::string msg;
+};
+#define FNO_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) throw CudaErr{e_, #call};                                 \
+    } while (0)
+
+// float -> BF16 bits, round to nearest even (the conversion the kernels use).
+uint16_t bf16_bits(float f)
+{
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+} // namespace
+
+struct rbc_fno {
+    rbc_fno_params p{};
+    int C = 0, W = 0, m = 0, my = 0, H = 0, nl = 0, nx = 0, ny = 0, P = 0, B = 0;
+    std::string last_error;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> owned;
+    long long nparam = 0, oPw = 0, oPb = 0, oQ1w = 0, oQ1b = 0, oQ2w = 0, oQ2b = 0;
+    std::vector<long long> oW, ob, oR;
+    float *param = nullptr, *grad = nullptr, *am = nullptr, *av = nullptr;
+    bf16* pbf = nullptr;
+    long long adam_t = 0;
+    bf16 *FxT = nullptr, *FyB = nullptr, *GyB = nullptr, *GxT = nullptr;
+    float* norm = nullptr; // [5][C]: x mean, 1/x std, d mean, d std, 1/d std
+    std::vector<float> norm_h;
+    bool have_norm = false;
+    // activations
+    bf16* x0 = nullptr;
+    std::vector<bf16*> h;
+    std::vector<float*> pre;
+    std::vector<bf16*> Ahat;
+    bf16 *A1 = nullptr, *Yh = nullptr, *Z = nullptr, *q1 = nullptr;
+    float *Kv = nullptr, *q1pre = nullptr, *out = nullptr, *target = nullptr, *xf = nullptr;
+    // backward
+    bf16 *gA = nullptr, *gB = nullptr, *dZ = nullptr, *dY = nullptr, *dAh = nullptr, *dA1 = nullptr;
+    float *dhs = nullptr, *wpart = nullptr, *cpart = nullptr, *lpart = nullptr;
+    size_t wpart_n = 0;
+    int nsplit_max = 0, ncol_blocks = 0, nloss_blocks = 0;
+    double* dloss = nullptr;
+    int dloss_n = 0;
+    // solver coupling
+    double *basis = nullptr, *proj = nullptr;
+    void* dec = nullptr;
+    void* backup = nullptr;
+    size_t dec_bytes = 0, backup_bytes = 0;
+    float *xcol = nullptr, *delta = nullptr;
+    // snapshot store
+    float* store = nullptr;
+    int nslots = 0;
+    int *src_d = nullptr, *dst_d = nullptr, *perm_d = nullptr;
+    double* stat_part = nullptr;
+    int nstat_blocks = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+template <typename T> T* falloc(rbc_fno* f, size_t n)
+{
+    void* p = nullptr;
+    FNO_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    f->owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+rbc_status ffail(rbc_fno* f, rbc_status s, const std::string& m)
+{
+    if (f) f->last_error = m;
+    return s;
+}
+
+#define FNO_GUARD(f)                                                                     \
+    if (!f) return RBC_ERR_INVALID_ARG;                                                  \
+    try {                                                                                \
+        FNO_CUDA(cudaSetDevice(f->p.device));
+#define FNO_GUARD_END(f)                                                                 \
+    }                                                                                    \
+    catch (const CudaErr& e) {                                                           \
+        return ffail(f, e.e == cudaErrorMemoryAllocation ? RBC_ERR_OUT_OF_MEMORY : RBC_ERR_CUDA, \
+                     std::string(e.what) + ": " + cudaGetErrorString(e.e));              \
+    }                                                                                    \
+    catch (const ArgErr& e) {                                                            \
+        return ffail(f, RBC_ERR_INVALID_ARG, e.msg);                                     \
+    }
+
+int load_mode(const bf16* base, long long rs, long long cs, long long bs, int rows, long long K)
+{
+    const bool al = ((uintptr_t)base % 16) == 0;
+    if (cs == 1 && rs % 8 == 0 && bs % 8 == 0 && K % 8 == 0 && al) return 2;
+    if (rs == 1 && cs % 8 == 0 && bs % 8 == 0 && rows % 8 == 0 && al) return 3;
+    return rs == 1 ? 1 : 0;
+}
+
+void gemm(cudaStream_t s, GemmOp op)
+{
+    // split-K chunks start at multiples of K: 16-byte loads along k need K and ktot % 8 == 0
+    long long kchk = op.K;
+    if (op.ktot > 0) kchk = (op.K % 8 == 0 && op.ktot % 8 == 0) ? 8 : 1;
+    op.amode = load_mode(op.A, op.a_rs, op.a_cs, op.a_bs, op.M, kchk);
+    op.bmode = load_mode(op.B, op.b_cs, op.b_rs, op.b_bs, op.N, kchk);
+    if (op.batch < 1 || op.batch > 65535 || op.M < 1 || op.N < 1 || op.K < 1) throw ArgErr{"gemm shape"};
+    const int BN = op.N <= 32 ? 32 : 64;
+    const int BM = op.M <= 32 ? 32 : (BN == 32 && op.M >= 8192 ? 128 : 64);
+    dim3 grid((op.M + BM - 1) / BM, (op.N + BN - 1) / BN, op.batch);
+    if (grid.y > 65535) throw ArgErr{"gemm N too large"};
+    if (BM == 32 && BN == 32) k_gemm<32, 32><<<grid, 128, 0, s>>>(op);
+    else if (BM == 32) k_gemm<32, 64><<<grid, 128, 0, s>>>(op);
+    else if (BM == 64 && BN == 32) k_gemm<64, 32><<<grid, 128, 0, s>>>(op);
+    else if (BM == 64) k_gemm<64, 64><<<grid, 128, 0, s>>>(op);
+    else k_gemm<128, 32><<<grid, 128, 0, s>>>(op);
+    FNO_CUDA(cudaGetLastError());
+}
+
+int grid_1d(long long n, int threads = 256, int cap = 148 * 8)
+{
+    long long b = (n + threads - 1) / threads;
+    return (int)std::max<long long>(1, std::min<long long>(b, cap));
+}
+
+// dW[o][i] (grad + off) = sum_m G[m][o] X[m][i] over M rows: split-K GEMM into slices,
+// then the slices summed in order.
+void wgrad(rbc_fno* f, cudaStream_t s, const bf16* G, int No, const bf16* X, int Ni, long long M, long long off)
+{
+    long long Kc = (M + f->nsplit_max - 1) / f->nsplit_max;
+    Kc = std::max<long long>(256, (Kc + 31) / 32 * 32);
+    const int ns = (int)((M + Kc - 1) / Kc);
+    if ((size_t)ns * No * Ni > f->wpart_n) throw ArgErr{"weight-gradient scratch too small"};
+    GemmOp op;
+    op.A = G;
+    op.a_rs = 1;
+    op.a_cs = No;
+    op.a_bs = Kc * No;
+    op.B = X;
+    op.b_rs = Ni;
+    op.b_cs = 1;
+    op.b_bs = Kc * Ni;
+    op.M = No;
+    op.N = Ni;
+    op.K = (int)Kc;
+    op.ktot = M;
+    op.batch = ns;
+    op.c_rs = Ni;
+    op.c_cs = 1;
+    op.c_bs = (long long)No * Ni;
+    op.outf = f->wpart;
+    gemm(s, op);
+    k_sum_slices<<<grid_1d((long long)No * Ni), 256, 0, s>>>(f->wpart, ns, (long long)No * Ni, f->grad + off, 0);
+    FNO_CUDA(cudaGetLastError());
+}
+
+// grad[off + n] = sum_m X[m][n].
+void colsum(rbc_fno* f, cudaStream_t s, const bf16* X, long long M, int N, long long off)
+{
+    if (N > 256) throw ArgErr{"column sum wider than a block"};
+    const int nb = f->ncol_blocks;
+    const long long rpb = (M + nb - 1) / nb;
+    k_colsum_part<<<nb, 256, 0, s>>>(X, M, N, rpb, f->cpart);
+    FNO_CUDA(cudaGetLastError());
+    k_sum_slices<<<grid_1d(N), 256, 0, s>>>(f->cpart, nb, N, f->grad + off, 0);
+    FNO_CUDA(cudaGetLastError());
+}
+
+const bf16* pb(const rbc_fno* f, long long off) { return f->pbf + off; }
+
+// Forward pass of B samples from f->x0 into f->out (FP32 [B P C]).
+void forward(rbc_fno* f, int B, cudaStream_t s)
+{
+    const int W = f->W, m = f->m, my = f->my, nx = f->nx, ny = f->ny, C = f->C, H = f->H;
+    const long long M = (long long)B * f->P, mW = (long long)m * W;
+    GemmOp op;
+    // lift
+    op = GemmOp();
+    op.A = f->x0; op.a_rs = C; op.a_cs = 1;
+    op.B = pb(f, f->oPw); op.b_rs = 1; op.b_cs = C;
+    op.M = (int)M; op.N = W; op.K = C;
+    op.c_rs = W; op.bias = f->param + f->oPb; op.outb = f->h[0];
+    gemm(s, op);
+    for (int l = 0; l < f->nl; ++l) {
+        // x-DFT: per (b, y): A1[kr][c] = sum_x Fx[kr][x] h[x][c]
+        op = GemmOp();
+        op.A = f->FxT; op.a_rs = nx; op.a_cs = 1;
+        op.B = f->h[l]; op.b_rs = W; op.b_cs = 1; op.b_bs = (long long)nx * W;
+        op.M = 2 * m; op.N = W; op.K = nx; op.batch = B * ny;
+        op.c_rs = W; op.c_bs = 2LL * m * W; op.outb = f->A1;
+        gemm(s, op);
+        // y-DFT: per b: Ahat[(ky, ri)][(kx, c)] = sum_(y, ri') Fy A1
+        op = GemmOp();
+        op.A = f->FyB; op.a_rs = 2 * ny; op.a_cs = 1;
+        op.B = f->A1; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * ny * mW;
+        op.M = 2 * my; op.N = (int)mW; op.K = 2 * ny; op.batch = B;
+        op.c_rs = mW; op.c_bs = 2LL * my * mW; op.outb = f->Ahat[l];
+        gemm(s, op);
+        // per-mode channel mixing
+        const size_t smf = (size_t)(2 * W * W + (128 / W) * 2 * W) * sizeof(float);
+        k_modemix_fwd<<<my * m, 128, smf, s>>>(f->Ahat[l], pb(f, f->oR[l]), f->Yh, B, m, W);
+        FNO_CUDA(cudaGetLastError());
+        // inverse y
+        op = GemmOp();
+        op.A = f->GyB; op.a_rs = 2 * my; op.a_cs = 1;
+        op.B = f->Yh; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * my * mW;
+        op.M = 2 * ny; op.N = (int)mW; op.K = 2 * my; op.batch = B;
+        op.c_rs = mW; op.c_bs = 2LL * ny * mW; op.outb = f->Z;
+        gemm(s, op);
+        // inverse x (FP32 result, added in the pointwise epilogue)
+        op = GemmOp();
+        op.A = f->GxT; op.a_rs = 2 * m; op.a_cs = 1;
+        op.B = f->Z; op.b_rs = W; op.b_cs = 1; op.b_bs = 2LL * m * W;
+        op.M = nx; op.N = W; op.K = 2 * m; op.batch = B * ny;
+        op.c_rs = W; op.c_bs = (long long)nx * W; op.outf = f->Kv;
+        gemm(s, op);
+        // pointwise map + spectral part + bias, activation
+        op = GemmOp();
+        op.A = f->h[l]; op.a_rs = W; op.a_cs = 1;
+        op.B = pb(f, f->oW[l]); op.b_rs = 1; op.b_cs = W;
+        op.M = (int)M; op.N = W; op.K = W;
+        op.c_rs = W; op.bias = f->param + f->ob[l]; op.add = f->Kv; op.pre = f->pre[l];
+        op.act = l + 1 < f->nl ? ACT_GELU : ACT_NONE; op.outb = f->h[l + 1];
+        gemm(s, op);
+    }
+    op = GemmOp();
+    op.A = f->h[f->nl]; op.a_rs = W; op.a_cs = 1;
+    op.B = pb(f, f->oQ1w); op.b_rs = 1; op.b_cs = W;
+    op.M = (int)M; op.N = H; op.K = W;
+    op.c_rs = H; op.bias = f->param + f->oQ1b; op.pre = f->q1pre; op.act = ACT_GELU; op.outb = f->q1;
+    gemm(s, op);
+    op = GemmOp();
+    op.A = f->q1; op.a_rs = H; op.a_cs = 1;
+    op.B = pb(f, f->oQ2w); op.b_rs = 1; op.b_cs = H;
+    op.M = (int)M; op.N = C; op.K = H;
+    op.c_rs = C; op.bias = f->param + f->oQ2b; op.outf = f->out;
+    gemm(s, op);
+}
+
+// Loss of f->out against f->target (B samples) into dloss[idx]; gradient into f->grad.
+void loss_backward(rbc_fno* f, int B, cudaStream_t s, int idx)
+{
+    const int W = f->W, m = f->m, my = f->my, nx = f->nx, ny = f->ny, C = f->C, H = f->H;
+    const long long M = (long long)B * f->P, mW = (long long)m * W, n = M * C;
+    k_mse<<<f->nloss_blocks, 256, 0, s>>>(f->out, f->target, n, f->gA, f->lpart);
+    FNO_CUDA(cudaGetLastError());
+    k_loss_final<<<1, 32, 0, s>>>(f->lpart, f->nloss_blocks, n, f->dloss, idx);
+    FNO_CUDA(cudaGetLastError());
+    // projection
+    wgrad(f, s, f->gA, C, f->q1, H, M, f->oQ2w);
+    colsum(f, s, f->gA, M, C, f->oQ2b);
+    GemmOp op;
+    op.A = f->gA; op.a_rs = C; op.a_cs = 1;
+    op.B = pb(f, f->oQ2w); op.b_rs = H; op.b_cs = 1;
+    op.M = (int)M; op.N = H; op.K = C;
+    op.c_rs = H; op.act = ACT_GELU_BWD; op.aux = f->q1pre; op.outb = f->gB;
+    gemm(s, op);
+    wgrad(f, s, f->gB, H, f->h[f->nl], W, M, f->oQ1w);
+    colsum(f, s, f->gB, M, H, f->oQ1b);
+    op = GemmOp();
+    op.A = f->gB; op.a_rs = H; op.a_cs = 1;
+    op.B = pb(f, f->oQ1w); op.b_rs = W; op.b_cs = 1;
+    op.M = (int)M; op.N = W; op.K = H;
+    op.c_rs = W; op.outb = f->gA;
+    gemm(s, op);
+    bf16* gp = f->gA;
+    bf16* gn = f->gB;
+    for (int l = f->nl - 1; l >= 0; --l) {
+        wgrad(f, s, gp, W, f->h[l], W, M, f->oW[l]);
+        colsum(f, s, gp, M, W, f->ob[l]);
+        // adjoint of the inverse x transform
+        op = GemmOp();
+        op.A = f->GxT; op.a_rs = 1; op.a_cs = 2 * m;
+        op.B = gp; op.b_rs = W; op.b_cs = 1; op.b_bs = (long long)nx * W;
+        op.M = 2 * m; op.N = W; op.K = nx; op.batch = B * ny;
+        op.c_rs = W; op.c_bs = 2LL * m * W; op.outb = f->dZ;
+        gemm(s, op);
+        // adjoint of the inverse y transform
+        op = GemmOp();
+        op.A = f->GyB; op.a_rs = 1; op.a_cs = 2 * my;
+        op.B = f->dZ; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * ny * mW;
+        op.M = 2 * my; op.N = (int)mW; op.K = 2 * ny; op.batch = B;
+        op.c_rs = mW; op.c_bs = 2LL * my * mW; op.outb = f->dY;
+        gemm(s, op);
+        const size_t smb = (size_t)(2 * W * W + 4 * W) * sizeof(float);
+        k_modemix_bwd<<<my * m, 256, smb, s>>>(f->Ahat[l], pb(f, f->oR[l]), f->dY, f->dAh, f->grad + f->oR[l], B,
+                                                m, W);
+        FNO_CUDA(cudaGetLastError());
+        // adjoint of the forward y transform
+        op = GemmOp();
+        op.A = f->FyB; op.a_rs = 1; op.a_cs = 2 * ny;
+        op.B = f->dAh; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * my * mW;
+        op.M = 2 * ny; op.N = (int)mW; op.K = 2 * my; op.batch = B;
+        op.c_rs = mW; op.c_bs = 2LL * ny * mW; op.outb = f->dA1;
+        gemm(s, op);
+        // adjoint of the forward x transform (FP32)
+        op = GemmOp();
+        op.A = f->FxT; op.a_rs = 1; op.a_cs = nx;
+        op.B = f->dA1; op.b_rs = W; op.b_cs = 1; op.b_bs = 2LL * m * W;
+        op.M = nx; op.N = W; op.K = 2 * m; op.batch = B * ny;
+        op.c_rs = W; op.c_bs = (long long)nx * W; op.outf = f->dhs;
+        gemm(s, op);
+        // adjoint of the pointwise map, plus the spectral part, times GELU' of the layer below
+        op = GemmOp();
+        op.A = gp; op.a_rs = W; op.a_cs = 1;
+        op.B = pb(f, f->oW[l]); op.b_rs = W; op.b_cs = 1;
+        op.M = (int)M; op.N = W; op.K = W;
+        op.c_rs = W; op.add = f->dhs;
+        if (l > 0) {
+            op.act = ACT_GELU_BWD;
+            op.aux = f->pre[l - 1];
+        }
+        op.outb = gn;
+        gemm(s, op);
+        std::swap(gp, gn);
+    }
+    wgrad(f, s, gp, W, f->x0, C, M, f->oPw);
+    colsum(f, s, gp, M, W, f->oPb);
+}
+
+void cast_params(rbc_fno* f, cudaStream_t s)
+{
+    k_cast_bf16<<<grid_1d(f->nparam), 256, 0, s>>>(f->param, f->pbf, f->nparam);
+    FNO_CUDA(cudaGetLastError());
+}
+
+void check_solver(const rbc_fno* f, const rbc_handle* h)
+{
+    const rbcint::GridDesc g = rbcint::grid(h);
+    if (g.nx != f->nx || g.ny != f->ny || g.L != f->p.nz) throw ArgErr{"solver grid does not match the surrogate"};
+    if (g.device != f->p.device) throw ArgErr{"solver and surrogate are on different devices"};
+}
+
+void check_status(rbc_status st, rbc_handle* h)
+{
+    if (st != RBC_OK) throw ArgErr{std::string("solver: ") + rbc_last_error(h)};
+}
+
+// One surrogate interval on the solver's stream: encode, network, decode into the state.
+void advance_once(rbc_fno* f, rbc_handle* h)
+{
+    cudaStream_t s = rbcint::stream(h);
+    check_status(rbcint::colloc_encode(h, f->p.nq, f->basis, f->xcol), h);
+    const int C = f->C;
+    k_normalize<<<grid_1d((long long)f->P * C), 256, 0, s>>>(f->xcol, f->P, C, f->norm, f->norm + C, f->x0);
+    FNO_CUDA(cudaGetLastError());
+    forward(f, 1, s);
+    k_denormalize<<<grid_1d((long long)f->P * C), 256, 0, s>>>(f->out, f->P, C, f->norm + 2 * C, f->norm + 3 * C,
+                                                               f->delta);
+    FNO_CUDA(cudaGetLastError());
+    check_status(rbcint::colloc_add(h, f->p.nq, f->proj, f->delta, f->dec), h);
+}
+
+void build_dft(rbc_fno* f)
+{
+    const int m = f->m, my = f->my, nx = f->nx, ny = f->ny;
+    std::vector<uint16_t> Fx((size_t)2 * m * nx), Fy((size_t)2 * my * 2 * ny), Gy((size_t)2 * ny * 2 * my),
+        Gx((size_t)nx * 2 * m);
+    auto bb = [](double v) { return bf16_bits((float)v); };
+    for (int kx = 0; kx < m; ++kx)
+        for (int x = 0; x < nx; ++x) {
+            const double a = kTwoPi * (double)((long long)kx * x % nx) / nx;
+            Fx[(size_t)kx * nx + x] = bb(std::cos(a));
+            Fx[(size_t)(m + kx) * nx + x] = bb(-std::sin(a));
+            const double w = (kx == 0 ? 1.0 : 2.0) / ((double)nx * ny);
+            Gx[(size_t)x * 2 * m + kx] = bb(w * std::cos(a));
+            Gx[(size_t)x * 2 * m + m + kx] = bb(-w * std::sin(a));
+        }
+    for (int ki = 0; ki < my; ++ki) {
+        const int ky = ki < m ? ki : ki - my;
+        for (int y = 0; y < ny; ++y) {
+            const long long e = (((long long)ky * y) % ny + ny) % ny;
+            const double a = kTwoPi * (double)e / ny, c = std::cos(a), sn = std::sin(a);
+            // forward: rows (ky, ri'), columns (y, ri)
+            Fy[(size_t)(2 * ki) * 2 * ny + 2 * y] = bb(c);
+            Fy[(size_t)(2 * ki) * 2 * ny + 2 * y + 1] = bb(sn);
+            Fy[(size_t)(2 * ki + 1) * 2 * ny + 2 * y] = bb(-sn);
+            Fy[(size_t)(2 * ki + 1) * 2 * ny + 2 * y + 1] = bb(c);
+            // inverse: rows (y, ri), columns (ky, ri')
+            Gy[(size_t)(2 * y) * 2 * my + 2 * ki] = bb(c);
+            Gy[(size_t)(2 * y) * 2 * my + 2 * ki + 1] = bb(-sn);
+            Gy[(size_t)(2 * y + 1) * 2 * my + 2 * ki] = bb(sn);
+            Gy[(size_t)(2 * y + 1) * 2 * my + 2 * ki + 1] = bb(c);
+        }
+    }
+    f->FxT = falloc<bf16>(f, Fx.size());
+    f->FyB = falloc<bf16>(f, Fy.size());
+    f->GyB = falloc<bf16>(f, Gy.size());
+    f->GxT = falloc<bf16>(f, Gx.size());
+    FNO_CUDA(cudaMemcpy(f->FxT, Fx.data(), Fx.size() * 2, cudaMemcpyHostToDevice));
+    FNO_CUDA(cudaMemcpy(f->FyB, Fy.data(), Fy.size() * 2, cudaMemcpyHostToDevice));
+    FNO_CUDA(cudaMemcpy(f->GyB, Gy.data(), Gy.size() * 2, cudaMemcpyHostToDevice));
+    FNO_CUDA(cudaMemcpy(f->GxT, Gx.data(), Gx.size() * 2, cudaMemcpyHostToDevice));
+}
+
+void init_params(rbc_fno* f, std::vector<float>& v)
+{
+    v.assign(f->nparam, 0.0f);
+    uint64_t k = 0;
+    auto uni = [&](float bound) {
+        return (float)((2.0 * rbcrng::unit_open(rbcrng::stream_at(f->p.seed, k++)) - 1.0) * bound);
+    };
+    auto lin = [&](long long ow, long long ob, int out, int in) {
+        const float b = 1.0f / std::sqrt((float)in);
+        for (long long i = 0; i < (long long)out * in; ++i) v[ow + i] = uni(b);
+        for (int i = 0; i < out; ++i) v[ob + i] = uni(b);
+    };
+    lin(f->oPw, f->oPb, f->W, f->C);
+    for (int l = 0; l < f->nl; ++l) {
+        lin(f->oW[l], f->ob[l], f->W, f->W);
+        const float sc = 1.0f / ((float)f->W * f->W);
+        const long long nr = (long long)f->my * f->m * 2 * f->W * f->W;
+        for (long long i = 0; i < nr; ++i) v[f->oR[l] + i] = sc * (0.5f * (uni(1.0f) + 1.0f));
+    }
+    lin(f->oQ1w, f->oQ1b, f->H, f->W);
+    lin(f->oQ2w, f->oQ2b, f->C, f->H);
+}
+
+} // namespace
+
+extern "C" {
+
+rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out)
+{
+    if (!p || !out) return RBC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (p->nx < 8 || p->ny < 8 || p->nq < 1 || p->nz < 1 || p->nq < p->nz || p->width < 8 || p->width > 64 ||
+        p->width % 8 || p->modes < 1 || 2 * p->modes > p->nx - 2 || 2 * p->modes > p->ny || p->layers < 1 ||
+        p->hidden < 8 || p->hidden > 256 || p->max_batch < 1 || 4 * p->nq > 256)
+        return RBC_ERR_INVALID_ARG;
+    rbc_fno* f = new rbc_fno;
+    f->p = *p;
+    f->C = 4 * p->nq;
+    f->W = p->width;
+    f->m = p->modes;
+    f->my = 2 * p->modes;
+    f->H = p->hidden;
+    f->nl = p->layers;
+    f->nx = p->nx;
+    f->ny = p->ny;
+    f->P = p->nx * p->ny;
+    f->B = p->max_batch;
+    try {
+        FNO_CUDA(cudaSetDevice(p->device));
+        FNO_CUDA(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
+        FNO_CUDA(cudaEventCreate(&f->ev0));
+        FNO_CUDA(cudaEventCreate(&f->ev1));
+        const int W = f->W, C = f->C, H = f->H;
+        long long o = 0;
+        f->oPw = o; o += (long long)W * C;
+        f->oPb = o; o += W;
+        for (int l = 0; l < f->nl; ++l) {
+            f->oW.push_back(o); o += (long long)W * W;
+            f->ob.push_back(o); o += W;
+            f->oR.push_back(o); o += (long long)f->my * f->m * 2 * W * W;
+        }
+        f->oQ1w = o; o += (long long)H * W;
+        f->oQ1b = o; o += H;
+        f->oQ2w = o; o += (long long)C * H;
+        f->oQ2b = o; o += C;
+        f->nparam = o;
+        f->param = falloc<float>(f, o);
+        f->grad = falloc<float>(f, o);
+        f->am = falloc<float>(f, o);
+        f->av = falloc<float>(f, o);
+        f->pbf = falloc<bf16>(f, o);
+        std::vector<float> v;
+        init_params(f, v);
+        FNO_CUDA(cudaMemcpy(f->param, v.data(), o * sizeof(float), cudaMemcpyHostToDevice));
+        FNO_CUDA(cudaMemset(f->grad, 0, o * sizeof(float)));
+        FNO_CUDA(cudaMemset(f->am, 0, o * sizeof(float)));
+        FNO_CUDA(cudaMemset(f->av, 0, o * sizeof(float)));
+        cast_params(f, f->stream);
+        build_dft(f);
+        f->norm = falloc<float>(f, 5 * C);
+        f->norm_h.assign(5 * (size_t)C, 0.0f);
+        for (int c = 0; c < C; ++c) f->norm_h[C + c] = f->norm_h[3 * C + c] = f->norm_h[4 * C + c] = 1.0f;
+        FNO_CUDA(cudaMemcpy(f->norm, f->norm_h.data(), 5 * C * sizeof(float), cudaMemcpyHostToDevice));
+        // activations for max_batch samples
+        const long long M = (long long)f->B * f->P, mW = (long long)f->m * W;
+        f->x0 = falloc<bf16>(f, M * C);
+        f->xf = falloc<float>(f, M * C);
+        for (int l = 0; l <= f->nl; ++l) f->h.push_back(falloc<bf16>(f, M * W));
+        for (int l = 0; l < f->nl; ++l) {
+            f->pre.push_back(falloc<float>(f, M * W));
+            f->Ahat.push_back(falloc<bf16>(f, (long long)f->B * 2 * f->my * mW));
+        }
+        f->A1 = falloc<bf16>(f, (long long)f->B * 2 * f->ny * mW);
+        f->Yh = falloc<bf16>(f, (long long)f->B * 2 * f->my * mW);
+        f->Z = falloc<bf16>(f, (long long)f->B * 2 * f->ny * mW);
+        f->Kv = falloc<float>(f, M * W);
+        f->q1pre = falloc<float>(f, M * H);
+        f->q1 = falloc<bf16>(f, M * H);
+        f->out = falloc<float>(f, M * C);
+        f->target = falloc<float>(f, M * C);
+        const int gw = std::max({W, H, C});
+        f->gA = falloc<bf16>(f, M * gw);
+        f->gB = falloc<bf16>(f, M * gw);
+        f->dhs = falloc<float>(f, M * W);
+        f->dZ = falloc<bf16>(f, (long long)f->B * 2 * f->ny * mW);
+        f->dY = falloc<bf16>(f, (long long)f->B * 2 * f->my * mW);
+        f->dAh = falloc<bf16>(f, (long long)f->B * 2 * f->my * mW);
+        f->dA1 = falloc<bf16>(f, (long long)f->B * 2 * f->ny * mW);
+        f->nsplit_max = 148 * 4;
+        f->wpart_n = (size_t)(f->nsplit_max + 1) * std::max({(long long)W * C, (long long)W * W, (long long)H * W,
+                                                              (long long)C * H});
+        f->wpart = falloc<float>(f, f->wpart_n);
+        f->ncol_blocks = 148 * 2;
+        f->cpart = falloc<float>(f, (size_t)f->ncol_blocks * 256);
+        f->nloss_blocks = 148 * 4;
+        f->lpart = falloc<float>(f, f->nloss_blocks);
+        f->dloss_n = 1 << 16;
+        f->dloss = falloc<double>(f, f->dloss_n);
+        // solver coupling (grids with nz vertical modes)
+        rbchost::CollocTables ct;
+        if (!rbchost::colloc_tables(p->nz, p->nq, ct)) throw ArgErr{"collocation tables"};
+        std::vector<double> bas((size_t)p->nq * 3 * p->nz), prj((size_t)2 * p->nz * p->nq);
+        for (int q = 0; q < p->nq; ++q)
+            for (int mm = 0; mm < p->nz; ++mm) {
+                bas[((size_t)q * 3 + 0) * p->nz + mm] = ct.C[q * p->nz + mm];
+                bas[((size_t)q * 3 + 1) * p->nz + mm] = ct.Cp[q * p->nz + mm];
+                bas[((size_t)q * 3 + 2) * p->nz + mm] = ct.S[q * p->nz + mm];
+            }
+        std::copy(ct.Ps.begin(), ct.Ps.end(), prj.begin());
+        std::copy(ct.Pc.begin(), ct.Pc.end(), prj.begin() + (size_t)p->nz * p->nq);
+        f->basis = falloc<double>(f, bas.size());
+        f->proj = falloc<double>(f, prj.size());
+        FNO_CUDA(cudaMemcpy(f->basis, bas.data(), bas.size() * sizeof(double), cudaMemcpyHostToDevice));
+        FNO_CUDA(cudaMemcpy(f->proj, prj.data(), prj.size() * sizeof(double), cudaMemcpyHostToDevice));
+        const size_t mox = (size_t)p->nx / 2 + 1, ckp = ((mox + 3) / 4) * 4;
+        f->dec_bytes = (size_t)4 * p->nz * f->P * sizeof(double) + (size_t)4 * p->nz * mox * p->ny * 16;
+        f->dec = falloc<unsigned char>(f, f->dec_bytes);
+        f->backup_bytes = ((size_t)3 * p->nz * ckp * p->ny + 2 * (size_t)p->nz) * 16;
+        f->backup = falloc<unsigned char>(f, f->backup_bytes);
+        f->xcol = falloc<float>(f, (size_t)f->P * C);
+        f->delta = falloc<float>(f, (size_t)f->P * C);
+        FNO_CUDA(cudaStreamSynchronize(f->stream));
+    } catch (const CudaErr& e) {
+        for (void* q : f->owned) cudaFree(q);
+        const bool oom = e.e == cudaErrorMemoryAllocation;
+        delete f;
+        return oom ? RBC_ERR_OUT_OF_MEMORY : RBC_ERR_CUDA;
+    } catch (const ArgErr&) {
+        for (void* q : f->owned) cudaFree(q);
+        delete f;
+        return RBC_ERR_INVALID_ARG;
+    }
+    *out = f;
+    return RBC_OK;
+}
+
+void rbc_fno_destroy(rbc_fno* f)
+{
+    if (!f) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(f->p.device);
+    if (f->stream) cudaStreamSynchronize(f->stream);
+    for (void* q : f->owned) cudaFree(q);
+    if (f->stream) cudaStreamDestroy(f->stream);
+    if (f->ev0) cudaEventDestroy(f->ev0);
+    if (f->ev1) cudaEventDestroy(f->ev1);
+    cudaSetDevice(cur);
+    delete f;
+}
+
+const char* rbc_fno_last_error(const rbc_fno* f) { return f ? f->last_error.c_str() : "null surrogate"; }
+
+long long rbc_fno_num_params(const rbc_fno* f) { return f ? f->nparam : 0; }
+
+rbc_status rbc_fno_get_params(rbc_fno* f, float* out, long long n)
+{
+    if (!out || (f && n != f->nparam)) return ffail(f, RBC_ERR_INVALID_ARG, "parameter count");
+    FNO_GUARD(f)
+    FNO_CUDA(cudaStreamSynchronize(f->stream));
+    FNO_CUDA(cudaMemcpy(out, f->param, n * sizeof(float), cudaMemcpyDeviceToHost));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_set_params(rbc_fno* f, const float* in, long long n)
+{
+    if (!in || (f && n != f->nparam)) return ffail(f, RBC_ERR_INVALID_ARG, "parameter count");
+    FNO_GUARD(f)
+    FNO_CUDA(cudaStreamSynchronize(f->stream));
+    FNO_CUDA(cudaMemcpy(f->param, in, n * sizeof(float), cudaMemcpyHostToDevice));
+    FNO_CUDA(cudaMemset(f->am, 0, n * sizeof(float)));
+    FNO_CUDA(cudaMemset(f->av, 0, n * sizeof(float)));
+    f->adam_t = 0;
+    cast_params(f, f->stream);
+    FNO_CUDA(cudaStreamSynchronize(f->stream));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_get_norm(rbc_fno* f, float* out)
+{
+    if (!out) return ffail(f, RBC_ERR_INVALID_ARG, "null output");
+    FNO_GUARD(f)
+    const int C = f->C;
+    for (int c = 0; c < C; ++c) {
+        out[c] = f->norm_h[c];
+        out[C + c] = 1.0f / f->norm_h[C + c];
+        out[2 * C + c] = f->norm_h[2 * C + c];
+        out[3 * C + c] = f->norm_h[3 * C + c];
+    }
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_set_norm(rbc_fno* f, const float* in)
+{
+    if (!in) return ffail(f, RBC_ERR_INVALID_ARG, "null input");
+    FNO_GUARD(f)
+    const int C = f->C;
+    for (int c = 0; c < C; ++c)
+        if (!(in[C + c] > 0) || !(in[3 * C + c] > 0)) throw ArgErr{"standard deviations must be positive"};
+    for (int c = 0; c < C; ++c) {
+        f->norm_h[c] = in[c];
+        f->norm_h[C + c] = 1.0f / in[C + c];
+        f->norm_h[2 * C + c] = in[2 * C + c];
+        f->norm_h[3 * C + c] = in[3 * C + c];
+        f->norm_h[4 * C + c] = 1.0f / in[3 * C + c];
+    }
+    FNO_CUDA(cudaMemcpyAsync(f->norm, f->norm_h.data(), 5 * C * sizeof(float), cudaMemcpyHostToDevice, f->stream));
+    FNO_CUDA(cudaStreamSynchronize(f->stream));
+    f->have_norm = true;
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_forward(rbc_fno* f, const float* x, int batch, float* y)
+{
+    if (!x || !y || (f && (batch < 1 || batch > f->B))) return ffail(f, RBC_ERR_INVALID_ARG, "bad forward arguments");
+    FNO_GUARD(f)
+    const long long n = (long long)batch * f->P * f->C;
+    FNO_CUDA(cudaMemcpyAsync(f->xf, x, n * sizeof(float), cudaMemcpyHostToDevice, f->stream));
+    k_cast_bf16<<<grid_1d(n), 256, 0, f->stream>>>(f->xf, f->x0, n);
+    FNO_CUDA(cudaGetLastError());
+    forward(f, batch, f->stream);
+    FNO_CUDA(cudaMemcpyAsync(y, f->out, n * sizeof(float), cudaMemcpyDeviceToHost, f->stream));
+    FNO_CUDA(cudaStreamSynchronize(f->stream));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_loss_grad(rbc_fno* f, const float* x, const float* target, int batch, double* loss, float* grad)
+{
+    if (!x || !target || !loss || !grad || (f && (batch < 1 || batch > f->B)))
+        return ffail(f, RBC_ERR_INVALID_ARG, "bad gradient arguments");
+    FNO_GUARD(f)
+    const long long n = (long long)batch * f->P * f->C;
+    FNO_CUDA(cudaMemcpyAsync(f->xf, x, n * sizeof(float), cudaMemcpyHostToDevice, f->stream));
+    FNO_CUDA(cudaMemcpyAsync(f->target, target, n * sizeof(float), cudaMemcpyHostToDevice, f->stream));
+    k_cast_bf16<<<grid_1d(n), 256, 0, f->stream>>>(f->xf, f->x0, n);
+    FNO_CUDA(cudaGetLastError());
+    forward(f, batch, f->stream);
+    loss_backward(f, batch, f->stream, 0);
+    FNO_CUDA(cudaMemcpyAsync(loss, f->dloss, sizeof(double), cudaMemcpyDeviceToHost, f->stream));
+    FNO_CUDA(cudaMemcpyAsync(grad, f->grad, f->nparam * sizeof(float), cudaMemcpyDeviceToHost, f->stream));
+    FNO_CUDA(cudaStreamSynchronize(f->stream));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_colloc_get(rbc_fno* f, rbc_handle* h, float* out)
+{
+    if (!h || !out) return ffail(f, RBC_ERR_INVALID_ARG, "null argument");
+    FNO_GUARD(f)
+    check_solver(f, h);
+    check_status(rbcint::colloc_encode(h, f->p.nq, f->basis, f->xcol), h);
+    cudaStream_t s = rbcint::stream(h);
+    FNO_CUDA(cudaMemcpyAsync(out, f->xcol, (size_t)f->P * f->C * sizeof(float), cudaMemcpyDeviceToHost, s));
+    FNO_CUDA(cudaStreamSynchronize(s));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_colloc_add(rbc_fno* f, rbc_handle* h, const float* delta)
+{
+    if (!h || !delta) return ffail(f, RBC_ERR_INVALID_ARG, "null argument");
+    FNO_GUARD(f)
+    check_solver(f, h);
+    cudaStream_t s = rbcint::stream(h);
+    FNO_CUDA(cudaMemcpyAsync(f->delta, delta, (size_t)f->P * f->C * sizeof(float), cudaMemcpyHostToDevice, s));
+    check_status(rbcint::colloc_add(h, f->p.nq, f->proj, f->delta, f->dec), h);
+    FNO_CUDA(cudaStreamSynchronize(s));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_dataset_reserve(rbc_fno* f, int nslots)
+{
+    if (nslots < 2) return ffail(f, RBC_ERR_INVALID_ARG, "need at least two slots");
+    FNO_GUARD(f)
+    if (f->store) throw ArgErr{"the snapshot store is already reserved"};
+    f->store = falloc<float>(f, (size_t)nslots * f->P * f->C);
+    f->nslots = nslots;
+    f->src_d = falloc<int>(f, nslots);
+    f->dst_d = falloc<int>(f, nslots);
+    f->perm_d = falloc<int>(f, nslots);
+    f->nstat_blocks = 148 * 4;
+    f->stat_part = falloc<double>(f, (size_t)f->nstat_blocks * 4 * f->C);
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_dataset_capture(rbc_fno* f, rbc_handle* h, int slot)
+{
+    if (!h || (f && (slot < 0 || slot >= f->nslots))) return ffail(f, RBC_ERR_INVALID_ARG, "bad slot");
+    FNO_GUARD(f)
+    check_solver(f, h);
+    float* dst = f->store + (size_t)slot * f->P * f->C;
+    check_status(rbcint::colloc_encode(h, f->p.nq, f->basis, dst), h);
+    FNO_CUDA(cudaStreamSynchronize(rbcint::stream(h)));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs, int epochs, int batch, double lr,
+                         unsigned long long seed, int fit_norm, double* epoch_loss)
+{
+    if (!src || !dst || !epoch_loss || npairs < 1 || epochs < 0 || batch < 1 || !(lr > 0))
+        return ffail(f, RBC_ERR_INVALID_ARG, "bad training arguments");
+    FNO_GUARD(f)
+    if (!f->store || npairs > f->nslots) throw ArgErr{"pairs exceed the snapshot store"};
+    if (batch > f->B || batch > npairs) throw ArgErr{"batch larger than max_batch or the pair count"};
+    for (int i = 0; i < npairs; ++i)
+        if (src[i] < 0 || src[i] >= f->nslots || dst[i] < 0 || dst[i] >= f->nslots) throw ArgErr{"slot out of range"};
+    cudaStream_t s = f->stream;
+    const int C = f->C;
+    const long long P = f->P;
+    FNO_CUDA(cudaMemcpyAsync(f->src_d, src, npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+    FNO_CUDA(cudaMemcpyAsync(f->dst_d, dst, npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (fit_norm || !f->have_norm) {
+        const long long rows = (long long)npairs * P;
+        const long long rpb = (rows + f->nstat_blocks - 1) / f->nstat_blocks;
+        k_pair_stats<<<f->nstat_blocks, 256, 0, s>>>(f->store, P, C, f->src_d, f->dst_d, npairs, rpb, f->stat_part);
+        FNO_CUDA(cudaGetLastError());
+        std::vector<double> part((size_t)f->nstat_blocks * 4 * C);
+        FNO_CUDA(cudaMemcpyAsync(part.data(), f->stat_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FNO_CUDA(cudaStreamSynchronize(s));
+        std::vector<double> sum(4 * (size_t)C, 0.0);
+        for (int b = 0; b < f->nstat_blocks; ++b)
+            for (int k = 0; k < 4 * C; ++k) sum[k] += part[(size_t)b * 4 * C + k];
+        for (int c = 0; c < C; ++c) {
+            const double n = (double)rows;
+            const double xm = sum[c] / n, xv = std::max(0.0, sum[C + c] / n - xm * xm);
+            const double dm = sum[2 * C + c] / n, dv = std::max(0.0, sum[3 * C + c] / n - dm * dm);
+            const double xs = xv > 0 ? std::sqrt(xv) : 1.0, ds = dv > 0 ? std::sqrt(dv) : 1.0;
+            f->norm_h[c] = (float)xm;
+            f->norm_h[C + c] = (float)(1.0 / xs);
+            f->norm_h[2 * C + c] = (float)dm;
+            f->norm_h[3 * C + c] = (float)ds;
+            f->norm_h[4 * C + c] = (float)(1.0 / ds);
+        }
+        FNO_CUDA(cudaMemcpyAsync(f->norm, f->norm_h.data(), 5 * C * sizeof(float), cudaMemcpyHostToDevice, s));
+        f->have_norm = true;
+    }
+    const int iters = npairs / batch;
+    if (iters > f->dloss_n) throw ArgErr{"too many iterations per epoch"};
+    const long long total = (long long)iters * epochs;
+    std::vector<int> perm(npairs);
+    std::vector<double> lh(iters);
+    long long it_glob = 0;
+    for (int e = 0; e < epochs; ++e) {
+        for (int i = 0; i < npairs; ++i) perm[i] = i;
+        for (int i = npairs - 1; i > 0; --i) {
+            const uint64_t r = rbcrng::stream_at(seed + 0x9E37ULL * (uint64_t)(e + 1), (uint64_t)i);
+            const int j = (int)(r % (uint64_t)(i + 1));
+            std::swap(perm[i], perm[j]);
+        }
+        FNO_CUDA(cudaMemcpyAsync(f->perm_d, perm.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+        for (int it = 0; it < iters; ++it, ++it_glob) {
+            k_gather_pairs<<<grid_1d((long long)batch * P * C), 256, 0, s>>>(
+                f->store, P * C, f->src_d, f->dst_d, f->perm_d + (size_t)it * batch, batch, C, f->norm, f->norm + C,
+                f->norm + 2 * C, f->norm + 4 * C, f->x0, f->target);
+            FNO_CUDA(cudaGetLastError());
+            forward(f, batch, s);
+            loss_backward(f, batch, s, it);
+            // cosine decay from lr to lr / 50 over the run
+            const double frac = total > 1 ? (double)it_glob / (double)(total - 1) : 0.0;
+            const double lr_t = lr * (0.02 + 0.98 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * frac)));
+            ++f->adam_t;
+            const float b1 = 0.9f, b2 = 0.999f;
+            const float c1 = 1.0f - std::pow(b1, (float)f->adam_t), c2 = 1.0f - std::pow(b2, (float)f->adam_t);
+            k_adam<<<grid_1d(f->nparam), 256, 0, s>>>(f->param, f->grad, f->am, f->av, f->nparam, (float)lr_t, b1,
+                                                      b2, 1e-8f, c1, c2);
+            FNO_CUDA(cudaGetLastError());
+            cast_params(f, s);
+        }
+        FNO_CUDA(cudaMemcpyAsync(lh.data(), f->dloss, iters * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FNO_CUDA(cudaStreamSynchronize(s));
+        double m = 0;
+        for (double v : lh) m += v;
+        epoch_loss[e] = m / iters;
+    }
+    FNO_CUDA(cudaStreamSynchronize(s));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_fno_advance(rbc_fno* f, rbc_handle* h, int n)
+{
+    if (!h || n < 0) return ffail(f, RBC_ERR_INVALID_ARG, "bad advance arguments");
+    FNO_GUARD(f)
+    check_solver(f, h);
+    for (int i = 0; i < n; ++i) advance_once(f, h);
+    FNO_CUDA(cudaStreamSynchronize(rbcint::stream(h)));
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_params* sp, rbc_surrogate_report* rep)
+{
+    if (!h || !sp || !rep || sp->intervals < 0 || sp->steps_per_interval < 1 || sp->judge_every < 1 ||
+        !(sp->nu_tol > 0) || sp->spec_bins < 0 || sp->spec_bins > 4096)
+        return ffail(f, RBC_ERR_INVALID_ARG, "bad surrogate-run arguments");
+    FNO_GUARD(f)
+    check_solver(f, h);
+    std::memset(rep, 0, sizeof(*rep));
+    cudaStream_t s = rbcint::stream(h);
+    const int nb = sp->spec_bins;
+    std::vector<double> spec_s(nb), spec_p(nb);
+    FNO_CUDA(cudaEventRecord(f->ev0, s));
+    long long fallback_left = 0;
+    for (int t = 0; t < sp->intervals; ++t) {
+        if (fallback_left != 0) {
+            check_status(rbc_step_async(h, sp->steps_per_interval), h);
+            ++rep->plain_intervals;
+            if (fallback_left > 0) --fallback_left;
+            continue;
+        }
+        if ((t + 1) % sp->judge_every != 0) {
+            advance_once(f, h);
+            ++rep->surrogate_intervals;
+            continue;
+        }
+        // check: the surrogate and the plain step over the same interval from one state
+        check_status(rbcint::state_save(h, f->backup), h);
+        advance_once(f, h);
+        double nu_s = 0, nu_p = 0;
+        check_status(rbcint::nu_wall(h, &nu_s), h);
+        if (nb > 0) check_status(rbc_spectrum(h, 0.0, spec_s.data(), nb), h);
+        check_status(rbcint::state_load(h, f->backup), h);
+        check_status(rbc_step_async(h, sp->steps_per_interval), h);
+        check_status(rbcint::nu_wall(h, &nu_p), h);
+        if (nb > 0) check_status(rbc_spectrum(h, 0.0, spec_p.data(), nb), h);
+        const double enu = std::fabs(nu_s - nu_p) / std::max(std::fabs(nu_p), 1e-300);
+        double num = 0, den = 0;
+        for (int i = 0; i < nb; ++i) {
+            num += (spec_s[i] - spec_p[i]) * (spec_s[i] - spec_p[i]);
+            den += spec_p[i] * spec_p[i];
+        }
+        const double esp = nb > 0 && den > 0 ? std::sqrt(num / den) : 0.0;
+        ++rep->checks;
+        ++rep->plain_intervals;
+        rep->last_nu_err = enu;
+        rep->last_spec_err = esp;
+        rep->max_nu_err = std::max(rep->max_nu_err, enu);
+        rep->max_spec_err = std::max(rep->max_spec_err, esp);
+        const bool bad = !(enu <= sp->nu_tol) || (sp->spec_tol > 0 && nb > 0 && !(esp <= sp->spec_tol));
+        if (bad) {
+            ++rep->fallbacks;
+            fallback_left = sp->fallback_intervals < 0 ? -1 : sp->fallback_intervals;
+        }
+    }
+    FNO_CUDA(cudaEventRecord(f->ev1, s));
+    FNO_CUDA(cudaEventSynchronize(f->ev1));
+    float ms = 0;
+    FNO_CUDA(cudaEventElapsedTime(&ms, f->ev0, f->ev1));
+    rep->ms = ms;
+    check_status(rbc_synchronize(h), h);
+    return RBC_OK;
+    FNO_GUARD_END(f)
+}
+
+} // extern "C"

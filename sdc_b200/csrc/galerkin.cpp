@@ -167,6 +167,46 @@ void build_tables(int L, Tables& T)
     int3(0, 3, 4, T.Ia12);
 }
 
+static bool ls_inverse(int nq, int L, const std::vector<double>& B, std::vector<double>& P)
+{
+    std::vector<double> N((size_t)L * L, 0.0), Ni;
+    for (int a = 0; a < L; ++a)
+        for (int b = 0; b < L; ++b) {
+            long double s = 0;
+            for (int q = 0; q < nq; ++q) s += (long double)B[q * L + a] * B[q * L + b];
+            N[a * L + b] = (double)s;
+        }
+    if (!lu_invert(L, N, Ni)) return false;
+    P.assign((size_t)L * nq, 0.0);
+    for (int m = 0; m < L; ++m)
+        for (int q = 0; q < nq; ++q) {
+            long double s = 0;
+            for (int a = 0; a < L; ++a) s += (long double)Ni[m * L + a] * B[q * L + a];
+            P[m * nq + q] = (double)s;
+        }
+    return true;
+}
+
+bool colloc_tables(int L, int nq, CollocTables& t)
+{
+    if (L < 1 || nq < L) return false;
+    t.L = L;
+    t.nq = nq;
+    std::vector<double> w;
+    composite_gl(1, nq, t.z, w);
+    std::sort(t.z.begin(), t.z.end());
+    t.C.resize((size_t)nq * L);
+    t.Cp.resize((size_t)nq * L);
+    t.S.resize((size_t)nq * L);
+    for (int q = 0; q < nq; ++q)
+        for (int m = 0; m < L; ++m) {
+            t.C[q * L + m] = basis(0, m, t.z[q]);
+            t.Cp[q * L + m] = basis(1, m, t.z[q]);
+            t.S[q * L + m] = basis(3, m, t.z[q]);
+        }
+    return ls_inverse(nq, L, t.S, t.Ps) && ls_inverse(nq, L, t.C, t.Pc);
+}
+
 double family_value(const Tables& T, int f, int i, int j, int k)
 {
     using namespace rbcprog;

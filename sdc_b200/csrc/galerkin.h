@@ -62,6 +62,15 @@ void pattern_theta(const GridInfo& g, int type, double mode, double amp, uint64_
 // Forward real 2-D FFT (unnormalised, e^{-i}) of real[ny][nx] into out[ny][nx/2+1]
 // (interleaved complex); nx, ny = 2^a 3^b.
 void rfft2(int nx, int ny, const double* real, double* out);
+// Collocation levels of the surrogate: the nq Gauss-Legendre nodes z_q on (-1/2, 1/2),
+// the basis values there (C, C', S at [q][m]) and the least-squares inverses of the
+// S and C samples (Ps, Pc at [m][q]: (B^T B)^-1 B^T for B[q][m] = S_m(z_q) or C_m(z_q)),
+// which recover the L mode amplitudes of any field that lies in the span exactly.
+struct CollocTables {
+    int L = 0, nq = 0;
+    std::vector<double> z, C, Cp, S, Ps, Pc;
+};
+bool colloc_tables(int L, int nq, CollocTables& t);
 // Tracer start patterns of particle_tracer::init_positions (rbc_tracer_init types).
 void tracer_pattern(int type, uint64_t seed, int n, double lx, double ly, double cx, double cy, double cz,
                     double sigma, double* xyz);
