@@ -310,7 +310,7 @@ long long rbc_kernel_launches(const rbc_handle* h);
 /* --- learned surrogate ----------------------------------------------------------- */
 /* No counterpart in the reference (jceyy/sdc has no learned component). A Fourier neural
  * operator over the horizontal plane advances a solver's state by one surrogate interval
- * (steps_per_interval plain steps) at a time. Its input and output are the collocation
+ * (interval_steps plain steps) at a time. Its input and output are the collocation
  * fields theta, u, v, w at the nq Gauss-Legendre levels z_q of (-1/2, 1/2): FP32
  * [ny][nx][4 nq], channel = field * nq + q. The network predicts their normalized
  * increment; the increment is projected back onto (theta, f, g, F, G) by least squares
@@ -329,6 +329,12 @@ typedef struct {
     int max_batch;     /* largest training batch */
     int device;
     unsigned long long seed; /* weight initialisation (SplitMix64) */
+    int interval_steps;      /* plain steps one application of the network replaces */
+    int physics_mean;        /* 1: after the network, the horizontal-mean modes (theta_k at
+                                q = 0, F_k, G_k; they set Nu_wall) are advanced by the plain
+                                step's own q = 0 recursion over interval_steps steps, forced by
+                                the solver's nonlinear operator at the interval start (linear
+                                in time with the previous interval's); 0: from the network */
 } rbc_fno_params;
 rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out);
 void rbc_fno_destroy(rbc_fno* m);
@@ -357,18 +363,25 @@ rbc_status rbc_fno_dataset_capture(rbc_fno* m, rbc_handle* h, int slot);
  * the normalization from these pairs. epoch_loss[e] = mean loss of epoch e. */
 rbc_status rbc_fno_train(rbc_fno* m, const int* src, const int* dst, int npairs, int epochs, int batch, double lr,
                          unsigned long long seed, int fit_norm, double* epoch_loss);
+/* Options of later rbc_fno_train calls. augment: 0 none; 1 each training pair mapped by
+ * a random reflection of the periodic box (x -> -x and/or y -> -y, velocities as
+ * vectors); 2 also the transpose x <-> y (square boxes: nx == ny and Lx == Ly). With
+ * augmentation the normalization gives the velocity channels mean 0 (and, with 2, one
+ * shared std). noise_rel > 0 adds N(0, (noise_rel * increment std)^2) noise per channel
+ * to each training input and trains toward the true next state from the noisy one, so
+ * that the network pulls drifted states back during a rollout. */
+rbc_status rbc_fno_set_train_options(rbc_fno* m, int augment, double noise_rel);
 /* n surrogate intervals of the solver's state. */
 rbc_status rbc_fno_advance(rbc_fno* m, rbc_handle* h, int n);
 
 /* Rollout with the plain step as judge: every judge_every-th interval the surrogate and
- * the plain step (steps_per_interval steps) each advance the same state; the rollout
+ * the plain step (interval_steps steps) each advance the same state; the rollout
  * keeps the plain result and compares Nu_wall (relative error) and the theta spectrum at
  * z = 0 (relative L2 error over spec_bins bins; 0 bins or spec_tol <= 0: not checked).
  * When an error exceeds its tolerance the plain step takes over for fallback_intervals
  * intervals (-1: the rest of the run). */
 typedef struct {
     int intervals;
-    int steps_per_interval;
     int judge_every;
     double nu_tol;
     double spec_tol;
@@ -380,7 +393,9 @@ typedef struct {
     double max_nu_err, max_spec_err, last_nu_err, last_spec_err;
     double ms;         /* device time of the rollout (CUDA events on the solver's stream) */
 } rbc_surrogate_report;
-rbc_status rbc_surrogate_run(rbc_fno* m, rbc_handle* h, const rbc_surrogate_params* p, rbc_surrogate_report* rep);
+/* nu_trace (may be NULL; at most 65536 intervals): Nu_wall after every interval. */
+rbc_status rbc_surrogate_run(rbc_fno* m, rbc_handle* h, const rbc_surrogate_params* p, rbc_surrogate_report* rep,
+                             double* nu_trace);
 
 #ifdef __cplusplus
 }

@@ -43,11 +43,11 @@ class _FnoParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nq", ctypes.c_int),
                 ("width", ctypes.c_int), ("modes", ctypes.c_int), ("layers", ctypes.c_int),
                 ("hidden", ctypes.c_int), ("max_batch", ctypes.c_int), ("device", ctypes.c_int),
-                ("seed", ctypes.c_ulonglong)]
+                ("seed", ctypes.c_ulonglong), ("interval_steps", ctypes.c_int), ("physics_mean", ctypes.c_int)]
 
 
 class _SurrogateParams(ctypes.Structure):
-    _fields_ = [("intervals", ctypes.c_int), ("steps_per_interval", ctypes.c_int), ("judge_every", ctypes.c_int),
+    _fields_ = [("intervals", ctypes.c_int), ("judge_every", ctypes.c_int),
                 ("nu_tol", ctypes.c_double), ("spec_tol", ctypes.c_double), ("spec_bins", ctypes.c_int),
                 ("fallback_intervals", ctypes.c_int)]
 
@@ -75,7 +75,8 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_init_pattern", "rbc_fno_create", "rbc_fno_destroy", "rbc_fno_last_error", "rbc_fno_num_params",
            "rbc_fno_get_params", "rbc_fno_set_params", "rbc_fno_get_norm", "rbc_fno_set_norm", "rbc_fno_forward",
            "rbc_fno_loss_grad", "rbc_fno_colloc_get", "rbc_fno_colloc_add", "rbc_fno_dataset_reserve",
-           "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run"]
+           "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run",
+           "rbc_fno_set_train_options"]
 INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
 TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
@@ -165,7 +166,8 @@ def lib():
     L.rbc_fno_train.argtypes = [vp, ip, ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                 ctypes.c_ulonglong, ctypes.c_int, _dp]
     L.rbc_fno_advance.argtypes = [vp, vp, ctypes.c_int]
-    L.rbc_surrogate_run.argtypes = [vp, vp, ctypes.POINTER(_SurrogateParams), ctypes.POINTER(_SurrogateReport)]
+    L.rbc_fno_set_train_options.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.rbc_surrogate_run.argtypes = [vp, vp, ctypes.POINTER(_SurrogateParams), ctypes.POINTER(_SurrogateReport), _dp]
     _LIB = L
     return L
 
@@ -464,10 +466,13 @@ class FNO:
     Channels are theta, u, v, w at nq collocation levels (C = 4 nq); arrays are float32
     [batch][ny][nx][C]."""
 
-    def __init__(self, nx, ny, nz, nq, width=32, modes=16, layers=4, hidden=128, max_batch=8, device=0, seed=0):
+    def __init__(self, nx, ny, nz, nq, width=32, modes=16, layers=4, hidden=128, max_batch=8, device=0, seed=0,
+                 interval_steps=40, physics_mean=True):
         self.nx, self.ny, self.nz, self.nq = nx, ny, nz, nq
         self.C = 4 * nq
-        p = _FnoParams(nx, ny, nz, nq, width, modes, layers, hidden, max_batch, device, seed)
+        self.interval_steps = interval_steps
+        p = _FnoParams(nx, ny, nz, nq, width, modes, layers, hidden, max_batch, device, seed, interval_steps,
+                       int(physics_mean))
         m = ctypes.c_void_p()
         st = lib().rbc_fno_create(ctypes.byref(p), ctypes.byref(m))
         if st != RBC_OK:
@@ -546,13 +551,23 @@ class FNO:
                                         batch, lr, seed, int(fit_norm), loss.ctypes.data_as(_dp)))
         return loss[:epochs]
 
+    def set_train_options(self, augment=0, noise_rel=0.0):
+        """augment: 0 none, 1 reflections, 2 reflections + transpose (square boxes)."""
+        self._check(lib().rbc_fno_set_train_options(self.m, augment, noise_rel))
+
     def advance(self, solver, n=1):
         self._check(lib().rbc_fno_advance(self.m, solver.h, n))
 
-    def run(self, solver, intervals, steps_per_interval, judge_every=10, nu_tol=1e-3, spec_tol=0.0, spec_bins=0,
-            fallback_intervals=-1):
-        p = _SurrogateParams(intervals, steps_per_interval, judge_every, nu_tol, spec_tol, spec_bins,
-                             fallback_intervals)
+    def run(self, solver, intervals, judge_every=10, nu_tol=1e-3, spec_tol=0.0, spec_bins=0, fallback_intervals=-1,
+            trace=False):
+        """Judged rollout (rbc_surrogate_run); with trace=True the report's "nu_trace" is
+        Nu_wall after every interval."""
+        p = _SurrogateParams(intervals, judge_every, nu_tol, spec_tol, spec_bins, fallback_intervals)
         r = _SurrogateReport()
-        self._check(lib().rbc_surrogate_run(self.m, solver.h, ctypes.byref(p), ctypes.byref(r)))
-        return {k: getattr(r, k) for k, _ in _SurrogateReport._fields_}
+        tr = np.zeros(max(intervals, 1)) if trace else None
+        self._check(lib().rbc_surrogate_run(self.m, solver.h, ctypes.byref(p), ctypes.byref(r),
+                                            tr.ctypes.data_as(_dp) if trace else None))
+        out = {k: getattr(r, k) for k, _ in _SurrogateReport._fields_}
+        if trace:
+            out["nu_trace"] = tr[:intervals]
+        return out

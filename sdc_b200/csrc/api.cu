@@ -12,6 +12,7 @@
 #include "solver_internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -60,6 +61,7 @@ bool fft_len_ok(int n)
 // ------------------------------------------------------------------ handle
 struct rbc_handle {
     rbc_params prm{};
+    unsigned long long uid = 0;   // unique per handle in the process (never reused)
     rbchost::GridInfo gi;
     rbchost::Tables tab;
     Geom G{};
@@ -711,6 +713,10 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
     if (!L_supported(p->nz, p->form == RBC_FORM_MIXED)) return RBC_ERR_UNSUPPORTED;
     rbc_handle* h = new rbc_handle;
     h->prm = *p;
+    {
+        static std::atomic<unsigned long long> next_uid{1};
+        h->uid = next_uid++;
+    }
     h->mixed = p->form == RBC_FORM_MIXED;
     if (p->diag_capacity > 0) h->ring_cap = p->diag_capacity;
     try {
@@ -1682,6 +1688,9 @@ GridDesc grid(const rbc_handle* h)
 }
 
 cudaStream_t stream(const rbc_handle* h) { return h->stream; }
+unsigned long long uid(const rbc_handle* h) { return h->uid; }
+bool has_tracers(const rbc_handle* h) { return h->ntr > 0; }
+void state_changed(rbc_handle* h) { h->have_hist = false; }
 
 void set_error(rbc_handle* h, const char* msg)
 {
@@ -1716,6 +1725,89 @@ rbc_status colloc_encode(rbc_handle* h, int nq, const double* d_basis, float* d_
     RBC_GUARD(h)
     if (h->mixed) encode_t<float>(h, nq, d_basis, d_out);
     else encode_t<double>(h, nq, d_basis, d_out);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+// Mean-mode forcing of the current state: g = (2 Re N_theta_k(q=0), 2 Pr NF_k, 2 Pr NG_k),
+// the q = 0 terms that the update kernel adds (inverse B of the nonlinear term), and the
+// current mean modes y0 = (Re theta_k(q=0), F_k, G_k).
+template <typename C>
+__global__ void k_mean_forcing(const C* __restrict__ N, const double* __restrict__ NFG,
+                               const double2* __restrict__ th, const double2* __restrict__ FG, size_t plane, int L,
+                               double pr, double* __restrict__ g, double* __restrict__ y0)
+{
+    const int k = threadIdx.x;
+    if (k >= L) return;
+    g[k] = 2.0 * (double)N[(size_t)k * plane].x;
+    g[L + k] = 2.0 * pr * NFG[k];
+    g[2 * L + k] = 2.0 * pr * NFG[L + k];
+    y0[k] = th[(size_t)k * plane].x;
+    y0[L + k] = FG[k].x;
+    y0[2 * L + k] = FG[L + k].x;
+}
+
+// nsub steps of the plain step's recursion for the mean modes (q = 0: theta_k, F_k, G_k
+// decouple from everything else): y <- (y + dt (1.5 g_s - 0.5 g_{s-1})) / (1 + dt a),
+// a = ((k+1) pi)^2 for theta and Pr ((k+1) pi)^2 for F, G, with the forcing g_s taken
+// linear in time through g0 (interval start) and gp (start of the previous interval,
+// nsub steps earlier); without gp the forcing is constant and the first step is Euler.
+__global__ void k_mean_advance(double2* __restrict__ th, double2* __restrict__ FG, size_t plane, int L,
+                               const double* __restrict__ y0, const double* __restrict__ g0,
+                               const double* __restrict__ gp, int nsub, double dt, double pr)
+{
+    const int i = threadIdx.x;
+    if (i >= 3 * L) return;
+    const int kind = i / L, k = i - kind * L;
+    const double mpi = (k + 1) * kPi;
+    const double a = (kind ? pr : 1.0) * mpi * mpi;
+    const double fac = 1.0 / (1.0 + dt * a);
+    const double slope = gp ? (g0[i] - gp[i]) / nsub : 0.0;
+    double y = y0[i], gprev = g0[i] - slope;
+    for (int s = 0; s < nsub; ++s) {
+        const double gs = g0[i] + slope * s;
+        const double incr = (gp || s > 0) ? 1.5 * gs - 0.5 * gprev : gs;
+        y = (y + dt * incr) * fac;
+        gprev = gs;
+    }
+    if (kind == 0) th[(size_t)k * plane] = make_double2(y, 0.0);
+    else FG[(kind - 1) * L + k] = make_double2(y, 0.0);
+}
+
+template <typename R> static void encode_forcing_t(rbc_handle* h, int nq, const double* basis, float* out, double* g,
+                                                   double* y0)
+{
+    typedef typename cplx_t<R>::type C;
+    encode_t<R>(h, nq, basis, out);
+    run_analysis<R>(h, h->G);
+    k_mean_forcing<C><<<1, 32, 0, h->stream>>>((const C*)h->N, h->NFG, h->th, h->FG, (size_t)h->G.ckp * h->G.ny,
+                                                h->G.L, h->G.pr, g, y0);
+    RBC_CUDA(cudaGetLastError());
+    h->launches += 1;
+}
+
+rbc_status colloc_encode_forcing(rbc_handle* h, int nq, const double* d_basis, float* d_out, double* d_g,
+                                 double* d_y0)
+{
+    if (!d_basis || !d_out || !d_g || !d_y0 || !h || nq < h->G.L)
+        return fail(h, RBC_ERR_INVALID_ARG, "bad collocation arguments");
+    RBC_GUARD(h)
+    flush_tracers(h); // a pending tracer advance runs on the current state first
+    if (h->mixed) encode_forcing_t<float>(h, nq, d_basis, d_out, d_g, d_y0);
+    else encode_forcing_t<double>(h, nq, d_basis, d_out, d_g, d_y0);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status mean_advance(rbc_handle* h, const double* d_y0, const double* d_g0, const double* d_gp, int nsub)
+{
+    if (!h || !d_y0 || !d_g0 || nsub < 1 || 3 * h->G.L > 64) return fail(h, RBC_ERR_INVALID_ARG, "bad mean-mode arguments");
+    RBC_GUARD(h)
+    k_mean_advance<<<1, 64, 0, h->stream>>>(h->th, h->FG, (size_t)h->G.ckp * h->G.ny, h->G.L, d_y0, d_g0, d_gp, nsub,
+                                            h->G.dt, h->G.pr);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+    h->have_hist = false;
     return RBC_OK;
     RBC_GUARD_END(h)
 }
@@ -1796,6 +1888,25 @@ rbc_status state_load(rbc_handle* h, const void* d_src)
     RBC_CUDA(cudaMemcpyAsync(h->g, s + 2 * pl, pl * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
     RBC_CUDA(cudaMemcpyAsync(h->FG, s + 3 * pl, 2 * h->G.L * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
     h->have_hist = false;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+__global__ void k_nu_wall_record(const double2* __restrict__ th, size_t plane, int L, double* __restrict__ out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double v = 1.0;
+        for (int k = 0; k < L; ++k) v -= (k + 1) * kPi * th[(size_t)k * plane].x;
+        *out = v;
+    }
+}
+
+rbc_status nu_wall_record(rbc_handle* h, double* d_out)
+{
+    if (!h || !d_out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
+    RBC_GUARD(h)
+    k_nu_wall_record<<<1, 32, 0, h->stream>>>(h->th, (size_t)h->G.ckp * h->G.ny, h->G.L, d_out);
+    RBC_CUDA(cudaGetLastError());
     return RBC_OK;
     RBC_GUARD_END(h)
 }

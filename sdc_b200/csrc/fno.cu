@@ -98,7 +98,23 @@ struct rbc_fno {
     // snapshot store
     float* store = nullptr;
     int nslots = 0;
-    int *src_d = nullptr, *dst_d = nullptr, *perm_d = nullptr;
+    int *src_d = nullptr, *dst_d = nullptr, *perm_d = nullptr, *sym_d = nullptr;
+    int augment = 0;          // training with the box's horizontal symmetries
+    float noise_rel = 0.0f;   // input noise, relative to each channel's increment std
+    double* trace = nullptr;  // per-interval Nu_wall of a rollout (device)
+    int trace_n = 0;
+    // mean modes advanced by the plain recursion: forcing now / one interval earlier, start values
+    double *g_now = nullptr, *g_prev = nullptr, *y0 = nullptr;
+    bool have_prev = false;
+    // executable graphs of one surrogate interval, per (solver, forcing buffers)
+    struct AdvGraph {
+        unsigned long long solver;
+        const double* g_now;
+        bool prev;
+        cudaGraphExec_t exec;
+    };
+    std::vector<AdvGraph> graphs;
+    bool use_graphs = true;
     double* stat_part = nullptr;
     int nstat_blocks = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -381,11 +397,18 @@ void check_status(rbc_status st, rbc_handle* h)
     if (st != RBC_OK) throw ArgErr{std::string("solver: ") + rbc_last_error(h)};
 }
 
-// One surrogate interval on the solver's stream: encode, network, decode into the state.
-void advance_once(rbc_fno* f, rbc_handle* h)
+// One surrogate interval on the solver's stream (advance_body: device work only; host
+// bookkeeping in advance_once): encode, network, decode into the state.
+// With physics_mean the horizontal-mean modes (theta_k(q=0), F_k, G_k, which set Nu_wall)
+// are then replaced by interval_steps recursions of the plain step's own q = 0 update,
+// forced by the solver's nonlinear operator at this and the previous interval's start.
+void advance_body(rbc_fno* f, rbc_handle* h)
 {
     cudaStream_t s = rbcint::stream(h);
-    check_status(rbcint::colloc_encode(h, f->p.nq, f->basis, f->xcol), h);
+    if (f->p.physics_mean)
+        check_status(rbcint::colloc_encode_forcing(h, f->p.nq, f->basis, f->xcol, f->g_now, f->y0), h);
+    else
+        check_status(rbcint::colloc_encode(h, f->p.nq, f->basis, f->xcol), h);
     const int C = f->C;
     k_normalize<<<grid_1d((long long)f->P * C), 256, 0, s>>>(f->xcol, f->P, C, f->norm, f->norm + C, f->x0);
     FNO_CUDA(cudaGetLastError());
@@ -394,6 +417,54 @@ void advance_once(rbc_fno* f, rbc_handle* h)
                                                                f->delta);
     FNO_CUDA(cudaGetLastError());
     check_status(rbcint::colloc_add(h, f->p.nq, f->proj, f->delta, f->dec), h);
+    if (f->p.physics_mean)
+        check_status(rbcint::mean_advance(h, f->y0, f->g_now, f->have_prev ? f->g_prev : nullptr, f->p.interval_steps),
+                     h);
+}
+
+void drop_graphs(rbc_fno* f)
+{
+    for (auto& g : f->graphs) cudaGraphExecDestroy(g.exec);
+    f->graphs.clear();
+}
+
+void advance_once(rbc_fno* f, rbc_handle* h)
+{
+    cudaStream_t s = rbcint::stream(h);
+    // one interval is ~40 kernel launches: replayed from an executable graph captured
+    // the first time for this solver and forcing-buffer order (a solver with tracers, or
+    // the legacy default stream, runs them directly)
+    if (f->use_graphs && s != nullptr && !rbcint::has_tracers(h)) {
+        const unsigned long long id = rbcint::uid(h);
+        cudaGraphExec_t exec = nullptr;
+        for (auto& g : f->graphs)
+            if (g.solver == id && g.g_now == f->g_now && g.prev == f->have_prev) exec = g.exec;
+        if (!exec) {
+            if (f->graphs.size() >= 16) drop_graphs(f);
+            cudaGraph_t graph = nullptr;
+            FNO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                advance_body(f, h);
+            } catch (...) {
+                cudaStreamEndCapture(s, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            FNO_CUDA(cudaStreamEndCapture(s, &graph));
+            const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            FNO_CUDA(e);
+            f->graphs.push_back({id, f->g_now, f->have_prev, exec});
+        }
+        FNO_CUDA(cudaGraphLaunch(exec, s));
+        rbcint::state_changed(h);
+    } else {
+        advance_body(f, h);
+    }
+    if (f->p.physics_mean) {
+        std::swap(f->g_now, f->g_prev);
+        f->have_prev = true;
+    }
 }
 
 void build_dft(rbc_fno* f)
@@ -471,7 +542,8 @@ rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out)
     *out = nullptr;
     if (p->nx < 8 || p->ny < 8 || p->nq < 1 || p->nz < 1 || p->nq < p->nz || p->width < 8 || p->width > 64 ||
         p->width % 8 || p->modes < 1 || 2 * p->modes > p->nx - 2 || 2 * p->modes > p->ny || p->layers < 1 ||
-        p->hidden < 8 || p->hidden > 256 || p->max_batch < 1 || 4 * p->nq > 256)
+        p->hidden < 8 || p->hidden > 256 || p->max_batch < 1 || 4 * p->nq > 256 || p->interval_steps < 1 ||
+        3 * p->nz > 64)
         return RBC_ERR_INVALID_ARG;
     rbc_fno* f = new rbc_fno;
     f->p = *p;
@@ -577,6 +649,11 @@ rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out)
         f->dec = falloc<unsigned char>(f, f->dec_bytes);
         f->backup_bytes = ((size_t)3 * p->nz * ckp * p->ny + 2 * (size_t)p->nz) * 16;
         f->backup = falloc<unsigned char>(f, f->backup_bytes);
+        f->g_now = falloc<double>(f, 3 * (size_t)p->nz);
+        f->g_prev = falloc<double>(f, 3 * (size_t)p->nz);
+        f->y0 = falloc<double>(f, 3 * (size_t)p->nz);
+        f->trace_n = 1 << 16;
+        f->trace = falloc<double>(f, f->trace_n);
         f->xcol = falloc<float>(f, (size_t)f->P * C);
         f->delta = falloc<float>(f, (size_t)f->P * C);
         FNO_CUDA(cudaStreamSynchronize(f->stream));
@@ -601,6 +678,8 @@ void rbc_fno_destroy(rbc_fno* f)
     cudaGetDevice(&cur);
     cudaSetDevice(f->p.device);
     if (f->stream) cudaStreamSynchronize(f->stream);
+    cudaDeviceSynchronize();
+    drop_graphs(f);
     for (void* q : f->owned) cudaFree(q);
     if (f->stream) cudaStreamDestroy(f->stream);
     if (f->ev0) cudaEventDestroy(f->ev0);
@@ -744,6 +823,7 @@ rbc_status rbc_fno_dataset_reserve(rbc_fno* f, int nslots)
     f->src_d = falloc<int>(f, nslots);
     f->dst_d = falloc<int>(f, nslots);
     f->perm_d = falloc<int>(f, nslots);
+    f->sym_d = falloc<int>(f, nslots);
     f->nstat_blocks = 148 * 4;
     f->stat_part = falloc<double>(f, (size_t)f->nstat_blocks * 4 * f->C);
     return RBC_OK;
@@ -788,14 +868,31 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
         std::vector<double> sum(4 * (size_t)C, 0.0);
         for (int b = 0; b < f->nstat_blocks; ++b)
             for (int k = 0; k < 4 * C; ++k) sum[k] += part[(size_t)b * 4 * C + k];
+        // per-channel mean and std; with symmetry augmentation the velocity channels have
+        // mean 0 (a flip reverses them) and, with the transpose, u and v share one std
+        const int nq = f->p.nq;
+        const double n = (double)rows;
+        std::vector<double> mean(2 * (size_t)C), sec(2 * (size_t)C);
         for (int c = 0; c < C; ++c) {
-            const double n = (double)rows;
-            const double xm = sum[c] / n, xv = std::max(0.0, sum[C + c] / n - xm * xm);
-            const double dm = sum[2 * C + c] / n, dv = std::max(0.0, sum[3 * C + c] / n - dm * dm);
+            mean[c] = sum[c] / n;
+            sec[c] = sum[C + c] / n;
+            mean[C + c] = sum[2 * C + c] / n;
+            sec[C + c] = sum[3 * C + c] / n;
+        }
+        if (f->augment)
+            for (int q = 0; q < nq; ++q)
+                for (int k = 0; k < 2; ++k) {
+                    const int cu = k * C + nq + q, cv = k * C + 2 * nq + q;
+                    mean[cu] = mean[cv] = 0.0;
+                    if (f->augment == 2) sec[cu] = sec[cv] = 0.5 * (sec[cu] + sec[cv]);
+                }
+        for (int c = 0; c < C; ++c) {
+            const double xv = std::max(0.0, sec[c] - mean[c] * mean[c]);
+            const double dv = std::max(0.0, sec[C + c] - mean[C + c] * mean[C + c]);
             const double xs = xv > 0 ? std::sqrt(xv) : 1.0, ds = dv > 0 ? std::sqrt(dv) : 1.0;
-            f->norm_h[c] = (float)xm;
+            f->norm_h[c] = (float)mean[c];
             f->norm_h[C + c] = (float)(1.0 / xs);
-            f->norm_h[2 * C + c] = (float)dm;
+            f->norm_h[2 * C + c] = (float)mean[C + c];
             f->norm_h[3 * C + c] = (float)ds;
             f->norm_h[4 * C + c] = (float)(1.0 / ds);
         }
@@ -805,7 +902,7 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
     const int iters = npairs / batch;
     if (iters > f->dloss_n) throw ArgErr{"too many iterations per epoch"};
     const long long total = (long long)iters * epochs;
-    std::vector<int> perm(npairs);
+    std::vector<int> perm(npairs), symv(npairs, 0);
     std::vector<double> lh(iters);
     long long it_glob = 0;
     for (int e = 0; e < epochs; ++e) {
@@ -816,10 +913,20 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
             std::swap(perm[i], perm[j]);
         }
         FNO_CUDA(cudaMemcpyAsync(f->perm_d, perm.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+        if (f->augment) {
+            const int nsym = f->augment == 2 ? 8 : 4;
+            for (int i = 0; i < npairs; ++i) {
+                const uint64_t r = rbcrng::stream_at(seed ^ 0x5EEDULL, (uint64_t)e * npairs + i);
+                symv[i] = nsym == 8 ? (int)(r % 8) : (int)(r % 4) * 2;
+            }
+            FNO_CUDA(cudaMemcpyAsync(f->sym_d, symv.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+        }
         for (int it = 0; it < iters; ++it, ++it_glob) {
             k_gather_pairs<<<grid_1d((long long)batch * P * C), 256, 0, s>>>(
-                f->store, P * C, f->src_d, f->dst_d, f->perm_d + (size_t)it * batch, batch, C, f->norm, f->norm + C,
-                f->norm + 2 * C, f->norm + 4 * C, f->x0, f->target);
+                f->store, f->nx, f->ny, f->p.nq, f->src_d, f->dst_d, f->perm_d + (size_t)it * batch,
+                f->augment ? f->sym_d + (size_t)it * batch : nullptr, batch, f->norm, f->norm + C,
+                f->norm + 2 * C, f->norm + 3 * C, f->norm + 4 * C, f->noise_rel,
+                rbcrng::mix64(seed ^ (0xA5A5ULL + (uint64_t)it_glob)), f->x0, f->target);
             FNO_CUDA(cudaGetLastError());
             forward(f, batch, s);
             loss_backward(f, batch, s, it);
@@ -845,21 +952,34 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
     FNO_GUARD_END(f)
 }
 
+rbc_status rbc_fno_set_train_options(rbc_fno* f, int augment, double noise_rel)
+{
+    if (!f) return RBC_ERR_INVALID_ARG;
+    if (augment < 0 || augment > 2 || (augment == 2 && f->nx != f->ny) || !(noise_rel >= 0) || noise_rel > 10)
+        return ffail(f, RBC_ERR_INVALID_ARG, "bad training options");
+    f->augment = augment;
+    f->noise_rel = (float)noise_rel;
+    return RBC_OK;
+}
+
 rbc_status rbc_fno_advance(rbc_fno* f, rbc_handle* h, int n)
 {
     if (!h || n < 0) return ffail(f, RBC_ERR_INVALID_ARG, "bad advance arguments");
     FNO_GUARD(f)
     check_solver(f, h);
+    f->have_prev = false;
     for (int i = 0; i < n; ++i) advance_once(f, h);
     FNO_CUDA(cudaStreamSynchronize(rbcint::stream(h)));
     return RBC_OK;
     FNO_GUARD_END(f)
 }
 
-rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_params* sp, rbc_surrogate_report* rep)
+rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_params* sp, rbc_surrogate_report* rep,
+                             double* nu_trace)
 {
-    if (!h || !sp || !rep || sp->intervals < 0 || sp->steps_per_interval < 1 || sp->judge_every < 1 ||
-        !(sp->nu_tol > 0) || sp->spec_bins < 0 || sp->spec_bins > 4096)
+    if (!h || !sp || !rep || sp->intervals < 0 || sp->judge_every < 1 ||
+        !(sp->nu_tol > 0) || sp->spec_bins < 0 || sp->spec_bins > 4096 ||
+        (f && nu_trace && sp->intervals > f->trace_n))
         return ffail(f, RBC_ERR_INVALID_ARG, "bad surrogate-run arguments");
     FNO_GUARD(f)
     check_solver(f, h);
@@ -869,16 +989,21 @@ rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_para
     std::vector<double> spec_s(nb), spec_p(nb);
     FNO_CUDA(cudaEventRecord(f->ev0, s));
     long long fallback_left = 0;
+    const int nstep = f->p.interval_steps;
+    f->have_prev = false;
     for (int t = 0; t < sp->intervals; ++t) {
         if (fallback_left != 0) {
-            check_status(rbc_step_async(h, sp->steps_per_interval), h);
+            check_status(rbc_step_async(h, nstep), h);
             ++rep->plain_intervals;
+            f->have_prev = false;
             if (fallback_left > 0) --fallback_left;
+            if (nu_trace) check_status(rbcint::nu_wall_record(h, f->trace + t), h);
             continue;
         }
         if ((t + 1) % sp->judge_every != 0) {
             advance_once(f, h);
             ++rep->surrogate_intervals;
+            if (nu_trace) check_status(rbcint::nu_wall_record(h, f->trace + t), h);
             continue;
         }
         // check: the surrogate and the plain step over the same interval from one state
@@ -888,7 +1013,8 @@ rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_para
         check_status(rbcint::nu_wall(h, &nu_s), h);
         if (nb > 0) check_status(rbc_spectrum(h, 0.0, spec_s.data(), nb), h);
         check_status(rbcint::state_load(h, f->backup), h);
-        check_status(rbc_step_async(h, sp->steps_per_interval), h);
+        check_status(rbc_step_async(h, nstep), h);
+        f->have_prev = false;
         check_status(rbcint::nu_wall(h, &nu_p), h);
         if (nb > 0) check_status(rbc_spectrum(h, 0.0, spec_p.data(), nb), h);
         const double enu = std::fabs(nu_s - nu_p) / std::max(std::fabs(nu_p), 1e-300);
@@ -909,6 +1035,7 @@ rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_para
             ++rep->fallbacks;
             fallback_left = sp->fallback_intervals < 0 ? -1 : sp->fallback_intervals;
         }
+        if (nu_trace) check_status(rbcint::nu_wall_record(h, f->trace + t), h);
     }
     FNO_CUDA(cudaEventRecord(f->ev1, s));
     FNO_CUDA(cudaEventSynchronize(f->ev1));
@@ -916,6 +1043,8 @@ rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_para
     FNO_CUDA(cudaEventElapsedTime(&ms, f->ev0, f->ev1));
     rep->ms = ms;
     check_status(rbc_synchronize(h), h);
+    if (nu_trace && sp->intervals > 0)
+        FNO_CUDA(cudaMemcpy(nu_trace, f->trace, sp->intervals * sizeof(double), cudaMemcpyDeviceToHost));
     return RBC_OK;
     FNO_GUARD_END(f)
 }

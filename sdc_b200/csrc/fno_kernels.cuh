@@ -12,6 +12,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include "splitmix.h"
+
 namespace rbcfno {
 
 typedef __nv_bfloat16 bf16;
@@ -398,23 +400,51 @@ __global__ void k_denormalize(const float* __restrict__ y, long long M, int C, c
 }
 
 // Training batch from the snapshot store: for batch entry b the pair (src, dst) =
-// (slots[perm[b]], slots2[perm[b]]): x = normalized snapshot src (BF16), target =
-// normalized increment dst - src (FP32). Snapshots are FP32 [nslot][P][C].
-__global__ void k_gather_pairs(const float* __restrict__ store, long long snap, const int* __restrict__ src,
-                               const int* __restrict__ dst, const int* __restrict__ perm, int nb, int C,
-                               const float* __restrict__ xm, const float* __restrict__ xis,
-                               const float* __restrict__ dm, const float* __restrict__ dis, bf16* __restrict__ x,
-                               float* __restrict__ target)
+// (slots[perm[b]], slots2[perm[b]]). Snapshots are FP32 [nslot][ny][nx][C] with channel
+// field * nq + level, fields theta, u, v, w. Entry b is first mapped by the horizontal
+// symmetry sym[b] of the periodic box (bit 0: transpose x <-> y, square boxes only;
+// bit 1: x -> -x; bit 2: y -> -y); velocities transform as vectors: with M the point map,
+// u_out(p) = M^T u_in(M p), i.e. (fx v, fy u) under the transpose and (fx u, fy v)
+// otherwise, fx, fy = -1 for a flipped direction. Then x = normalized (snapshot src + e)
+// (BF16) and target = normalized increment dst - (src + e) (FP32), e = noise_rel * std of
+// the channel's increment * N(0,1) (SplitMix64 + Box-Muller on element index i of this
+// batch with seed nseed; noise_rel = 0: no noise).
+__global__ void k_gather_pairs(const float* __restrict__ store, int nx, int ny, int nq, const int* __restrict__ src,
+                               const int* __restrict__ dst, const int* __restrict__ perm, const int* __restrict__ sym,
+                               int nb, const float* __restrict__ xm, const float* __restrict__ xis,
+                               const float* __restrict__ dm, const float* __restrict__ ds,
+                               const float* __restrict__ dis, float noise_rel, unsigned long long nseed,
+                               bf16* __restrict__ x, float* __restrict__ target)
 {
+    const int C = 4 * nq;
+    const long long snap = (long long)nx * ny * C;
     const long long n = (long long)nb * snap;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int b = (int)(i / snap);
         const long long e = i - (long long)b * snap;
         const int c = (int)(e % C);
+        const long long p = e / C;
+        const int y = (int)(p / nx), xx = (int)(p - (long long)y * nx);
+        const int sy = sym ? sym[b] : 0;
+        const int y1 = (sy & 4) ? (ny - y) % ny : y, x1 = (sy & 2) ? (nx - xx) % nx : xx;
+        const int ys = (sy & 1) ? x1 : y1, xs = (sy & 1) ? y1 : x1;
+        const int fo = c / nq, q = c - fo * nq;
+        int fi = fo;
+        float sgn = 1.0f;
+        if (fo == 1) { fi = (sy & 1) ? 2 : 1; sgn = (sy & 2) ? -1.0f : 1.0f; }
+        else if (fo == 2) { fi = (sy & 1) ? 1 : 2; sgn = (sy & 4) ? -1.0f : 1.0f; }
+        const long long es = ((long long)ys * nx + xs) * C + fi * nq + q;
         const int pi = perm[b];
-        const float a = store[(long long)src[pi] * snap + e], z = store[(long long)dst[pi] * snap + e];
-        x[i] = __float2bfloat16_rn((a - xm[c]) * xis[c]);
-        target[i] = ((z - a) - dm[c]) * dis[c];
+        const float a = sgn * store[(long long)src[pi] * snap + es], z = sgn * store[(long long)dst[pi] * snap + es];
+        float a_in = a;
+        if (noise_rel > 0.0f) {
+            const double u1 = rbcrng::unit_open(rbcrng::stream_at(nseed, 2 * (uint64_t)i));
+            const double u2 = rbcrng::unit_open(rbcrng::stream_at(nseed, 2 * (uint64_t)i + 1));
+            const double g = cos(6.283185307179586 * u2) * sqrt(-2.0 * log(u1));
+            a_in = a + (float)(noise_rel * ds[c] * g);
+        }
+        x[i] = __float2bfloat16_rn((a_in - xm[c]) * xis[c]);
+        target[i] = ((z - a_in) - dm[c]) * dis[c];
     }
 }
 

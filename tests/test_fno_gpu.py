@@ -146,7 +146,7 @@ def test_training_reduces_loss_and_predicts_increment():
     """Trained on the even-numbered pairs (10 steps apart) of four runs, the network
     predicts most of the increment of the odd-numbered pairs it has not seen: what the
     learned part gains over persistence (predicting no change)."""
-    f = sdc_b200.FNO(32, 32, 2, 4, width=16, modes=6, layers=2, hidden=32, max_batch=4, seed=1)
+    f = sdc_b200.FNO(32, 32, 2, 4, width=16, modes=6, layers=2, hidden=32, max_batch=4, seed=1, interval_steps=10)
     runs = [run_snapshots(SMALL, ra, seed, 1500, 10, 21) for ra, seed in
             [(3000.0, 1), (3700.0, 2), (4400.0, 3), (5000.0, 4)]]
     f.reserve(sum(len(r) for r in runs))
@@ -178,22 +178,57 @@ def test_training_reduces_loss_and_predicts_increment():
 
 
 def test_surrogate_judge_takes_over():
-    f = sdc_b200.FNO(32, 32, 2, 4, width=16, modes=6, layers=2, hidden=32, max_batch=2, seed=2)
+    f = sdc_b200.FNO(32, 32, 2, 4, width=16, modes=6, layers=2, hidden=32, max_batch=2, seed=2, interval_steps=10)
     s = sdc_b200.Solver(*SMALL)
     s.init_fields(4, 1e-2, 4.0)
     s.step(500)
     st = s.get_state()
     # an untrained network fails a tight check: the plain step runs the rest
-    r = f.run(s, intervals=20, steps_per_interval=10, judge_every=5, nu_tol=1e-12, spec_bins=16, spec_tol=0.0,
+    r = f.run(s, intervals=20, judge_every=5, nu_tol=1e-12, spec_bins=16, spec_tol=0.0,
               fallback_intervals=-1)
     assert (r["checks"], r["fallbacks"], r["surrogate_intervals"], r["plain_intervals"]) == (1, 1, 4, 16), r
     # a loose check never fails: every fifth interval is a plain one
     s.set_state(*st)
-    r = f.run(s, intervals=20, steps_per_interval=10, judge_every=5, nu_tol=1e9, spec_bins=16, spec_tol=1e9)
+    r = f.run(s, intervals=20, judge_every=5, nu_tol=1e9, spec_bins=16, spec_tol=1e9)
     assert (r["checks"], r["fallbacks"], r["surrogate_intervals"], r["plain_intervals"]) == (4, 0, 16, 4), r
     assert r["ms"] > 0 and r["max_nu_err"] >= r["last_nu_err"] >= 0
     # every check fails and fallback_intervals = 2: checks at t = 2, 5, 8, 11, two plain
     # intervals after each of the first three, the surrogate only at t = 0, 1
     s.set_state(*st)
-    r = f.run(s, intervals=12, steps_per_interval=10, judge_every=3, nu_tol=1e-12, fallback_intervals=2)
+    r = f.run(s, intervals=12, judge_every=3, nu_tol=1e-12, fallback_intervals=2)
     assert (r["checks"], r["fallbacks"], r["surrogate_intervals"], r["plain_intervals"]) == (4, 4, 2, 10), r
+
+
+def test_physics_mean_modes_track_the_plain_step():
+    """With the network's increment zeroed, one surrogate interval still advances the
+    horizontal-mean modes (theta_k at q = 0, F_k, G_k) by the plain step's own q = 0
+    recursion: they follow the plain run over the same steps to a small fraction of their
+    change, while without the physics update they stay where they were."""
+    s = sdc_b200.Solver(*SMALL)
+    s.init_fields(5, 1e-2, 4.0)
+    s.step(1500)
+    st0 = s.get_state()
+    s.step(10)
+    ref = s.get_state()
+    mean = lambda st: np.concatenate([st[0][:, 0, 0].real, st[3].real, st[4].real])
+    m0, mref = mean(st0), mean(ref)
+    change = np.abs(mref - m0).max()
+    assert change > 1e-8
+    # the forcing is taken constant over the interval (no previous interval): in this
+    # growth phase that leaves a fraction of the change
+    for pm, bound in ((True, 0.25), (False, None)):
+        f = sdc_b200.FNO(32, 32, 2, 4, width=16, modes=6, layers=2, hidden=32, max_batch=1, seed=2,
+                         interval_steps=10, physics_mean=pm)
+        f.set_params(np.zeros(f.num_params, np.float32))
+        C = 16
+        f.set_norm(np.stack([np.zeros(C), np.ones(C), np.zeros(C), np.ones(C)]).astype(np.float32))
+        s.set_state(*st0)
+        f.advance(s, 1)
+        got = s.get_state()
+        # everything but the mean modes is unchanged (zero increment)
+        assert rel_err(got[0][:, 1:, :], st0[0][:, 1:, :]) == 0.0
+        err = np.abs(mean(got) - mref).max()
+        if bound is None:
+            assert err == pytest.approx(change, rel=1e-12)
+        else:
+            assert err < bound * change, (err, change)
