@@ -293,7 +293,10 @@ class Solver:
 
     def close(self):
         if getattr(self, "h", None) and getattr(self, "_owned", True):
-            lib().rbc_destroy(self.h)
+            try:
+                lib().rbc_destroy(self.h)
+            except TypeError:  # interpreter shutdown: module globals are gone
+                pass
         self.h = None
 
     @property
@@ -481,7 +484,10 @@ class FNO:
 
     def close(self):
         if getattr(self, "m", None):
-            lib().rbc_fno_destroy(self.m)
+            try:
+                lib().rbc_fno_destroy(self.m)
+            except TypeError:  # interpreter shutdown: module globals are gone
+                pass
         self.m = None
 
     __del__ = close

@@ -22,49 +22,69 @@
 
 namespace rbck {
 
+// One thread per point; the block's [256][4 nq] output tile goes through shared memory
+// (row stride 4 nq + 1) so that the channel-last rows are written with coalesced stores.
 template <typename R, int L>
 __global__ void __launch_bounds__(256) k_colloc_encode(const R* __restrict__ phys, int P, int nq,
                                                        const double* __restrict__ basis, float* __restrict__ out)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= P) return;
-    double u11[L], u21[L], u31[L], u12[L], u22[L], th[L];
-#pragma unroll
-    for (int m = 0; m < L; ++m) {
-        u11[m] = phys[(size_t)(0 * L + m) * P + p];
-        u21[m] = phys[(size_t)(1 * L + m) * P + p];
-        u31[m] = phys[(size_t)(2 * L + m) * P + p];
-        u12[m] = phys[(size_t)(3 * L + m) * P + p];
-        u22[m] = phys[(size_t)(4 * L + m) * P + p];
-        th[m] = phys[(size_t)(5 * L + m) * P + p];
-    }
-    float* o = out + (size_t)p * 4 * nq;
-    for (int q = 0; q < nq; ++q) {
-        const double* b = basis + (size_t)q * 3 * L; // C, C', S
-        double t = 0, u = 0, v = 0, w = 0;
+    extern __shared__ float tile[]; // [256][4 nq + 1]
+    const int C = 4 * nq, ld = C + 1;
+    const int p0 = blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
+    if (p < P) {
+        double u11[L], u21[L], u31[L], u12[L], u22[L], th[L];
 #pragma unroll
         for (int m = 0; m < L; ++m) {
-            const double C = b[m], Cp = b[L + m], S = b[2 * L + m];
-            t += S * th[m];
-            u += Cp * u11[m] + S * u12[m];
-            v += Cp * u21[m] + S * u22[m];
-            w += C * u31[m];
+            u11[m] = phys[(size_t)(0 * L + m) * P + p];
+            u21[m] = phys[(size_t)(1 * L + m) * P + p];
+            u31[m] = phys[(size_t)(2 * L + m) * P + p];
+            u12[m] = phys[(size_t)(3 * L + m) * P + p];
+            u22[m] = phys[(size_t)(4 * L + m) * P + p];
+            th[m] = phys[(size_t)(5 * L + m) * P + p];
         }
-        o[q] = (float)t;
-        o[nq + q] = (float)u;
-        o[2 * nq + q] = (float)v;
-        o[3 * nq + q] = (float)w;
+        float* o = tile + threadIdx.x * ld;
+        for (int q = 0; q < nq; ++q) {
+            const double* b = basis + (size_t)q * 3 * L; // C, C', S
+            double t = 0, u = 0, v = 0, w = 0;
+#pragma unroll
+            for (int m = 0; m < L; ++m) {
+                const double Cb = b[m], Cp = b[L + m], S = b[2 * L + m];
+                t += S * th[m];
+                u += Cp * u11[m] + S * u12[m];
+                v += Cp * u21[m] + S * u22[m];
+                w += Cb * u31[m];
+            }
+            o[q] = (float)t;
+            o[nq + q] = (float)u;
+            o[2 * nq + q] = (float)v;
+            o[3 * nq + q] = (float)w;
+        }
+    }
+    __syncthreads();
+    const int np = min((int)blockDim.x, P - p0);
+    for (int e = threadIdx.x; e < np * C; e += blockDim.x) {
+        const int r = e / C, c = e - r * C;
+        out[(size_t)p0 * C + e] = tile[r * ld + c];
     }
 }
 
-// planes [4][L][P]: Theta, W, U, V mode amplitudes of the increment at every point.
+// planes [4][L][P]: Theta, W, U, V mode amplitudes of the increment at every point. The
+// block's [256][4 nq] input tile is read with coalesced loads into shared memory first.
 template <int L>
 __global__ void __launch_bounds__(256) k_colloc_project(const float* __restrict__ delta, int P, int nq,
                                                         const double* __restrict__ proj, double* __restrict__ planes)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ float tile[]; // [256][4 nq + 1]
+    const int C = 4 * nq, ld = C + 1;
+    const int p0 = blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
+    const int np = min((int)blockDim.x, P - p0);
+    for (int e = threadIdx.x; e < np * C; e += blockDim.x) {
+        const int r = e / C, c = e - r * C;
+        tile[r * ld + c] = delta[(size_t)p0 * C + e];
+    }
+    __syncthreads();
     if (p >= P) return;
-    const float* d = delta + (size_t)p * 4 * nq;
+    const float* d = tile + threadIdx.x * ld;
     const double *Ps = proj, *Pc = proj + (size_t)L * nq;
     double a[4][L];
 #pragma unroll
@@ -73,11 +93,11 @@ __global__ void __launch_bounds__(256) k_colloc_project(const float* __restrict_
         const double t = d[q], u = d[nq + q], v = d[2 * nq + q], w = d[3 * nq + q];
 #pragma unroll
         for (int m = 0; m < L; ++m) {
-            const double s = Ps[m * nq + q], c = Pc[m * nq + q];
-            a[0][m] += s * t;
-            a[1][m] += c * w;
-            a[2][m] += s * u;
-            a[3][m] += s * v;
+            const double sv = Ps[m * nq + q], cv = Pc[m * nq + q];
+            a[0][m] += sv * t;
+            a[1][m] += cv * w;
+            a[2][m] += sv * u;
+            a[3][m] += sv * v;
         }
     }
 #pragma unroll
@@ -88,6 +108,9 @@ __global__ void __launch_bounds__(256) k_colloc_project(const float* __restrict_
 
 // Direct DFT of each real row (plane, y) for the kept columns c < ckeep:
 // out[(plane ckeep + c) Ny + y] = sum_x row[x] e^{-2 pi i c x / Nx}. Grid nplanes * Ny.
+// Each thread owns one c and walks x in blocks of 8: the phase of the block start comes
+// from the exact table, the 7 steps inside by multiplication with e^{-2 pi i c / Nx}, so the
+// table is read once per 8 terms (rounding growth ~8 ulp) and the row is a broadcast.
 __global__ void __launch_bounds__(128) k_colloc_row_dft(const double* __restrict__ planes, int nx, int ny, int ckeep,
                                                         const double2* __restrict__ twx, double2* __restrict__ out)
 {
@@ -102,14 +125,15 @@ __global__ void __launch_bounds__(128) k_colloc_row_dft(const double* __restrict
     }
     __syncthreads();
     for (int c = threadIdx.x; c < ckeep; c += blockDim.x) {
+        const double2 st = tw[c];
         double re = 0, im = 0;
-        int idx = 0;
-        for (int x = 0; x < nx; ++x) {
-            const double2 w = tw[idx];
-            re += row[x] * w.x;
-            im += row[x] * w.y;
-            idx += c;
-            if (idx >= nx) idx -= nx;
+        for (int x0 = 0; x0 < nx; x0 += 8) {
+            double2 w = tw[(int)(((long long)c * x0) % nx)];
+            for (int x = x0; x < x0 + 8 && x < nx; ++x) {
+                re += row[x] * w.x;
+                im += row[x] * w.y;
+                w = make_double2(w.x * st.x - w.y * st.y, w.x * st.y + w.y * st.x);
+            }
         }
         out[((size_t)plane * ckeep + c) * ny + y] = make_double2(re, im);
     }
@@ -142,17 +166,19 @@ __global__ void __launch_bounds__(256) k_colloc_assemble(const double2* __restri
         double2 s[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) s[a] = make_double2(0, 0);
-        int idx = 0;
-        for (int y = 0; y < ny; ++y) {
-            const double2 w = tw[idx];
+        // phase of each block of 8 terms from the exact table, 7 rotations inside
+        const double2 st = tw[rs];
+        for (int y0 = 0; y0 < ny; y0 += 8) {
+            double2 w = tw[(int)(((long long)rs * y0) % ny)];
+            for (int y = y0; y < y0 + 8 && y < ny; ++y) {
 #pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const double2 v = col[a * ny + y];
-                s[a].x += v.x * w.x - v.y * w.y;
-                s[a].y += v.x * w.y + v.y * w.x;
+                for (int a = 0; a < 4; ++a) {
+                    const double2 v = col[a * ny + y];
+                    s[a].x += v.x * w.x - v.y * w.y;
+                    s[a].y += v.x * w.y + v.y * w.x;
+                }
+                w = make_double2(w.x * st.x - w.y * st.y, w.x * st.y + w.y * st.x);
             }
-            idx += rs;
-            if (idx >= ny) idx -= ny;
         }
 #pragma unroll
         for (int a = 0; a < 4; ++a) {

@@ -89,6 +89,8 @@ struct rbc_fno {
     int nsplit_max = 0, ncol_blocks = 0, nloss_blocks = 0;
     double* dloss = nullptr;
     int dloss_n = 0;
+    float* skbuf = nullptr;   // split-K slices of one-batch GEMMs
+    size_t skcap = 0;
     // solver coupling
     double *basis = nullptr, *proj = nullptr;
     void* dec = nullptr;
@@ -158,16 +160,9 @@ int load_mode(const bf16* base, long long rs, long long cs, long long bs, int ro
     return rs == 1 ? 1 : 0;
 }
 
-void gemm(cudaStream_t s, GemmOp op)
+constexpr int kSMs = 148;
+void launch_gemm(cudaStream_t s, const GemmOp& op, int BM, int BN)
 {
-    // split-K chunks start at multiples of K: 16-byte loads along k need K and ktot % 8 == 0
-    long long kchk = op.K;
-    if (op.ktot > 0) kchk = (op.K % 8 == 0 && op.ktot % 8 == 0) ? 8 : 1;
-    op.amode = load_mode(op.A, op.a_rs, op.a_cs, op.a_bs, op.M, kchk);
-    op.bmode = load_mode(op.B, op.b_cs, op.b_rs, op.b_bs, op.N, kchk);
-    if (op.batch < 1 || op.batch > 65535 || op.M < 1 || op.N < 1 || op.K < 1) throw ArgErr{"gemm shape"};
-    const int BN = op.N <= 32 ? 32 : 64;
-    const int BM = op.M <= 32 ? 32 : (BN == 32 && op.M >= 8192 ? 128 : 64);
     dim3 grid((op.M + BM - 1) / BM, (op.N + BN - 1) / BN, op.batch);
     if (grid.y > 65535) throw ArgErr{"gemm N too large"};
     if (BM == 32 && BN == 32) k_gemm<32, 32><<<grid, 128, 0, s>>>(op);
@@ -177,6 +172,75 @@ void gemm(cudaStream_t s, GemmOp op)
     else k_gemm<128, 32><<<grid, 128, 0, s>>>(op);
     FNO_CUDA(cudaGetLastError());
 }
+
+// Tile choice: the largest tile that still gives one full wave of CTAs (148 SMs), else
+// the one with the most CTAs. A one-batch product with too few CTAs and a plain store
+// epilogue is split along K into FP32 slices (scratch splitk, cap floats) summed in order
+// by k_splitk_finish.
+void gemm_on(cudaStream_t s, GemmOp op, float* splitk, size_t cap)
+{
+    if (op.batch < 1 || op.batch > 65535 || op.M < 1 || op.N < 1 || op.K < 1) throw ArgErr{"gemm shape"};
+    // split-K chunks start at multiples of K: 16-byte loads along k need K and ktot % 8 == 0
+    long long kchk = op.K;
+    if (op.ktot > 0) kchk = (op.K % 8 == 0 && op.ktot % 8 == 0) ? 8 : 1;
+    op.amode = load_mode(op.A, op.a_rs, op.a_cs, op.a_bs, op.M, kchk);
+    op.bmode = load_mode(op.B, op.b_cs, op.b_rs, op.b_bs, op.N, kchk);
+    op.vec2 = (op.c_cs == 1 && op.c_rs % 2 == 0 && op.c_bs % 2 == 0 && op.N % 2 == 0) ? 1 : 0;
+    static const int tiles[5][2] = {{128, 32}, {64, 64}, {64, 32}, {32, 64}, {32, 32}};
+    auto ctas = [&](int bm, int bn) {
+        return (long long)((op.M + bm - 1) / bm) * ((op.N + bn - 1) / bn) * op.batch;
+    };
+    int BM = 32, BN = 32;
+    bool found = false;
+    for (auto& t : tiles) {
+        // no tile more than half empty along M or N; the 128-row tile only for N <= 32
+        if ((t[0] > 32 && t[0] >= 2 * op.M) || (t[1] > 32 && t[1] >= 2 * op.N) || (t[0] == 128 && op.N > 32))
+            continue;
+        if (ctas(t[0], t[1]) >= kSMs) {
+            BM = t[0];
+            BN = t[1];
+            found = true;
+            break;
+        }
+    }
+    if (!found) {
+        BM = 32;
+        BN = 32;
+    }
+    const bool plain = !op.bias && !op.add && !op.aux && !op.pre && op.act == ACT_NONE && op.alpha == 1.0f;
+    const long long n_ctas = ctas(BM, BN);
+    if (!found && plain && op.batch == 1 && op.ktot == 0 && op.K >= 128 && splitk) {
+        int S = (int)std::min<long long>(op.K / 32, (2 * kSMs + n_ctas - 1) / n_ctas);
+        const int Kc = ((op.K + S - 1) / S + 31) / 32 * 32;
+        S = (op.K + Kc - 1) / Kc;
+        if (S > 1 && (size_t)S * op.M * op.N <= cap) {
+            GemmOp p = op;
+            p.K = Kc;
+            p.ktot = op.K;
+            p.batch = S;
+            p.a_bs = (long long)Kc * op.a_cs;
+            p.b_bs = (long long)Kc * op.b_rs;
+            p.c_rs = op.N;
+            p.c_cs = 1;
+            p.c_bs = (long long)op.M * op.N;
+            p.outf = splitk;
+            p.outb = nullptr;
+            p.vec2 = op.N % 2 == 0 ? 1 : 0;
+            const long long kc8 = (Kc % 8 == 0 && op.K % 8 == 0) ? 8 : 1;
+            p.amode = load_mode(p.A, p.a_rs, p.a_cs, p.a_bs, p.M, kc8);
+            p.bmode = load_mode(p.B, p.b_cs, p.b_rs, p.b_bs, p.N, kc8);
+            launch_gemm(s, p, BM, BN);
+            const long long mn = (long long)op.M * op.N;
+            k_splitk_finish<<<(int)std::min<long long>((mn + 255) / 256, 4 * kSMs), 256, 0, s>>>(
+                splitk, S, op.M, op.N, op.c_rs, op.c_cs, op.outf, op.outb);
+            FNO_CUDA(cudaGetLastError());
+            return;
+        }
+    }
+    launch_gemm(s, op, BM, BN);
+}
+
+void gemm(rbc_fno* f, cudaStream_t s, const GemmOp& op) { gemm_on(s, op, f->skbuf, f->skcap); }
 
 int grid_1d(long long n, int threads = 256, int cap = 148 * 8)
 {
@@ -210,7 +274,7 @@ void wgrad(rbc_fno* f, cudaStream_t s, const bf16* G, int No, const bf16* X, int
     op.c_cs = 1;
     op.c_bs = (long long)No * Ni;
     op.outf = f->wpart;
-    gemm(s, op);
+    gemm(f, s, op);
     k_sum_slices<<<grid_1d((long long)No * Ni), 256, 0, s>>>(f->wpart, ns, (long long)No * Ni, f->grad + off, 0);
     FNO_CUDA(cudaGetLastError());
 }
@@ -241,7 +305,7 @@ void forward(rbc_fno* f, int B, cudaStream_t s)
     op.B = pb(f, f->oPw); op.b_rs = 1; op.b_cs = C;
     op.M = (int)M; op.N = W; op.K = C;
     op.c_rs = W; op.bias = f->param + f->oPb; op.outb = f->h[0];
-    gemm(s, op);
+    gemm(f, s, op);
     for (int l = 0; l < f->nl; ++l) {
         // x-DFT: per (b, y): A1[kr][c] = sum_x Fx[kr][x] h[x][c]
         op = GemmOp();
@@ -249,14 +313,14 @@ void forward(rbc_fno* f, int B, cudaStream_t s)
         op.B = f->h[l]; op.b_rs = W; op.b_cs = 1; op.b_bs = (long long)nx * W;
         op.M = 2 * m; op.N = W; op.K = nx; op.batch = B * ny;
         op.c_rs = W; op.c_bs = 2LL * m * W; op.outb = f->A1;
-        gemm(s, op);
+        gemm(f, s, op);
         // y-DFT: per b: Ahat[(ky, ri)][(kx, c)] = sum_(y, ri') Fy A1
         op = GemmOp();
         op.A = f->FyB; op.a_rs = 2 * ny; op.a_cs = 1;
         op.B = f->A1; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * ny * mW;
         op.M = 2 * my; op.N = (int)mW; op.K = 2 * ny; op.batch = B;
         op.c_rs = mW; op.c_bs = 2LL * my * mW; op.outb = f->Ahat[l];
-        gemm(s, op);
+        gemm(f, s, op);
         // per-mode channel mixing
         const size_t smf = (size_t)(2 * W * W + (128 / W) * 2 * W) * sizeof(float);
         k_modemix_fwd<<<my * m, 128, smf, s>>>(f->Ahat[l], pb(f, f->oR[l]), f->Yh, B, m, W);
@@ -267,14 +331,14 @@ void forward(rbc_fno* f, int B, cudaStream_t s)
         op.B = f->Yh; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * my * mW;
         op.M = 2 * ny; op.N = (int)mW; op.K = 2 * my; op.batch = B;
         op.c_rs = mW; op.c_bs = 2LL * ny * mW; op.outb = f->Z;
-        gemm(s, op);
+        gemm(f, s, op);
         // inverse x (FP32 result, added in the pointwise epilogue)
         op = GemmOp();
         op.A = f->GxT; op.a_rs = 2 * m; op.a_cs = 1;
         op.B = f->Z; op.b_rs = W; op.b_cs = 1; op.b_bs = 2LL * m * W;
         op.M = nx; op.N = W; op.K = 2 * m; op.batch = B * ny;
         op.c_rs = W; op.c_bs = (long long)nx * W; op.outf = f->Kv;
-        gemm(s, op);
+        gemm(f, s, op);
         // pointwise map + spectral part + bias, activation
         op = GemmOp();
         op.A = f->h[l]; op.a_rs = W; op.a_cs = 1;
@@ -282,20 +346,20 @@ void forward(rbc_fno* f, int B, cudaStream_t s)
         op.M = (int)M; op.N = W; op.K = W;
         op.c_rs = W; op.bias = f->param + f->ob[l]; op.add = f->Kv; op.pre = f->pre[l];
         op.act = l + 1 < f->nl ? ACT_GELU : ACT_NONE; op.outb = f->h[l + 1];
-        gemm(s, op);
+        gemm(f, s, op);
     }
     op = GemmOp();
     op.A = f->h[f->nl]; op.a_rs = W; op.a_cs = 1;
     op.B = pb(f, f->oQ1w); op.b_rs = 1; op.b_cs = W;
     op.M = (int)M; op.N = H; op.K = W;
     op.c_rs = H; op.bias = f->param + f->oQ1b; op.pre = f->q1pre; op.act = ACT_GELU; op.outb = f->q1;
-    gemm(s, op);
+    gemm(f, s, op);
     op = GemmOp();
     op.A = f->q1; op.a_rs = H; op.a_cs = 1;
     op.B = pb(f, f->oQ2w); op.b_rs = 1; op.b_cs = H;
     op.M = (int)M; op.N = C; op.K = H;
     op.c_rs = C; op.bias = f->param + f->oQ2b; op.outf = f->out;
-    gemm(s, op);
+    gemm(f, s, op);
 }
 
 // Loss of f->out against f->target (B samples) into dloss[idx]; gradient into f->grad.
@@ -315,7 +379,7 @@ void loss_backward(rbc_fno* f, int B, cudaStream_t s, int idx)
     op.B = pb(f, f->oQ2w); op.b_rs = H; op.b_cs = 1;
     op.M = (int)M; op.N = H; op.K = C;
     op.c_rs = H; op.act = ACT_GELU_BWD; op.aux = f->q1pre; op.outb = f->gB;
-    gemm(s, op);
+    gemm(f, s, op);
     wgrad(f, s, f->gB, H, f->h[f->nl], W, M, f->oQ1w);
     colsum(f, s, f->gB, M, H, f->oQ1b);
     op = GemmOp();
@@ -323,7 +387,7 @@ void loss_backward(rbc_fno* f, int B, cudaStream_t s, int idx)
     op.B = pb(f, f->oQ1w); op.b_rs = W; op.b_cs = 1;
     op.M = (int)M; op.N = W; op.K = H;
     op.c_rs = W; op.outb = f->gA;
-    gemm(s, op);
+    gemm(f, s, op);
     bf16* gp = f->gA;
     bf16* gn = f->gB;
     for (int l = f->nl - 1; l >= 0; --l) {
@@ -335,14 +399,14 @@ void loss_backward(rbc_fno* f, int B, cudaStream_t s, int idx)
         op.B = gp; op.b_rs = W; op.b_cs = 1; op.b_bs = (long long)nx * W;
         op.M = 2 * m; op.N = W; op.K = nx; op.batch = B * ny;
         op.c_rs = W; op.c_bs = 2LL * m * W; op.outb = f->dZ;
-        gemm(s, op);
+        gemm(f, s, op);
         // adjoint of the inverse y transform
         op = GemmOp();
         op.A = f->GyB; op.a_rs = 1; op.a_cs = 2 * my;
         op.B = f->dZ; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * ny * mW;
         op.M = 2 * my; op.N = (int)mW; op.K = 2 * ny; op.batch = B;
         op.c_rs = mW; op.c_bs = 2LL * my * mW; op.outb = f->dY;
-        gemm(s, op);
+        gemm(f, s, op);
         const size_t smb = (size_t)(2 * W * W + 4 * W) * sizeof(float);
         k_modemix_bwd<<<my * m, 256, smb, s>>>(f->Ahat[l], pb(f, f->oR[l]), f->dY, f->dAh, f->grad + f->oR[l], B,
                                                 m, W);
@@ -353,14 +417,14 @@ void loss_backward(rbc_fno* f, int B, cudaStream_t s, int idx)
         op.B = f->dAh; op.b_rs = mW; op.b_cs = 1; op.b_bs = 2LL * my * mW;
         op.M = 2 * ny; op.N = (int)mW; op.K = 2 * my; op.batch = B;
         op.c_rs = mW; op.c_bs = 2LL * ny * mW; op.outb = f->dA1;
-        gemm(s, op);
+        gemm(f, s, op);
         // adjoint of the forward x transform (FP32)
         op = GemmOp();
         op.A = f->FxT; op.a_rs = 1; op.a_cs = nx;
         op.B = f->dA1; op.b_rs = W; op.b_cs = 1; op.b_bs = 2LL * m * W;
         op.M = nx; op.N = W; op.K = 2 * m; op.batch = B * ny;
         op.c_rs = W; op.c_bs = (long long)nx * W; op.outf = f->dhs;
-        gemm(s, op);
+        gemm(f, s, op);
         // adjoint of the pointwise map, plus the spectral part, times GELU' of the layer below
         op = GemmOp();
         op.A = gp; op.a_rs = W; op.a_cs = 1;
@@ -372,7 +436,7 @@ void loss_backward(rbc_fno* f, int B, cudaStream_t s, int idx)
             op.aux = f->pre[l - 1];
         }
         op.outb = gn;
-        gemm(s, op);
+        gemm(f, s, op);
         std::swap(gp, gn);
     }
     wgrad(f, s, gp, W, f->x0, C, M, f->oPw);
@@ -626,6 +690,8 @@ rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out)
         f->cpart = falloc<float>(f, (size_t)f->ncol_blocks * 256);
         f->nloss_blocks = 148 * 4;
         f->lpart = falloc<float>(f, f->nloss_blocks);
+        f->skcap = (size_t)1 << 20;
+        f->skbuf = falloc<float>(f, f->skcap);
         f->dloss_n = 1 << 16;
         f->dloss = falloc<double>(f, f->dloss_n);
         // solver coupling (grids with nz vertical modes)

@@ -42,6 +42,8 @@ struct GemmOp {
     bf16* outb = nullptr;        // BF16 output (round to nearest even)
     int act = ACT_NONE;
     int amode = 0, bmode = 0;    // tile load modes (set by the host, see load_tile)
+    int vec2 = 0;                // 1: outputs/addends of columns n, n+1 are adjacent and 8-byte
+                                 //    aligned (c_cs == 1, c_rs and c_bs even, N even)
 };
 
 constexpr int kBK = 32, kSK = kBK + 8; // k tile and padded shared row (80 bytes)
@@ -157,25 +159,66 @@ __global__ void __launch_bounds__(128) k_gemm(GemmOp op)
         __syncthreads();
     }
     const long long cz = (long long)z * op.c_bs;
+    auto epi = [&](float v, long long o, int n) -> float {
+        v *= op.alpha;
+        if (op.bias) v += op.bias[n];
+        if (op.add) v += op.add[o];
+        if (op.pre) op.pre[o] = v;
+        if (op.act == ACT_GELU) v = gelu(v);
+        else if (op.act == ACT_GELU_BWD) v *= gelu_grad(op.aux[o]);
+        return v;
+    };
 #pragma unroll
     for (int i = 0; i < MT; ++i)
 #pragma unroll
         for (int j = 0; j < NT; ++j)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int m = m0 + wm * (BM / 2) + i * 16 + gq + (e >> 1) * 8;
-                const int n = n0 + wn * (BN / 2) + j * 8 + 2 * tq + (e & 1);
+            for (int h2 = 0; h2 < 2; ++h2) {
+                const int m = m0 + wm * (BM / 2) + i * 16 + gq + h2 * 8;
+                const int n = n0 + wn * (BN / 2) + j * 8 + 2 * tq;
                 if (m >= op.M || n >= op.N) continue;
                 const long long o = cz + m * op.c_rs + n * op.c_cs;
-                float v = op.alpha * acc[i][j][e];
-                if (op.bias) v += op.bias[n];
-                if (op.add) v += op.add[o];
-                if (op.pre) op.pre[o] = v;
-                if (op.act == ACT_GELU) v = gelu(v);
-                else if (op.act == ACT_GELU_BWD) v *= gelu_grad(op.aux[o]);
-                if (op.outf) op.outf[o] = v;
-                if (op.outb) op.outb[o] = __float2bfloat16_rn(v);
+                if (op.vec2) {
+                    // columns n, n + 1 together: 8-byte FP32 and 4-byte BF16 accesses
+                    float2 v = make_float2(acc[i][j][2 * h2] * op.alpha, acc[i][j][2 * h2 + 1] * op.alpha);
+                    if (op.bias) { v.x += op.bias[n]; v.y += op.bias[n + 1]; }
+                    if (op.add) { const float2 a = *reinterpret_cast<const float2*>(op.add + o); v.x += a.x; v.y += a.y; }
+                    if (op.pre) *reinterpret_cast<float2*>(op.pre + o) = v;
+                    if (op.act == ACT_GELU) { v.x = gelu(v.x); v.y = gelu(v.y); }
+                    else if (op.act == ACT_GELU_BWD) {
+                        const float2 a = *reinterpret_cast<const float2*>(op.aux + o);
+                        v.x *= gelu_grad(a.x);
+                        v.y *= gelu_grad(a.y);
+                    }
+                    if (op.outf) *reinterpret_cast<float2*>(op.outf + o) = v;
+                    if (op.outb) *reinterpret_cast<__nv_bfloat162*>(op.outb + o) = __floats2bfloat162_rn(v.x, v.y);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        if (n + e >= op.N) continue;
+                        const long long oe = o + e * op.c_cs;
+                        const float v = epi(acc[i][j][2 * h2 + e], oe, n + e);
+                        if (op.outf) op.outf[oe] = v;
+                        if (op.outb) op.outb[oe] = __float2bfloat16_rn(v);
+                    }
+                }
             }
+}
+
+// Split-K finish: out(m, n) = sum of the nsplit FP32 slices [s][M][N] (in order), stored
+// as FP32 and/or BF16 at z c_bs + m c_rs + n c_cs of a one-batch GEMM.
+__global__ void k_splitk_finish(const float* __restrict__ part, int nsplit, int M, int N, long long c_rs,
+                                long long c_cs, float* __restrict__ outf, bf16* __restrict__ outb)
+{
+    const long long mn = (long long)M * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < mn; i += (long long)gridDim.x * blockDim.x) {
+        float v = 0.0f;
+        for (int s = 0; s < nsplit; ++s) v += part[s * mn + i];
+        const int m = (int)(i / N), n = (int)(i - (long long)m * N);
+        const long long o = m * c_rs + n * c_cs;
+        if (outf) outf[o] = v;
+        if (outb) outb[o] = __float2bfloat16_rn(v);
+    }
 }
 
 // Spectral channel mixing, one CTA per retained mode (ky index, kx):
