@@ -1700,10 +1700,9 @@ void set_error(rbc_handle* h, const char* msg)
 template <typename R, int L> static void encode_L(rbc_handle* h, int nq, const double* basis, float* out)
 {
     const int P = h->G.P;
-    const size_t sm = (size_t)256 * (4 * nq + 1) * sizeof(float);
-    if (sm > 48 * 1024)
-        RBC_CUDA(cudaFuncSetAttribute(k_colloc_encode<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_colloc_encode<R, L><<<(P + 255) / 256, 256, sm, h->stream>>>((const R*)h->phys, P, nq, basis, out);
+    // 64-point blocks: a 128 x 128 plane gives 256 CTAs
+    const size_t sm = (size_t)64 * (4 * nq + 1) * sizeof(float);
+    k_colloc_encode<R, L><<<(P + 63) / 64, 64, sm, h->stream>>>((const R*)h->phys, P, nq, basis, out);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -1826,10 +1825,8 @@ template <int L> static void add_L(rbc_handle* h, int nq, const double* proj, co
     const Geom& G = h->G;
     double* planes = static_cast<double*>(scratch);
     double2* rows = reinterpret_cast<double2*>(planes + (size_t)4 * L * G.P);
-    const size_t sm_pr = (size_t)256 * (4 * nq + 1) * sizeof(float);
-    if (sm_pr > 48 * 1024)
-        RBC_CUDA(cudaFuncSetAttribute(k_colloc_project<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pr));
-    k_colloc_project<L><<<(G.P + 255) / 256, 256, sm_pr, h->stream>>>(delta, G.P, nq, proj, planes);
+    const size_t sm_pr = (size_t)64 * (4 * nq + 1) * sizeof(float);
+    k_colloc_project<L><<<(G.P + 63) / 64, 64, sm_pr, h->stream>>>(delta, G.P, nq, proj, planes);
     RBC_CUDA(cudaGetLastError());
     const size_t sm_row = (size_t)G.nx * (sizeof(double2) + sizeof(double));
     k_colloc_row_dft<<<4 * L * G.ny, 128, sm_row, h->stream>>>(planes, G.nx, G.ny, G.ckeep, h->twx, rows);

@@ -22,13 +22,13 @@
 
 namespace rbck {
 
-// One thread per point; the block's [256][4 nq] output tile goes through shared memory
+// One thread per point; the block's [points][4 nq] output tile goes through shared memory
 // (row stride 4 nq + 1) so that the channel-last rows are written with coalesced stores.
 template <typename R, int L>
 __global__ void __launch_bounds__(256) k_colloc_encode(const R* __restrict__ phys, int P, int nq,
                                                        const double* __restrict__ basis, float* __restrict__ out)
 {
-    extern __shared__ float tile[]; // [256][4 nq + 1]
+    extern __shared__ float tile[]; // [blockDim.x][4 nq + 1]
     const int C = 4 * nq, ld = C + 1;
     const int p0 = blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
     if (p < P) {
@@ -69,12 +69,12 @@ __global__ void __launch_bounds__(256) k_colloc_encode(const R* __restrict__ phy
 }
 
 // planes [4][L][P]: Theta, W, U, V mode amplitudes of the increment at every point. The
-// block's [256][4 nq] input tile is read with coalesced loads into shared memory first.
+// block's [points][4 nq] input tile is read with coalesced loads into shared memory first.
 template <int L>
 __global__ void __launch_bounds__(256) k_colloc_project(const float* __restrict__ delta, int P, int nq,
                                                         const double* __restrict__ proj, double* __restrict__ planes)
 {
-    extern __shared__ float tile[]; // [256][4 nq + 1]
+    extern __shared__ float tile[]; // [blockDim.x][4 nq + 1]
     const int C = 4 * nq, ld = C + 1;
     const int p0 = blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
     const int np = min((int)blockDim.x, P - p0);

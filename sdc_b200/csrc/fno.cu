@@ -275,7 +275,8 @@ void wgrad(rbc_fno* f, cudaStream_t s, const bf16* G, int No, const bf16* X, int
     op.c_bs = (long long)No * Ni;
     op.outf = f->wpart;
     gemm(f, s, op);
-    k_sum_slices<<<grid_1d((long long)No * Ni), 256, 0, s>>>(f->wpart, ns, (long long)No * Ni, f->grad + off, 0);
+    k_sum_slices<<<(int)(((long long)No * Ni + 31) / 32), dim3(32, 32), 0, s>>>(f->wpart, ns, (long long)No * Ni,
+                                                                                f->grad + off, 0);
     FNO_CUDA(cudaGetLastError());
 }
 
@@ -287,7 +288,7 @@ void colsum(rbc_fno* f, cudaStream_t s, const bf16* X, long long M, int N, long 
     const long long rpb = (M + nb - 1) / nb;
     k_colsum_part<<<nb, 256, 0, s>>>(X, M, N, rpb, f->cpart);
     FNO_CUDA(cudaGetLastError());
-    k_sum_slices<<<grid_1d(N), 256, 0, s>>>(f->cpart, nb, N, f->grad + off, 0);
+    k_sum_slices<<<(N + 31) / 32, dim3(32, 32), 0, s>>>(f->cpart, nb, N, f->grad + off, 0);
     FNO_CUDA(cudaGetLastError());
 }
 
@@ -682,7 +683,7 @@ rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out)
         f->dY = falloc<bf16>(f, (long long)f->B * 2 * f->my * mW);
         f->dAh = falloc<bf16>(f, (long long)f->B * 2 * f->my * mW);
         f->dA1 = falloc<bf16>(f, (long long)f->B * 2 * f->ny * mW);
-        f->nsplit_max = 148 * 4;
+        f->nsplit_max = 148 * 2;
         f->wpart_n = (size_t)(f->nsplit_max + 1) * std::max({(long long)W * C, (long long)W * W, (long long)H * W,
                                                               (long long)C * H});
         f->wpart = falloc<float>(f, f->wpart_n);

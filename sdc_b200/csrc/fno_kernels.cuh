@@ -363,15 +363,24 @@ __global__ void __launch_bounds__(256) k_colsum_part(const bf16* __restrict__ X,
     }
 }
 
-// out[j] (+)= sum_s in[s n + j], s in order.
-__global__ void k_sum_slices(const float* __restrict__ in, int nslices, long long n, float* __restrict__ out,
-                             int accumulate)
+// out[j] (+)= sum_s in[s n + j]. Block (32, 32): lane x owns column j of its 32-column
+// chunk, row y sums slices y, y + 32, ... in order, then the 32 row sums are added in a
+// fixed tree: the result does not depend on scheduling.
+__global__ void __launch_bounds__(1024) k_sum_slices(const float* __restrict__ in, int nslices, long long n,
+                                                     float* __restrict__ out, int accumulate)
 {
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
-        float s = 0.0f;
-        for (int q = 0; q < nslices; ++q) s += in[q * n + j];
-        out[j] = accumulate ? out[j] + s : s;
+    __shared__ float red[32][33];
+    const long long j = (long long)blockIdx.x * 32 + threadIdx.x;
+    float s = 0.0f;
+    if (j < n)
+        for (int q = threadIdx.y; q < nslices; q += 32) s += in[q * n + j];
+    red[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 16; w > 0; w >>= 1) {
+        if (threadIdx.y < w) red[threadIdx.y][threadIdx.x] += red[threadIdx.y + w][threadIdx.x];
+        __syncthreads();
     }
+    if (threadIdx.y == 0 && j < n) out[j] = accumulate ? out[j] + red[0][threadIdx.x] : red[0][threadIdx.x];
 }
 
 // Mean-squared-error loss: per-block partial sums of (y - t)^2 (part[blockIdx.x]) and the
