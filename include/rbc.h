@@ -369,8 +369,11 @@ rbc_status rbc_fno_train(rbc_fno* m, const int* src, const int* dst, int npairs,
  * augmentation the normalization gives the velocity channels mean 0 (and, with 2, one
  * shared std). noise_rel > 0 adds N(0, (noise_rel * increment std)^2) noise per channel
  * to each training input and trains toward the true next state from the noisy one, so
- * that the network pulls drifted states back during a rollout. */
-rbc_status rbc_fno_set_train_options(rbc_fno* m, int augment, double noise_rel);
+ * that the network pulls drifted states back during a rollout. pushforward = 1: on every
+ * other iteration a pair's input is the network's own prediction from the previous
+ * snapshot of the same run (no gradient through that first application), trained toward
+ * the pair's true next state (pairs without a previous one use their own input). */
+rbc_status rbc_fno_set_train_options(rbc_fno* m, int augment, double noise_rel, int pushforward);
 /* n surrogate intervals of the solver's state. */
 rbc_status rbc_fno_advance(rbc_fno* m, rbc_handle* h, int n);
 

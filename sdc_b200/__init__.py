@@ -166,7 +166,7 @@ def lib():
     L.rbc_fno_train.argtypes = [vp, ip, ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                 ctypes.c_ulonglong, ctypes.c_int, _dp]
     L.rbc_fno_advance.argtypes = [vp, vp, ctypes.c_int]
-    L.rbc_fno_set_train_options.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.rbc_fno_set_train_options.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
     L.rbc_surrogate_run.argtypes = [vp, vp, ctypes.POINTER(_SurrogateParams), ctypes.POINTER(_SurrogateReport), _dp]
     _LIB = L
     return L
@@ -557,9 +557,10 @@ class FNO:
                                         batch, lr, seed, int(fit_norm), loss.ctypes.data_as(_dp)))
         return loss[:epochs]
 
-    def set_train_options(self, augment=0, noise_rel=0.0):
-        """augment: 0 none, 1 reflections, 2 reflections + transpose (square boxes)."""
-        self._check(lib().rbc_fno_set_train_options(self.m, augment, noise_rel))
+    def set_train_options(self, augment=0, noise_rel=0.0, pushforward=False):
+        """augment: 0 none, 1 reflections, 2 reflections + transpose (square boxes);
+        pushforward: every other iteration trains on the network's own predictions."""
+        self._check(lib().rbc_fno_set_train_options(self.m, augment, noise_rel, int(pushforward)))
 
     def advance(self, solver, n=1):
         self._check(lib().rbc_fno_advance(self.m, solver.h, n))

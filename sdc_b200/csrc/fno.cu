@@ -100,9 +100,11 @@ struct rbc_fno {
     // snapshot store
     float* store = nullptr;
     int nslots = 0;
-    int *src_d = nullptr, *dst_d = nullptr, *perm_d = nullptr, *sym_d = nullptr;
+    int *src_d = nullptr, *dst_d = nullptr, *sym_d = nullptr;
+    int *aslot_d = nullptr, *zslot_d = nullptr, *pfslot_d = nullptr, *usepred_d = nullptr;
     int augment = 0;          // training with the box's horizontal symmetries
     float noise_rel = 0.0f;   // input noise, relative to each channel's increment std
+    int pushforward = 0;      // every other iteration: inputs are the network's own predictions
     double* trace = nullptr;  // per-interval Nu_wall of a rollout (device)
     int trace_n = 0;
     // mean modes advanced by the plain recursion: forcing now / one interval earlier, start values
@@ -889,8 +891,11 @@ rbc_status rbc_fno_dataset_reserve(rbc_fno* f, int nslots)
     f->nslots = nslots;
     f->src_d = falloc<int>(f, nslots);
     f->dst_d = falloc<int>(f, nslots);
-    f->perm_d = falloc<int>(f, nslots);
     f->sym_d = falloc<int>(f, nslots);
+    f->aslot_d = falloc<int>(f, nslots);
+    f->zslot_d = falloc<int>(f, nslots);
+    f->pfslot_d = falloc<int>(f, nslots);
+    f->usepred_d = falloc<int>(f, nslots);
     f->nstat_blocks = 148 * 4;
     f->stat_part = falloc<double>(f, (size_t)f->nstat_blocks * 4 * f->C);
     return RBC_OK;
@@ -969,9 +974,17 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
     const int iters = npairs / batch;
     if (iters > f->dloss_n) throw ArgErr{"too many iterations per epoch"};
     const long long total = (long long)iters * epochs;
-    std::vector<int> perm(npairs), symv(npairs, 0);
+    // the pair that ends where pair i starts (same run), for pushforward inputs
+    std::vector<int> prev(npairs, -1);
+    {
+        std::vector<int> by_dst(f->nslots, -1);
+        for (int i = 0; i < npairs; ++i) by_dst[dst[i]] = i;
+        for (int i = 0; i < npairs; ++i) prev[i] = by_dst[src[i]];
+    }
+    std::vector<int> perm(npairs), symv(npairs, 0), aslot(npairs), zslot(npairs), pfslot(npairs), usepred(npairs);
     std::vector<double> lh(iters);
     long long it_glob = 0;
+    const long long nel = (long long)batch * P * C;
     for (int e = 0; e < epochs; ++e) {
         for (int i = 0; i < npairs; ++i) perm[i] = i;
         for (int i = npairs - 1; i > 0; --i) {
@@ -979,21 +992,43 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
             const int j = (int)(r % (uint64_t)(i + 1));
             std::swap(perm[i], perm[j]);
         }
-        FNO_CUDA(cudaMemcpyAsync(f->perm_d, perm.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
-        if (f->augment) {
-            const int nsym = f->augment == 2 ? 8 : 4;
-            for (int i = 0; i < npairs; ++i) {
+        for (int i = 0; i < npairs; ++i) {
+            const int pi = perm[i];
+            aslot[i] = src[pi];
+            zslot[i] = dst[pi];
+            pfslot[i] = prev[pi] >= 0 ? src[prev[pi]] : src[pi];
+            usepred[i] = prev[pi] >= 0 ? 1 : 0;
+            if (f->augment) {
+                const int nsym = f->augment == 2 ? 8 : 4;
                 const uint64_t r = rbcrng::stream_at(seed ^ 0x5EEDULL, (uint64_t)e * npairs + i);
                 symv[i] = nsym == 8 ? (int)(r % 8) : (int)(r % 4) * 2;
             }
-            FNO_CUDA(cudaMemcpyAsync(f->sym_d, symv.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
         }
+        FNO_CUDA(cudaMemcpyAsync(f->aslot_d, aslot.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+        FNO_CUDA(cudaMemcpyAsync(f->zslot_d, zslot.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+        FNO_CUDA(cudaMemcpyAsync(f->pfslot_d, pfslot.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+        FNO_CUDA(cudaMemcpyAsync(f->usepred_d, usepred.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
+        if (f->augment)
+            FNO_CUDA(cudaMemcpyAsync(f->sym_d, symv.data(), npairs * sizeof(int), cudaMemcpyHostToDevice, s));
         for (int it = 0; it < iters; ++it, ++it_glob) {
-            k_gather_pairs<<<grid_1d((long long)batch * P * C), 256, 0, s>>>(
-                f->store, f->nx, f->ny, f->p.nq, f->src_d, f->dst_d, f->perm_d + (size_t)it * batch,
-                f->augment ? f->sym_d + (size_t)it * batch : nullptr, batch, f->norm, f->norm + C,
-                f->norm + 2 * C, f->norm + 3 * C, f->norm + 4 * C, f->noise_rel,
-                rbcrng::mix64(seed ^ (0xA5A5ULL + (uint64_t)it_glob)), f->x0, f->target);
+            const size_t o = (size_t)it * batch;
+            const int* symp = f->augment ? f->sym_d + o : nullptr;
+            const unsigned long long nseed = rbcrng::mix64(seed ^ (0xA5A5ULL + (uint64_t)it_glob));
+            const bool pf = f->pushforward && (it & 1);
+            if (pf) {
+                // the network's prediction from the previous snapshot of each pair's run
+                k_gather_slots<<<grid_1d(nel), 256, 0, s>>>(f->store, f->nx, f->ny, f->p.nq, f->pfslot_d + o, nullptr,
+                                                            symp, nullptr, nullptr, batch, f->norm, f->norm + C,
+                                                            f->norm + 2 * C, f->norm + 3 * C, f->norm + 4 * C, 0.0f, 0,
+                                                            f->x0, nullptr);
+                FNO_CUDA(cudaGetLastError());
+                forward(f, batch, s);
+            }
+            k_gather_slots<<<grid_1d(nel), 256, 0, s>>>(f->store, f->nx, f->ny, f->p.nq,
+                                                        pf ? f->pfslot_d + o : f->aslot_d + o, f->zslot_d + o, symp,
+                                                        f->usepred_d + o, pf ? f->out : nullptr, batch, f->norm,
+                                                        f->norm + C, f->norm + 2 * C, f->norm + 3 * C, f->norm + 4 * C,
+                                                        f->noise_rel, nseed, f->x0, f->target);
             FNO_CUDA(cudaGetLastError());
             forward(f, batch, s);
             loss_backward(f, batch, s, it);
@@ -1019,13 +1054,15 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
     FNO_GUARD_END(f)
 }
 
-rbc_status rbc_fno_set_train_options(rbc_fno* f, int augment, double noise_rel)
+rbc_status rbc_fno_set_train_options(rbc_fno* f, int augment, double noise_rel, int pushforward)
 {
     if (!f) return RBC_ERR_INVALID_ARG;
-    if (augment < 0 || augment > 2 || (augment == 2 && f->nx != f->ny) || !(noise_rel >= 0) || noise_rel > 10)
+    if (augment < 0 || augment > 2 || (augment == 2 && f->nx != f->ny) || !(noise_rel >= 0) || noise_rel > 10 ||
+        pushforward < 0 || pushforward > 1)
         return ffail(f, RBC_ERR_INVALID_ARG, "bad training options");
     f->augment = augment;
     f->noise_rel = (float)noise_rel;
+    f->pushforward = pushforward;
     return RBC_OK;
 }
 

@@ -451,22 +451,24 @@ __global__ void k_denormalize(const float* __restrict__ y, long long M, int C, c
     }
 }
 
-// Training batch from the snapshot store: for batch entry b the pair (src, dst) =
-// (slots[perm[b]], slots2[perm[b]]). Snapshots are FP32 [nslot][ny][nx][C] with channel
-// field * nq + level, fields theta, u, v, w. Entry b is first mapped by the horizontal
-// symmetry sym[b] of the periodic box (bit 0: transpose x <-> y, square boxes only;
-// bit 1: x -> -x; bit 2: y -> -y); velocities transform as vectors: with M the point map,
-// u_out(p) = M^T u_in(M p), i.e. (fx v, fy u) under the transpose and (fx u, fy v)
-// otherwise, fx, fy = -1 for a flipped direction. Then x = normalized (snapshot src + e)
-// (BF16) and target = normalized increment dst - (src + e) (FP32), e = noise_rel * std of
-// the channel's increment * N(0,1) (SplitMix64 + Box-Muller on element index i of this
-// batch with seed nseed; noise_rel = 0: no noise).
-__global__ void k_gather_pairs(const float* __restrict__ store, int nx, int ny, int nq, const int* __restrict__ src,
-                               const int* __restrict__ dst, const int* __restrict__ perm, const int* __restrict__ sym,
-                               int nb, const float* __restrict__ xm, const float* __restrict__ xis,
-                               const float* __restrict__ dm, const float* __restrict__ ds,
-                               const float* __restrict__ dis, float noise_rel, unsigned long long nseed,
-                               bf16* __restrict__ x, float* __restrict__ target)
+// Training batch from the snapshot store. Snapshots are FP32 [nslot][ny][nx][C] with
+// channel field * nq + level, fields theta, u, v, w. Batch entry b reads snapshots
+// a_slot[b] and z_slot[b] through the horizontal symmetry sym[b] of the periodic box
+// (bit 0: transpose x <-> y, square boxes only; bit 1: x -> -x; bit 2: y -> -y);
+// velocities transform as vectors: with M the point map, u_out(p) = M^T u_in(M p), i.e.
+// (fx v, fy u) under the transpose and (fx u, fy v) otherwise, fx, fy = -1 for a flipped
+// direction. The input state is s = a (+ the network's denormalized prediction pred[i]
+// when use_pred[b]: the pushforward input), plus e = noise_rel * std of the channel's
+// increment * N(0,1) (SplitMix64 + Box-Muller on element index i with seed nseed;
+// noise_rel = 0: no noise). x = normalized s (BF16); target = normalized increment z - s
+// (not written when target is null).
+__global__ void k_gather_slots(const float* __restrict__ store, int nx, int ny, int nq,
+                               const int* __restrict__ a_slot, const int* __restrict__ z_slot,
+                               const int* __restrict__ sym, const int* __restrict__ use_pred,
+                               const float* __restrict__ pred, int nb, const float* __restrict__ xm,
+                               const float* __restrict__ xis, const float* __restrict__ dm,
+                               const float* __restrict__ ds, const float* __restrict__ dis, float noise_rel,
+                               unsigned long long nseed, bf16* __restrict__ x, float* __restrict__ target)
 {
     const int C = 4 * nq;
     const long long snap = (long long)nx * ny * C;
@@ -486,8 +488,8 @@ __global__ void k_gather_pairs(const float* __restrict__ store, int nx, int ny, 
         if (fo == 1) { fi = (sy & 1) ? 2 : 1; sgn = (sy & 2) ? -1.0f : 1.0f; }
         else if (fo == 2) { fi = (sy & 1) ? 1 : 2; sgn = (sy & 4) ? -1.0f : 1.0f; }
         const long long es = ((long long)ys * nx + xs) * C + fi * nq + q;
-        const int pi = perm[b];
-        const float a = sgn * store[(long long)src[pi] * snap + es], z = sgn * store[(long long)dst[pi] * snap + es];
+        float a = sgn * store[(long long)a_slot[b] * snap + es];
+        if (pred && use_pred[b]) a += pred[i] * ds[c] + dm[c];
         float a_in = a;
         if (noise_rel > 0.0f) {
             const double u1 = rbcrng::unit_open(rbcrng::stream_at(nseed, 2 * (uint64_t)i));
@@ -496,7 +498,10 @@ __global__ void k_gather_pairs(const float* __restrict__ store, int nx, int ny, 
             a_in = a + (float)(noise_rel * ds[c] * g);
         }
         x[i] = __float2bfloat16_rn((a_in - xm[c]) * xis[c]);
-        target[i] = ((z - a_in) - dm[c]) * dis[c];
+        if (target) {
+            const float z = sgn * store[(long long)z_slot[b] * snap + es];
+            target[i] = ((z - a_in) - dm[c]) * dis[c];
+        }
     }
 }
 

@@ -232,3 +232,26 @@ def test_physics_mean_modes_track_the_plain_step():
             assert err == pytest.approx(change, rel=1e-12)
         else:
             assert err < bound * change, (err, change)
+
+
+def test_pushforward_and_augmented_training_run():
+    """Training with the box symmetries, input noise and pushforward inputs (the network's
+    own prediction from the previous snapshot of a run) stays finite and lowers the loss."""
+    f = sdc_b200.FNO(32, 32, 2, 4, width=16, modes=6, layers=2, hidden=32, max_batch=4, seed=3, interval_steps=10)
+    runs = [run_snapshots(SMALL, ra, seed, 1500, 10, 9) for ra, seed in [(3500.0, 6), (4500.0, 7)]]
+    f.reserve(sum(len(r) for r in runs))
+    s = sdc_b200.Solver(*SMALL)
+    slot, src, dst = 0, [], []
+    for r in runs:
+        for k, st in enumerate(r):
+            s.set_state(*st)
+            f.capture(s, slot)
+            if k:
+                src.append(slot - 1)
+                dst.append(slot)
+            slot += 1
+    f.set_train_options(augment=2, noise_rel=0.1, pushforward=True)
+    losses = f.train(np.array(src), np.array(dst), epochs=30, batch=4, lr=3e-3, seed=1)
+    assert np.all(np.isfinite(losses)) and losses[-1] < 0.5 * losses[0], losses
+    with pytest.raises(sdc_b200.RBCError):
+        f.set_train_options(augment=3)
