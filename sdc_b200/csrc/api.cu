@@ -812,7 +812,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         }
         h->partial = dalloc<double>(2 * (size_t)h->upd_blocks, h->owned);
         h->th00 = dalloc<double>(L, h->owned);
-        h->ring = dalloc<double>(4 * (size_t)h->ring_cap, h->owned);
+        h->ring = dalloc<double>(4 * ((size_t)h->ring_cap + 1), h->owned); // + the newest entry
         h->ticket = dalloc<unsigned int>(1, h->owned);
         h->step_counter = dalloc<long long>(1, h->owned);
         h->err = dalloc<int>(1, h->owned);
@@ -820,7 +820,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         RBC_CUDA(cudaMemset(h->ticket, 0, sizeof(unsigned int)));
         RBC_CUDA(cudaMemset(h->step_counter, 0, sizeof(long long)));
         RBC_CUDA(cudaMemset(h->err, 0, sizeof(int)));
-        RBC_CUDA(cudaMemset(h->ring, 0, 4 * (size_t)h->ring_cap * sizeof(double)));
+        RBC_CUDA(cudaMemset(h->ring, 0, 4 * ((size_t)h->ring_cap + 1) * sizeof(double)));
         RBC_CUDA(cudaMemset(h->th, 0, plane * L * sizeof(double2)));
         RBC_CUDA(cudaMemset(h->f, 0, plane * L * sizeof(double2)));
         RBC_CUDA(cudaMemset(h->g, 0, plane * L * sizeof(double2)));
@@ -1025,8 +1025,7 @@ rbc_status rbc_step_async(rbc_handle* h, int nsteps)
 rbc_status rbc_synchronize(rbc_handle* h)
 {
     RBC_GUARD(h)
-    RBC_CUDA(cudaStreamSynchronize(h->stream));
-    return check_err(h);
+    return check_err(h); // its read of the error word waits for all work on the stream
     RBC_GUARD_END(h)
 }
 
@@ -1276,26 +1275,31 @@ rbc_status rbc_synthesis(rbc_handle* h, double* out)
 
 rbc_status rbc_diagnostics(rbc_handle* h, rbc_diag* out)
 {
-    int n = 0;
     if (!out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
-    rbc_status s = rbc_diag_history(h, out, 1, &n);
-    if (s != RBC_OK) return s;
-    if (n == 0) {
-        // no step yet: Nu_wall of the current state only
-        RBC_GUARD(h)
-        std::vector<double2> t((size_t)h->G.L * h->G.ckp * h->G.ny);
-        RBC_CUDA(cudaMemcpyAsync(t.data(), h->th, t.size() * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
-        RBC_CUDA(cudaStreamSynchronize(h->stream));
-        double nu = 1.0;
-        for (int k = 0; k < h->G.L; ++k) nu -= (k + 1) * kPi * t[(size_t)k * h->G.ckp * h->G.ny].x;
-        out->nu_wall = nu;
-        out->nu_vol = NAN;
-        out->ke = NAN;
-        out->step = 0;
+    RBC_GUARD(h)
+    // the update kernel keeps the newest entry after the ring: one read
+    double last[4];
+    RBC_CUDA(cudaMemcpyAsync(last, h->ring + 4 * (size_t)h->ring_cap, sizeof(last), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    if (last[3] > 0) {
+        out->nu_wall = last[0];
+        out->nu_vol = last[1];
+        out->ke = last[2];
+        out->step = (long long)last[3];
         return RBC_OK;
-        RBC_GUARD_END(h)
     }
+    // no step yet: Nu_wall of the current state only
+    std::vector<double2> t((size_t)h->G.L * h->G.ckp * h->G.ny);
+    RBC_CUDA(cudaMemcpyAsync(t.data(), h->th, t.size() * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    double nu = 1.0;
+    for (int k = 0; k < h->G.L; ++k) nu -= (k + 1) * kPi * t[(size_t)k * h->G.ckp * h->G.ny].x;
+    out->nu_wall = nu;
+    out->nu_vol = NAN;
+    out->ke = NAN;
+    out->step = 0;
     return RBC_OK;
+    RBC_GUARD_END(h)
 }
 
 rbc_status rbc_diag_history(rbc_handle* h, rbc_diag* out, int n, int* count)
@@ -1307,16 +1311,23 @@ rbc_status rbc_diag_history(rbc_handle* h, rbc_diag* out, int n, int* count)
     RBC_CUDA(cudaStreamSynchronize(h->stream));
     long long avail = steps < h->ring_cap ? steps : h->ring_cap;
     if (avail > n) avail = n;
-    std::vector<double> slot(4);
-    for (long long i = 0; i < avail; ++i) {
-        const long long s = steps - avail + 1 + i; // 1-based step number
-        RBC_CUDA(cudaMemcpyAsync(slot.data(), h->ring + 4 * (size_t)((s - 1) % h->ring_cap), 4 * sizeof(double),
+    // the newest `avail` entries are ring slots (steps - avail) .. (steps - 1) mod cap: at
+    // most two contiguous pieces
+    std::vector<double> buf(4 * (size_t)avail);
+    const long long first = (steps - avail) % h->ring_cap;
+    const long long n1 = std::min<long long>(avail, h->ring_cap - first);
+    if (n1 > 0)
+        RBC_CUDA(cudaMemcpyAsync(buf.data(), h->ring + 4 * (size_t)first, 4 * n1 * sizeof(double),
                                  cudaMemcpyDeviceToHost, h->stream));
-        RBC_CUDA(cudaStreamSynchronize(h->stream));
-        out[i].nu_wall = slot[0];
-        out[i].nu_vol = slot[1];
-        out[i].ke = slot[2];
-        out[i].step = (long long)slot[3];
+    if (avail > n1)
+        RBC_CUDA(cudaMemcpyAsync(buf.data() + 4 * n1, h->ring, 4 * (avail - n1) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    for (long long i = 0; i < avail; ++i) {
+        out[i].nu_wall = buf[4 * i];
+        out[i].nu_vol = buf[4 * i + 1];
+        out[i].ke = buf[4 * i + 2];
+        out[i].step = (long long)buf[4 * i + 3];
     }
     *count = (int)avail;
     return RBC_OK;

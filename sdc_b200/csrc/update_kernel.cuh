@@ -35,7 +35,7 @@ struct UpdateArgs {
     double* partial;           // [gridDim.x][2]
     unsigned int* ticket;      // last-block counter (self-resetting)
     double* th00;              // [L] Re theta(q=0) after the step
-    double* ring;              // [cap][4] = nu_wall, nu_vol, ke, step
+    double* ring;              // [cap + 1][4] = nu_wall, nu_vol, ke, step; entry cap = newest
     int ring_cap;
     long long* step_counter;
     int* err;
@@ -270,6 +270,12 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
         slot[1] = 1.0 + b;
         slot[2] = 0.5 * a;
         slot[3] = (double)s;
+        // the newest entry again, after the ring: one read gives the latest diagnostics
+        double* last = A.ring + 4 * (size_t)A.ring_cap;
+        last[0] = nuw;
+        last[1] = 1.0 + b;
+        last[2] = 0.5 * a;
+        last[3] = (double)s;
         *A.ticket = 0u;
     }
 }

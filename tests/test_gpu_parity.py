@@ -163,6 +163,24 @@ def test_diagnostics_match_oracle():
     assert hist.shape == (5, 4) and list(hist[:, 3]) == [1, 2, 3, 4, 5]
 
 
+def test_diag_history_ring_wraps():
+    """With a ring of 8 entries and 21 steps the history returns the newest 8 in step
+    order across the wrap, and the last equals rbc_diagnostics; before any step the
+    diagnostics hold only Nu_wall of the current state."""
+    case = SMALL_CASES[2]
+    s = sdc_b200.Solver(*case, diag_capacity=8)
+    nx, ny, L = case[:3]
+    s.set_state(*random_state(nx, ny, L, seed=22, amp=0.05))
+    d0 = s.diagnostics()
+    assert d0["step"] == 0 and np.isfinite(d0["nu_wall"]) and np.isnan(d0["ke"])
+    s.step(21)
+    hist = s.diag_history(20)
+    assert hist.shape == (8, 4) and list(hist[:, 3]) == list(range(14, 22))
+    d = s.diagnostics()
+    assert d["step"] == 21 and d["nu_wall"] == hist[-1, 0] and d["ke"] == hist[-1, 2]
+    assert s.diag_history(3).shape == (3, 4)
+
+
 @pytest.mark.parametrize("z", [0.0, 0.23])
 def test_spectrum_matches_oracle(z):
     case = SMALL_CASES[4]
@@ -196,6 +214,24 @@ def test_tracers_match_oracle():
     assert np.abs(got - xyz).max() > 1e-6  # they moved
     for name, a, b in zip(("theta", "f", "g", "F", "G"), s.get_state(), o.get_state()):
         assert rel_err(a, b) < 1e-10
+
+
+def test_tracers_match_oracle_over_40_steps():
+    """Tracer positions after 40 steps (graph-replayed steps with the advance on the side
+    stream) still match the oracle."""
+    case = (64, 64, 4, 8.0, 8.0, 3000.0, 1.0, 1e-3)
+    n = 4096
+    s, o = make_pair(case, n_tracers=n)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=43, amp=0.05)
+    s.set_state(*st)
+    o.set_state(*st)
+    xyz = oracle.tracer_positions(3, n, case[3], case[4])
+    s.tracers_set(xyz)
+    o.tracers_set(xyz)
+    s.step(40)
+    o.step(40)
+    assert np.abs(s.tracers_get() - o.tracers_get()).max() < 1e-9
 
 
 def test_tracer_seed_matches_oracle_generator():
