@@ -103,6 +103,7 @@ struct rbc_handle {
     int trk_cap = 0, trk_period = 1;
     long long trk_next = 0;       // step of the oldest unread frame (a multiple of trk_period)
     double* trsums = nullptr;     // [4] moment sums
+    long long* tr_step = nullptr; // step counter as of the tracer advance (see snapshot_step)
     // the tracer advance runs on a side stream, forked after the contraction and joined
     // after the update, so that it overlaps the analysis FFTs and the update
     cudaStream_t side = nullptr;
@@ -362,6 +363,14 @@ static void join_tracer(rbc_handle* h)
     h->join_pending = false;
 }
 
+// The tracer advance of step m reads m (diffusion noise, track frame) while, on the side
+// stream, the update kernel of the step it overlaps increments the step counter: the
+// advance reads a copy taken on the main stream before the fork.
+static void snapshot_step(rbc_handle* h)
+{
+    RBC_CUDA(cudaMemcpyAsync(h->tr_step, h->step_counter, sizeof(long long), cudaMemcpyDeviceToDevice, h->stream));
+}
+
 // Forward x and y transforms of the contracted groups (after the contraction). With a
 // pending tracer advance the tracer kernel is forked onto the side stream right after
 // the contraction that wrote its node records; defer_join leaves the join to the caller
@@ -371,6 +380,7 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     typedef typename cplx_t<R>::type C;
     RBC_DISPATCH_L(launch_contract, R, G.L, h);
     if (h->tracer_pending) {
+        snapshot_step(h);
         if (h->side && !h->profiling) {
             RBC_CUDA(cudaEventRecord(h->ev_fork, h->stream));
             RBC_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
@@ -451,6 +461,7 @@ static void tracer_setup(rbc_handle* h)
     h->nv = dalloc<unsigned char>((size_t)h->G.P * ((5 * L + 1) & ~1) * rsz, h->owned);
     RBC_CUDA(cudaMemset(h->trpos, 0, 3 * (size_t)h->ntr * sizeof(double)));
     h->trsums = dalloc<double>(4, h->owned);
+    h->tr_step = dalloc<long long>(1, h->owned);
     RBC_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
     RBC_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     RBC_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
@@ -510,7 +521,7 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.zmax = 0.5f - 1e-3;
     A.sigma = h->tr_sigma;
     A.noise_seed = h->prm.noise_seed;
-    A.step_counter = h->step_counter;
+    A.step_counter = h->tr_step;
     A.track = h->trk;
     A.track_cap = h->trk_cap;
     A.track_period = h->trk_period;
@@ -547,6 +558,7 @@ template <typename R> static void flush_tracers_t(rbc_handle* h)
     if (!h->tracer_pending) return;
     run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
     RBC_DISPATCH_L(launch_contract, R, h->G.L, h); // writes the node records
+    snapshot_step(h);
     launch_tracer_from_synthesis<R>(h);
     h->tracer_pending = false;
 }
