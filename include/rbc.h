@@ -229,7 +229,10 @@ rbc_status rbc_track_write(const char* path, const char* description, const floa
                            const unsigned int* times, int nframes, int n);
 
 /* --- diagnostics --------------------------------------------------------------- */
-/* Diagnostics of the latest step (or of the initial state before any step). */
+/* Diagnostics of the latest step (or of the initial state before any step). Waits for the
+ * handle's stream and, like rbc_synchronize, returns RBC_ERR_NAN once a non-finite value
+ * has appeared: rbc_step_async followed by rbc_diagnostics advances and reads the result
+ * with one host wait. */
 rbc_status rbc_diagnostics(rbc_handle* h, rbc_diag* out);
 /* The last min(n, steps, capacity) per-step entries, oldest first; *count receives the
  * number written. */

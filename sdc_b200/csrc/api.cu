@@ -1289,10 +1289,15 @@ rbc_status rbc_diagnostics(rbc_handle* h, rbc_diag* out)
 {
     if (!out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
     RBC_GUARD(h)
-    // the update kernel keeps the newest entry after the ring: one read
+    // the update kernel keeps the newest entry after the ring; it and the error word are
+    // read with one wait for the stream
     double last[4];
+    int e = 0;
     RBC_CUDA(cudaMemcpyAsync(last, h->ring + 4 * (size_t)h->ring_cap, sizeof(last), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaMemcpyAsync(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     RBC_CUDA(cudaStreamSynchronize(h->stream));
+    if (e & RBC_DEVERR_NAN) return fail(h, RBC_ERR_NAN, "non-finite value in the state");
+    if (e) return fail(h, RBC_ERR_CUDA, "device error word set");
     if (last[3] > 0) {
         out->nu_wall = last[0];
         out->nu_vol = last[1];

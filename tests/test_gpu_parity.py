@@ -266,6 +266,13 @@ def test_nan_in_state_reported():
     with pytest.raises(sdc_b200.RBCError) as e:
         s.step(2)
     assert e.value.status == 3
+    # the one-wait pattern (enqueue, then read the diagnostics) reports it as well
+    s2, _ = make_pair(C1)
+    s2.set_state(*st)
+    s2.step_async(2)
+    with pytest.raises(sdc_b200.RBCError) as e2:
+        s2.diagnostics()
+    assert e2.value.status == 3
 
 
 def test_kernel_launch_count():
