@@ -240,6 +240,10 @@ def mixed_form(s64, stream, args, local, world):
 SURR = dict(nx=128, ny=128, nz=6, lx=16.0, ly=16.0, pr=1.0, dt=5e-4)
 SURR_NET = dict(nq=12, width=32, modes=16, layers=4, hidden=128)
 SURR_INTERVAL = 40
+# The same surrogate on the plain step's own 256 x 256 x 8 grid (Lx = Ly = 32, Pr = 0.9,
+# rollout at its Ra = 5000; without tracers): 16 collocation levels, fewer runs.
+SURR_C2 = dict(nx=256, ny=256, nz=8, lx=32.0, ly=32.0, pr=0.9, dt=5e-4)
+SURR_C2_NET = dict(nq=16, width=32, modes=16, layers=4, hidden=128)
 
 
 def nu_wall_of(state):
@@ -249,11 +253,10 @@ def nu_wall_of(state):
     return 1.0 - sum((k + 1) * np.pi * th[k, 0, 0].real for k in range(th.shape[0]))
 
 
-def spun_up_states(ras, seeds, local, t_spin=10.0, dt_spin=1e-3):
-    """States of the surrogate grid after t_spin time units from seeded perturbations, one
+def spun_up_states(ras, seeds, local, t_spin=10.0, dt_spin=1e-3, c=SURR):
+    """States of the surrogate grid c after t_spin time units from seeded perturbations, one
     per (Ra, seed), advanced together as one ensemble (concurrent CUDA-graph branches)."""
     import sdc_b200
-    c = SURR
     cfg = [(c["nx"], c["ny"], c["nz"], c["lx"], c["ly"], float(ra), c["pr"], dt_spin) for ra in ras]
     e = sdc_b200.Ensemble(cfg, nstreams=16, device=local)
     for m, sd in zip(e.members, seeds):
@@ -264,12 +267,11 @@ def spun_up_states(ras, seeds, local, t_spin=10.0, dt_spin=1e-3):
     return out
 
 
-def snapshot_pairs(f, ras, starts, nsnap, local, slot0=0):
+def snapshot_pairs(f, ras, starts, nsnap, local, slot0=0, c=SURR):
     """Captures nsnap snapshots, SURR_INTERVAL plain steps apart, of one run per (Ra, start
-    state) into the surrogate's store from slot0 on; the runs advance together as one
-    ensemble. Returns the (src, dst) slot pairs of consecutive snapshots."""
+    state) on grid c into the surrogate's store from slot0 on; the runs advance together
+    as one ensemble. Returns the (src, dst) slot pairs of consecutive snapshots."""
     import sdc_b200
-    c = SURR
     cfg = [(c["nx"], c["ny"], c["nz"], c["lx"], c["ly"], float(ra), c["pr"], c["dt"]) for ra in ras]
     e = sdc_b200.Ensemble(cfg, nstreams=16, device=local)
     for m, st in zip(e.members, starts):
@@ -289,31 +291,30 @@ def snapshot_pairs(f, ras, starts, nsnap, local, slot0=0):
 
 
 def surrogate_form(local, epochs=80, ntraj=50, nsnap=41, n_intervals=200, judge_every=10, augment=2,
-                   noise_rel=0.0, physics_mean=True):
-    """Trains the surrogate on ntraj * (nsnap - 1) snapshot pairs of the plain solver at
-    Ra ~ U[2500, 6000], Pr = 1 (runs spun up for 10 time units from seeded perturbations),
-    then times a rollout at Ra = 4500 from a held-out state: the surrogate with the plain
+                   noise_rel=0.0, physics_mean=True, c=SURR, net=SURR_NET, batch=16, ra=4500.0):
+    """Trains the surrogate on ntraj * (nsnap - 1) snapshot pairs of the plain solver on
+    grid c at Ra ~ U[2500, 6000] (runs spun up for 10 time units from seeded perturbations),
+    then times a rollout at Ra = ra from a held-out state: the surrogate with the plain
     step judging every judge_every-th interval (Nu_wall tolerance 1e-3) against the plain
     step alone over the same sim time."""
     import numpy as np
     import torch
     import sdc_b200
-    c = SURR
-    f = sdc_b200.FNO(c["nx"], c["ny"], c["nz"], max_batch=16, device=local, seed=7, interval_steps=SURR_INTERVAL,
-                     physics_mean=physics_mean, **SURR_NET)
+    f = sdc_b200.FNO(c["nx"], c["ny"], c["nz"], max_batch=batch, device=local, seed=7, interval_steps=SURR_INTERVAL,
+                     physics_mean=physics_mean, **net)
     f.reserve(ntraj * nsnap)
     ras = np.random.default_rng(11).uniform(2500.0, 6000.0, ntraj)
     t0 = time.perf_counter()
-    starts = spun_up_states(ras, 100 + np.arange(ntraj), local)
-    src, dst = snapshot_pairs(f, ras, starts, nsnap, local)
+    starts = spun_up_states(ras, 100 + np.arange(ntraj), local, c=c)
+    src, dst = snapshot_pairs(f, ras, starts, nsnap, local, c=c)
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    f.set_train_options(augment=augment, noise_rel=noise_rel)
-    losses = f.train(src, dst, epochs=epochs, batch=16, lr=1e-3, seed=3)
+    f.set_train_options(augment=augment if c["nx"] == c["ny"] and c["lx"] == c["ly"] else min(augment, 1),
+                        noise_rel=noise_rel)
+    losses = f.train(src, dst, epochs=epochs, batch=batch, lr=1e-3, seed=3)
     train_s = time.perf_counter() - t0
 
-    ra = 4500.0
-    st0 = spun_up_states([ra], [999], local)[0]
+    st0 = spun_up_states([ra], [999], local, c=c)[0]
     stream = torch.cuda.Stream()
     nsteps = n_intervals * SURR_INTERVAL
     mk = lambda: sdc_b200.Solver(c["nx"], c["ny"], c["nz"], c["lx"], c["ly"], ra, c["pr"], c["dt"], device=local,
@@ -375,7 +376,7 @@ def surrogate_form(local, epochs=80, ntraj=50, nsnap=41, n_intervals=200, judge_
     # the same rollout without the learned part: zero increment from the network (the
     # fluctuations persist), mean modes still advanced by the plain recursion
     g = sdc_b200.FNO(c["nx"], c["ny"], c["nz"], max_batch=1, device=local, seed=7, interval_steps=SURR_INTERVAL,
-                     physics_mean=physics_mean, **SURR_NET)
+                     physics_mean=physics_mean, **net)
     g.set_params(np.zeros(g.num_params, np.float32))
     C = g.C
     g.set_norm(np.stack([np.zeros(C), np.ones(C), np.zeros(C), np.ones(C)]).astype(np.float32))
@@ -383,16 +384,19 @@ def surrogate_form(local, epochs=80, ntraj=50, nsnap=41, n_intervals=200, judge_
     g.close()
     plain.close()
     f.close()
-    return {"config": "FNO 4 layers x width 32, 16 modes, (theta,u,v,w) at 12 levels of 128x128x6, "
-                      "Lx=Ly=16, Pr=1; interval 40 steps of dt=5e-4; rollout Ra=4500, judge every %d "
-                      "intervals (Nu tol 1e-3, fallback %d intervals)" % (judge_every, judge_every),
+    return {"config": "FNO %d layers x width %d, %d modes, (theta,u,v,w) at %d levels of %dx%dx%d, "
+                      "Lx=Ly=%g, Pr=%g; interval 40 steps of dt=%g; %d pairs from %d runs at Ra U[2500,6000]; "
+                      "rollout Ra=%g without tracers, judge every %d intervals (Nu tol 1e-3, fallback %d "
+                      "intervals)" % (net["layers"], net["width"], net["modes"], net["nq"], c["nx"], c["ny"],
+                                      c["nz"], c["lx"], c["pr"], c["dt"], len(src), ntraj, ra, judge_every,
+                                      judge_every),
             "value": rep["sim_time_per_s"], "unit": "sim-time/s",
             "plain_value": sim_t / (ms_plain * 1e-3), "speedup_vs_plain": ms_plain / rep["ms"],
             "sim_time": sim_t, "nu_wall_plain": nu_plain, "nu_err_vs_plain": rep["nu_err_vs_plain"],
             "nu_mean_err_vs_plain": rep["nu_mean_err_vs_plain"],
             "nu_mean_err_le_1e-3": bool(rep["nu_mean_err_vs_plain"] <= 1e-3), "report": rep,
             "one_interval_err_vs_increment": one_interval_err, "zero_increment_report": rep0,
-            "train": {"pairs": len(src), "runs": ntraj, "epochs": epochs, "batch": 16, "augment": augment,
+            "train": {"pairs": len(src), "runs": ntraj, "epochs": epochs, "batch": batch, "augment": augment,
                       "noise_rel": noise_rel, "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
                       "seconds": train_s, "data_seconds": gen_s},
             "dtype": "bf16 GEMMs, f32 accumulate/loss/Adam; f64 state and judge"}
@@ -608,6 +612,8 @@ def main():
             forms["batched"] = batched_form(local)
         if not args.no_surrogate:
             forms["surrogate"] = surrogate_form(local, epochs=args.surrogate_epochs)
+            forms["surrogate_256x256x8"] = surrogate_form(local, epochs=60, ntraj=20, nsnap=41, c=SURR_C2,
+                                                          net=SURR_C2_NET, batch=8, ra=WORK["ra"])
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
