@@ -310,6 +310,18 @@ rbc_status rbc_nonlinear_noalloc(int device, int nx, int ny, int nz, double lx, 
 /* Device kernel launches issued by the last rbc_step call (for launch accounting). */
 long long rbc_kernel_launches(const rbc_handle* h);
 
+/* Second-order structure function of a mid-plane field over nsamples displacements
+ * r_i = r_min + i (r_max - r_min) / nsamples along x (direction 0) or y (1), i < nsamples:
+ * out[i] = sum over the half spectrum of |FFT[a(x + r) - a(x)] / P|^2. Replaces
+ * structure_function_2d::calculate_{temperature,u_1,u_2}_structure_function_{x,y}
+ * (gpu_flow/code/postProcessing/structure_function_2d.h:19-54, .cu:32-405), with its field
+ * definitions: field 0 theta from mode 0 only, 1 u_1, 2 u_2 from C'_1, C'_2 at z = 0 (its
+ * literal lambdas) and mode 0 of g. The reference's result is complex with a zero imaginary
+ * part; the real part is returned. */
+typedef enum { RBC_SF_THETA = 0, RBC_SF_U1 = 1, RBC_SF_U2 = 2 } rbc_sf_field;
+rbc_status rbc_structure_function(rbc_handle* h, int field, int direction, double r_min, double r_max,
+                                  int nsamples, double* out);
+
 /* --- learned surrogate ----------------------------------------------------------- */
 /* No counterpart in the reference (jceyy/sdc has no learned component). A Fourier neural
  * operator over the horizontal plane advances a solver's state by one surrogate interval

@@ -76,7 +76,7 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_fno_get_params", "rbc_fno_set_params", "rbc_fno_get_norm", "rbc_fno_set_norm", "rbc_fno_forward",
            "rbc_fno_loss_grad", "rbc_fno_colloc_get", "rbc_fno_colloc_add", "rbc_fno_dataset_reserve",
            "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run",
-           "rbc_fno_set_train_options"]
+           "rbc_fno_set_train_options", "rbc_structure_function"]
 INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
 TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
@@ -146,6 +146,8 @@ def lib():
     L.rbc_launch_config.argtypes = [vp, ip, ip]
     L.rbc_kernel_launches.argtypes = [vp]
     L.rbc_kernel_launches.restype = ctypes.c_longlong
+    L.rbc_structure_function.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, _dp]
     L.rbc_fno_create.argtypes = [ctypes.POINTER(_FnoParams), ctypes.POINTER(vp)]
     L.rbc_fno_destroy.argtypes = [vp]
     L.rbc_fno_destroy.restype = None
@@ -444,6 +446,15 @@ class Solver:
         cnt = ctypes.c_int(0)
         self._check(lib().rbc_diag_history(self.h, arr, n, ctypes.byref(cnt)))
         return np.array([(d.nu_wall, d.nu_vol, d.ke, d.step) for d in arr[:cnt.value]]).reshape(-1, 4)
+
+    def structure_function(self, field, direction, r_min, r_max, nsamples):
+        """Second-order structure function of the mid-plane field ("theta", "u1", "u2")
+        along "x" or "y" (rbc_structure_function)."""
+        out = np.zeros(nsamples)
+        fi = {"theta": 0, "u1": 1, "u2": 2}[field]
+        di = {"x": 0, "y": 1}[direction]
+        self._check(lib().rbc_structure_function(self.h, fi, di, r_min, r_max, nsamples, out.ctypes.data_as(_dp)))
+        return out
 
     def spectrum(self, nbins, z=0.0):
         out = np.zeros(nbins)

@@ -227,6 +227,58 @@ __global__ void k_spectrum(const double2* __restrict__ th, Geom G, double z, int
     if (threadIdx.x == 0) bins[b] = red[0];
 }
 
+// Second-order structure functions of the mid-plane fields, one CTA per displacement
+// (structure_function_2d.cu:32-405). The reference forms the spectrum of the shifted
+// difference D(k) = (e^{i k.r} - 1) A(k), transforms it to physical space, raises it to
+// the power order/2 = 1 (its only caller uses order 2), transforms back, scales by 1/P
+// and sums |.|^2 over the half spectrum. For a dealiased state with the Hermitian kx = 0
+// column that round trip is the identity, so the sum is taken directly:
+//   S2(r) = sum_k (2 - 2 cos(k.r)) |A(k)|^2.
+// A(k) is the reference's mid-plane field, including its fixed choices
+// (twiddle_by_shift_*, structure_function_2d.cu:444-656): theta: theta_0 (mode 0 only);
+// u1: i kx sum_{m<2} z_m f_m + i ky g_0; u2: i ky sum_{m<2} z_m f_m - i kx g_0, with
+// z_m = C'_m(0) from its literal lambdas 4.73004074 and 7.85320462. Wavenumber rows
+// r <= Ny/2 count as positive (get_wave_number_by_index_real_matrix_structure_function).
+__global__ void k_structure_function(const double2* __restrict__ th, const double2* __restrict__ f,
+                                     const double2* __restrict__ g, Geom G, int field, int dir, double r_min,
+                                     double r_inc, double* __restrict__ out)
+{
+    const int b = blockIdx.x;
+    const double rd = r_min + b * r_inc;
+    const double r1 = dir == 0 ? rd : 0.0, r2 = dir == 1 ? rd : 0.0;
+    const double la = 4.73004074, lb = 7.85320462;
+    const double z0 = la * sinh(la * 0.0) / cosh(la * 0.5) + la * sin(la * 0.0) / cos(la * 0.5);
+    const double z1 = lb * cosh(lb * 0.0) / sinh(lb * 0.5) - lb * cos(lb * 0.0) / sin(lb * 0.5);
+    const size_t plane = (size_t)G.ckp * G.ny;
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < G.ckeep * G.ny; e += blockDim.x) {
+        const int c = e / G.ny, r = e - c * G.ny;
+        const double kx = c * 2 * kPi / G.lx;
+        const double ky = (r < G.ny / 2 + 1 ? r : r - G.ny) * 2 * kPi / G.ly;
+        const size_t o = (size_t)c * G.ny + r;
+        double2 a;
+        if (field == 0) {
+            a = th[o];
+        } else {
+            double2 fz = f[o] * z0;
+            if (G.L > 1) fz = fz + f[plane + o] * z1;
+            const double2 g0 = g[o];
+            // u1 = i kx fz + i ky g0, u2 = i ky fz - i kx g0
+            a = field == 1 ? make_double2(-(kx * fz.y + ky * g0.y), kx * fz.x + ky * g0.x)
+                           : make_double2(-(ky * fz.y - kx * g0.y), ky * fz.x - kx * g0.x);
+        }
+        acc += (2.0 - 2.0 * cos(kx * r1 + ky * r2)) * (a.x * a.x + a.y * a.y);
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) red[threadIdx.x] += red[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[b] = red[0];
+}
+
 // ------------------------------------------------------------------ dispatch
 template <typename R, int L> static void setup_contract(rbc_handle* h)
 {
@@ -1361,6 +1413,25 @@ rbc_status rbc_spectrum(rbc_handle* h, double z, double* bins, int nbins)
     k_spectrum<<<nbins, 256, 0, h->stream>>>(h->th, h->G, z, nbins, d);
     RBC_CUDA(cudaGetLastError());
     RBC_CUDA(cudaMemcpyAsync(bins, d, nbins * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_structure_function(rbc_handle* h, int field, int direction, double r_min, double r_max,
+                                  int nsamples, double* out)
+{
+    if (!out || nsamples <= 0 || field < 0 || field > 2 || direction < 0 || direction > 1 ||
+        !std::isfinite(r_min) || !std::isfinite(r_max))
+        return fail(h, RBC_ERR_INVALID_ARG, "bad structure-function arguments");
+    RBC_GUARD(h)
+    double* d = reinterpret_cast<double*>(h->N); // scratch: nsamples doubles
+    const size_t cap = 3 * (size_t)h->G.ckp * h->G.ny * h->G.L * (h->mixed ? sizeof(float2) : sizeof(double2));
+    if ((size_t)nsamples * sizeof(double) > cap) throw ArgError{"too many structure-function samples"};
+    const double inc = (r_max - r_min) / nsamples; // the reference's sample spacing
+    k_structure_function<<<nsamples, 256, 0, h->stream>>>(h->th, h->f, h->g, h->G, field, direction, r_min, inc, d);
+    RBC_CUDA(cudaGetLastError());
+    RBC_CUDA(cudaMemcpyAsync(out, d, nsamples * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     RBC_CUDA(cudaStreamSynchronize(h->stream));
     return RBC_OK;
     RBC_GUARD_END(h)

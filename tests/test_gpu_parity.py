@@ -195,6 +195,21 @@ def test_spectrum_matches_oracle(z):
     assert rel_err(a, b) < 1e-12
 
 
+@pytest.mark.parametrize("field", ["theta", "u1", "u2"])
+@pytest.mark.parametrize("direction", ["x", "y"])
+def test_structure_function_matches_oracle(field, direction):
+    """The spectral sum of the library against the reference's FFT round trip (oracle)."""
+    from oracle.structure import structure_function
+    case = (64, 48, 4, 8.0, 6.0, 3000.0, 1.0, 1e-3)
+    s = sdc_b200.Solver(*case)
+    nx, ny, L = case[:3]
+    st = random_state(nx, ny, L, seed=51, amp=1.0)
+    s.set_state(*st)
+    got = s.structure_function(field, direction, 0.1, 3.1, 12)
+    ref = structure_function(st[0], st[1], st[2], field, direction, 0.1, 3.1, 12, nx, case[3], case[4])
+    assert rel_err(got, ref) < 1e-12, rel_err(got, ref)
+
+
 def test_tracers_match_oracle():
     case = (64, 64, 4, 8.0, 8.0, 3000.0, 1.0, 1e-3)
     n = 4096
