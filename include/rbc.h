@@ -66,7 +66,12 @@ typedef struct {
     unsigned long long noise_seed; /* seed of that noise (see rbc_tracers_advance) */
     int track_frames;  /* device ring of recorded tracer positions, in frames (0: no tracks) */
     int track_period;  /* steps between recorded frames (0 or 1: every step) */
+    int field_ops;     /* buffers of the field operators: RBC_FIELD_FREEZE | RBC_FIELD_HEAT
+                          (0: none; see rbc_freeze_mask and rbc_heat_mask) */
 } rbc_params;
+
+#define RBC_FIELD_FREEZE 1 /* frozen planes [3][L][Ny][Nx] and their mask */
+#define RBC_FIELD_HEAT 2   /* heating mask [Ny][Nx] */
 
 /* Diagnostics of the state after a step (no reference counterpart). */
 typedef struct {
@@ -321,6 +326,39 @@ long long rbc_kernel_launches(const rbc_handle* h);
 typedef enum { RBC_SF_THETA = 0, RBC_SF_U1 = 1, RBC_SF_U2 = 2 } rbc_sf_field;
 rbc_status rbc_structure_function(rbc_handle* h, int field, int direction, double r_min, double r_max,
                                   int nsamples, double* out);
+
+/* --- field operators of the iteration loop ----------------------------------------- */
+/* The reference's freeze and heating operators (main.cu:569-590, -freeze_circle N and
+ * -temp_circle N). Both work plane by plane (each vertical mode of a field on its own) on
+ * the physical Nx x Ny grid of the unnormalised C2R, where a mask [Ny][Nx] (row-major,
+ * column = x index) is 1 to keep the current value; then they scale by 1/(Nx Ny) and
+ * return with the unnormalised R2C, which the next step dealiases. Masks:
+ *   RBC_MASK_CIRCLE     1 where (col - cx Nx)^2 + (row - cy Ny)^2 > (size/2 min(Nx, Ny))^2
+ *   RBC_MASK_RECTANGLE  1 where col < size Nx, col > (1 - size) Nx, row < size Ny or
+ *                       row > (1 - size) Ny (a frame of width size around the box)
+ * with (cx, cy) = (0.5, 0.5) for the freeze and (0.2, 0.3) for the heating, as the
+ * reference's kernels fix them. The handle needs the buffers named in
+ * rbc_params.field_ops. A pending tracer advance runs on the state before an operator
+ * changes it; the AB2 history is kept (the reference's stepper keeps its res_1). */
+typedef enum { RBC_MASK_CIRCLE = 0, RBC_MASK_RECTANGLE = 1 } rbc_mask_shape;
+/* Takes the mask and the C2R of theta, f and g (the frozen planes) of the current state.
+ * Replaces freeze_operator::freeze_circle / freeze_rectangle
+ * (gpu_flow/code/operator/freeze_operator.cu:34-111; main.cu calls freeze_circle(0.8)).
+ * The state is left as it is; the reference's out-of-place cuFFT C2R there may overwrite
+ * its input, which cuFFT leaves unspecified. */
+rbc_status rbc_freeze_mask(rbc_handle* h, int shape, double size);
+/* theta, f, g = R2C(mask ? C2R(field) : frozen) / (Nx Ny); F and G untouched. No-op before
+ * rbc_freeze_mask. Replaces freeze_operator::calculate_operator (freeze_operator.cu:120-208). */
+rbc_status rbc_freeze_apply(rbc_handle* h);
+/* Sets the heating mask and increment (the reference adds 1.5/100). Replaces
+ * masktemp::temp_circle / temp_rectangle (gpu_flow/code/operator/masktemp.cu:36-95; main.cu
+ * calls temp_rectangle(0.1)); the reference's unused C2R copy of theta is not taken. */
+rbc_status rbc_heat_mask(rbc_handle* h, int shape, double size, double increment);
+/* theta = R2C(mask ? C2R(theta) : C2R(theta) + increment) / (Nx Ny), every vertical mode.
+ * No-op before rbc_heat_mask. Replaces masktemp::calculate_operator (masktemp.cu:104-157). */
+rbc_status rbc_heat_apply(rbc_handle* h);
+/* Drops the frozen planes and the heating mask (later applies are no-ops again). */
+rbc_status rbc_field_ops_reset(rbc_handle* h);
 
 /* --- learned surrogate ----------------------------------------------------------- */
 /* No counterpart in the reference (jceyy/sdc has no learned component). A Fourier neural

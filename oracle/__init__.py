@@ -77,6 +77,16 @@ def lib():
         L.oracle_tracer_pattern.argtypes = ([ctypes.c_int, ctypes.c_uint64, ctypes.c_int] + [ctypes.c_double] * 6 +
                                             [_dp])
         L.oracle_tracer_pattern.restype = None
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.oracle_field_mask.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 3 + [ip]
+        L.oracle_field_mask.restype = None
+        L.oracle_freeze_mask.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.oracle_freeze_mask.restype = None
+        L.oracle_heat_mask.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.oracle_heat_mask.restype = None
+        for name in ("oracle_freeze_apply", "oracle_heat_apply"):
+            getattr(L, name).argtypes = [ctypes.c_void_p]
+            getattr(L, name).restype = None
         _LIB = L
     return _LIB
 
@@ -110,6 +120,17 @@ def irfft2(a, nx):
     ny = a.shape[0]
     out = np.zeros((ny, nx))
     lib().oracle_irfft2(nx, ny, _ptr(a), _ptr(out))
+    return out
+
+
+MASK_SHAPES = {"circle": 0, "rectangle": 1}
+
+
+def field_mask(nx, ny, shape, cx, cy, size):
+    """Mask [Ny][Nx] of the freeze / heating operators (1 keeps the current value)."""
+    out = np.zeros((ny, nx), np.int32)
+    lib().oracle_field_mask(nx, ny, MASK_SHAPES[shape], cx, cy, size,
+                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
     return out
 
 
@@ -211,6 +232,19 @@ class Oracle:
 
     def step(self, n=1):
         lib().oracle_step(self.h, n)
+
+    # freeze_operator / masktemp of the reference's iteration loop
+    def freeze_mask(self, shape, size):
+        lib().oracle_freeze_mask(self.h, MASK_SHAPES[shape], size)
+
+    def freeze_apply(self):
+        lib().oracle_freeze_apply(self.h)
+
+    def heat_mask(self, shape, size, increment=1.5 / 100):
+        lib().oracle_heat_mask(self.h, MASK_SHAPES[shape], size, increment)
+
+    def heat_apply(self):
+        lib().oracle_heat_apply(self.h)
 
     def nonlinear(self):
         b = self._bufs()

@@ -1205,7 +1205,33 @@ extern "C" {
 
 struct oracle_handle {
     Solver s;
+    // freeze_operator and masktemp (gpu_flow/code/operator/freeze_operator.cu, masktemp.cu)
+    std::vector<int> fmask, hmask;
+    std::vector<double> frozen; // [3][L][Ny][Nx]: C2R of theta, f, g at the freeze
+    bool frozen_set = false, heat_set = false;
+    double heat_inc = 0.0;
 };
+
+// init_mask_physical_space_circle / _rectangle (freeze_operator.cu:261-308,
+// masktemp.cu:211-259) on the row-major [Ny][Nx] grid, col = index % Nx: 1 keeps the
+// current value. The circle's centre is (cx Nx, cy Ny): (0.5, 0.5) in freeze_operator,
+// (0.2, 0.3) in masktemp.
+void oracle_field_mask(int nx, int ny, int shape, double cx, double cy, double size, int* out)
+{
+    for (int i = 0; i < nx * ny; ++i) {
+        const int col = i % nx, row = (i % (nx * ny)) / nx;
+        int m = 0;
+        if (shape == 0) {
+            const double d2 = (col - cx * nx) * (col - cx * nx) + (row - cy * ny) * (row - cy * ny);
+            const int min_len = ny < nx ? ny : nx;
+            const double dmax = size * 0.5 * min_len;
+            if (d2 > dmax * dmax) m = 1;
+        } else {
+            if (col < size * nx || col > (1 - size) * nx || row < size * ny || row > (1 - size) * ny) m = 1;
+        }
+        out[i] = m;
+    }
+}
 
 oracle_handle* oracle_create(int nx, int ny, int L, double lx, double ly, double ra, double pr, double dt, int nthreads)
 {
@@ -1217,6 +1243,70 @@ oracle_handle* oracle_create(int nx, int ny, int L, double lx, double ly, double
     return h;
 }
 void oracle_destroy(oracle_handle* h) { delete h; }
+
+// freeze_operator::freeze_circle / freeze_rectangle -> freeze_mask (freeze_operator.cu:34-111):
+// the mask and the unnormalised C2R of every vertical mode of theta, f and g. The state is
+// not changed here (cuFFT's out-of-place C2R leaves its input unspecified).
+void oracle_freeze_mask(oracle_handle* h, int shape, double size)
+{
+    Solver& s = h->s;
+    const int L = s.p.L, P = s.P;
+    h->fmask.assign(P, 0);
+    oracle_field_mask(s.p.nx, s.p.ny, shape, 0.5, 0.5, size, h->fmask.data());
+    h->frozen.assign((size_t)3 * L * P, 0.0);
+    const std::vector<cd>* fl[3] = {&s.th, &s.f, &s.g};
+    for (int fi = 0; fi < 3; ++fi)
+        for (int k = 0; k < L; ++k) s.fft.c2r(&(*fl[fi])[(size_t)s.S * k], &h->frozen[((size_t)fi * L + k) * P]);
+    h->frozen_set = true;
+}
+
+// The per-point operation of apply_mask (freeze_operator.cu:242-257, masktemp.cu:191-208)
+// between the C2R and the R2C of every vertical mode of the field.
+static void mask_field(Solver& s, std::vector<cd>& a, const std::vector<int>& mask, const double* frozen, double inc)
+{
+    const int L = s.p.L, P = s.P;
+    std::vector<double> x(P);
+    const double factor = 1. / P;
+    for (int k = 0; k < L; ++k) {
+        s.fft.c2r(&a[(size_t)s.S * k], x.data());
+        for (int i = 0; i < P; ++i) {
+            double entry;
+            if (mask[i] == 1) entry = x[i];
+            else entry = frozen ? frozen[(size_t)k * P + i] : x[i] + inc;
+            x[i] = factor * entry;
+        }
+        s.fft.r2c(x.data(), &a[(size_t)s.S * k]);
+    }
+}
+
+// freeze_operator::calculate_operator (freeze_operator.cu:120-208); nothing before a freeze.
+void oracle_freeze_apply(oracle_handle* h)
+{
+    if (!h->frozen_set) return;
+    Solver& s = h->s;
+    const size_t LP = (size_t)s.p.L * s.P;
+    mask_field(s, s.th, h->fmask, &h->frozen[0], 0.0);
+    mask_field(s, s.f, h->fmask, &h->frozen[LP], 0.0);
+    mask_field(s, s.g, h->fmask, &h->frozen[2 * LP], 0.0);
+}
+
+// masktemp::temp_circle / temp_rectangle (masktemp.cu:36-95): the mask (its C2R copy of
+// theta is never read and is not taken).
+void oracle_heat_mask(oracle_handle* h, int shape, double size, double increment)
+{
+    Solver& s = h->s;
+    h->hmask.assign(s.P, 0);
+    oracle_field_mask(s.p.nx, s.p.ny, shape, 0.2, 0.3, size, h->hmask.data());
+    h->heat_inc = increment;
+    h->heat_set = true;
+}
+
+// masktemp::calculate_operator (masktemp.cu:104-157); nothing before the mask is set.
+void oracle_heat_apply(oracle_handle* h)
+{
+    if (!h->heat_set) return;
+    mask_field(h->s, h->s.th, h->hmask, nullptr, h->heat_inc);
+}
 void oracle_set_threads(oracle_handle* h, int n) { h->s.nthreads = n > 0 ? n : 1; }
 
 // state buffers: interleaved complex doubles; theta/f/g [L][Ny][Nx/2+1], F/G [L]

@@ -31,7 +31,7 @@ class _Params(ctypes.Structure):
                 ("pr", ctypes.c_double), ("dt", ctypes.c_double), ("form", ctypes.c_int),
                 ("n_tracers", ctypes.c_int), ("device", ctypes.c_int), ("diag_capacity", ctypes.c_int),
                 ("tune", ctypes.c_int), ("tracer_diffusivity", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong),
-                ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int)]
+                ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int), ("field_ops", ctypes.c_int)]
 
 
 class _Diag(ctypes.Structure):
@@ -76,7 +76,10 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_fno_get_params", "rbc_fno_set_params", "rbc_fno_get_norm", "rbc_fno_set_norm", "rbc_fno_forward",
            "rbc_fno_loss_grad", "rbc_fno_colloc_get", "rbc_fno_colloc_add", "rbc_fno_dataset_reserve",
            "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run",
-           "rbc_fno_set_train_options", "rbc_structure_function"]
+           "rbc_fno_set_train_options", "rbc_structure_function", "rbc_freeze_mask", "rbc_freeze_apply",
+           "rbc_heat_mask", "rbc_heat_apply", "rbc_field_ops_reset"]
+FIELD_OPS = {"freeze": 1, "heat": 2}
+MASK_SHAPES = {"circle": 0, "rectangle": 1}
 INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
 TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
@@ -148,6 +151,11 @@ def lib():
     L.rbc_kernel_launches.restype = ctypes.c_longlong
     L.rbc_structure_function.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_int, _dp]
+    L.rbc_freeze_mask.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.rbc_freeze_apply.argtypes = [vp]
+    L.rbc_heat_mask.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    L.rbc_heat_apply.argtypes = [vp]
+    L.rbc_field_ops_reset.argtypes = [vp]
     L.rbc_fno_create.argtypes = [ctypes.POINTER(_FnoParams), ctypes.POINTER(vp)]
     L.rbc_fno_destroy.argtypes = [vp]
     L.rbc_fno_destroy.restype = None
@@ -219,9 +227,12 @@ def dump_write(path, arr, real_bytes=8):
 
 
 def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False,
-                tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1):
+                tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=()):
+    ops = 0
+    for name in field_ops:
+        ops |= FIELD_OPS[name]
     return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)),
-                   tracer_diffusivity, noise_seed, track_frames, track_period)
+                   tracer_diffusivity, noise_seed, track_frames, track_period, ops)
 
 
 def track_write(path, frames, times, description=""):
@@ -275,7 +286,8 @@ class Solver:
     """One RBC run on one GPU (mirrors the reference's operator set, see include/rbc.h)."""
 
     def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0,
-                 tune=False, tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, _handle=None):
+                 tune=False, tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
+                 _handle=None):
         self.nx, self.ny, self.L = nx, ny, nz
         self.mox = nx // 2 + 1
         self.n_tracers = n_tracers
@@ -286,7 +298,7 @@ class Solver:
             self.h = _handle
             return
         p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune,
-                        tracer_diffusivity, noise_seed, track_frames, track_period)
+                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops)
         h = ctypes.c_void_p()
         st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
         if st != RBC_OK:
@@ -455,6 +467,25 @@ class Solver:
         di = {"x": 0, "y": 1}[direction]
         self._check(lib().rbc_structure_function(self.h, fi, di, r_min, r_max, nsamples, out.ctypes.data_as(_dp)))
         return out
+
+    # field operators of the iteration loop (freeze, heating); field_ops at construction
+    # names the buffers ("freeze", "heat")
+    def freeze_mask(self, shape="circle", size=0.8):
+        """Mask and frozen planes of the current state (freeze_circle / freeze_rectangle)."""
+        self._check(lib().rbc_freeze_mask(self.h, MASK_SHAPES[shape], size))
+
+    def freeze_apply(self):
+        self._check(lib().rbc_freeze_apply(self.h))
+
+    def heat_mask(self, shape="rectangle", size=0.1, increment=1.5 / 100):
+        """Heating mask and increment (temp_rectangle / temp_circle)."""
+        self._check(lib().rbc_heat_mask(self.h, MASK_SHAPES[shape], size, increment))
+
+    def heat_apply(self):
+        self._check(lib().rbc_heat_apply(self.h))
+
+    def field_ops_reset(self):
+        self._check(lib().rbc_field_ops_reset(self.h))
 
     def spectrum(self, nbins, z=0.0):
         out = np.zeros(nbins)

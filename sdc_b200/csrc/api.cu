@@ -9,6 +9,7 @@
 #include "tracer_kernel.cuh"
 #include "update_kernel.cuh"
 #include "colloc_kernels.cuh"
+#include "mask_kernels.cuh"
 #include "solver_internal.h"
 
 #include <algorithm>
@@ -111,6 +112,13 @@ struct rbc_handle {
     bool join_pending = false;
     long long launches = 0;
     int contract_grid = 0, contract_smem = 0;
+    // field operators of the iteration loop (freeze, heating), when rbc_params.field_ops
+    // asks for their buffers
+    unsigned char *fmask = nullptr, *hmask = nullptr; // [Ny][Nx], 1 keeps the current value
+    double* frozen = nullptr;                        // [3][L][Ny][Nx] C2R of theta, f, g
+    bool frozen_set = false, heat_set = false;
+    double heat_inc = 0.0;
+    int mask_nb = 1;                                 // row pairs per k_mask_rows CTA
     // CUDA graphs of one steady-state (AB2) step: [0] without, [1] with the pending
     // tracer advance at its start
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -764,6 +772,72 @@ static void twiddles(int n, std::vector<double2>& tw)
     }
 }
 
+// ------------------------------------------------------------------ field operators
+static size_t smem_mask_cols(const rbc_handle* h)
+{
+    return (size_t)(h->G.ny + h->py.chunk * h->py.stride) * sizeof(double2);
+}
+static size_t smem_mask_rows(const rbc_handle* h, int nb)
+{
+    return (size_t)(h->G.nx + nb * h->px.stride + 2 * nb * h->G.ckeep) * sizeof(double2);
+}
+
+// Buffers of the freeze and heating operators. Their column and row passes use the
+// synthesis scratch H (8 L planes of R complex values; 3 L FP64 planes fit in both forms).
+static void field_ops_setup(rbc_handle* h)
+{
+    const int ops = h->prm.field_ops;
+    if (!ops) return;
+    const Geom& G = h->G;
+    if (ops & RBC_FIELD_FREEZE) {
+        h->fmask = dalloc<unsigned char>((size_t)G.P, h->owned);
+        h->frozen = dalloc<double>((size_t)3 * G.L * G.P, h->owned);
+    }
+    if (ops & RBC_FIELD_HEAT) h->hmask = dalloc<unsigned char>((size_t)G.P, h->owned);
+    int dev = 0, optin = 0;
+    RBC_CUDA(cudaGetDevice(&dev));
+    RBC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    int nb = h->px.chunk;
+    while (nb > 1 && smem_mask_rows(h, nb) > (size_t)optin) nb /= 2;
+    if (smem_mask_rows(h, nb) > (size_t)optin || smem_mask_cols(h) > (size_t)optin)
+        throw ArgError{"grid too large for the field operators' shared memory"};
+    h->mask_nb = nb;
+    RBC_CUDA(cudaFuncSetAttribute(k_mask_cols<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_mask_cols<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_mask_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+}
+
+// One operator over the first nfields of (theta, f, g): KM1, KM2 and (unless the pass
+// only takes the frozen planes) KM3.
+static void mask_pass(rbc_handle* h, int nfields, int op, const unsigned char* mask, double increment)
+{
+    const Geom& G = h->G;
+    MaskFields fl{{h->th, h->f, h->g}};
+    const int planes = nfields * G.L;
+    double2* S = static_cast<double2*>(h->H);
+    const int W = h->py.chunk;
+    const dim3 gc((G.ckeep + W - 1) / W, planes);
+    k_mask_cols<1><<<gc, kThreads, smem_mask_cols(h), h->stream>>>(G, W, h->py, h->twy, fl, S);
+    RBC_CUDA(cudaGetLastError());
+    const int nb = h->mask_nb;
+    k_mask_rows<<<dim3((G.ny + 2 * nb - 1) / (2 * nb), planes), kThreads, smem_mask_rows(h, nb), h->stream>>>(
+        G, nb, h->px, h->twx, S, op, mask, h->frozen, increment);
+    RBC_CUDA(cudaGetLastError());
+    h->launches += 2;
+    if (op == MASK_SNAPSHOT) return;
+    k_mask_cols<-1><<<gc, kThreads, smem_mask_cols(h), h->stream>>>(G, W, h->py, h->twy, fl, S);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
+static void make_mask(rbc_handle* h, unsigned char* mask, int shape, double cx, double cy, double size)
+{
+    const int P = h->G.P;
+    k_field_mask<<<(P + 255) / 256, 256, 0, h->stream>>>(mask, h->G.nx, h->G.ny, shape, cx, cy, size);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
 rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
 {
     if (!p || !out) return RBC_ERR_INVALID_ARG;
@@ -774,6 +848,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         p->track_period < 0 || (p->track_frames > 0 && p->n_tracers == 0))
         return RBC_ERR_INVALID_ARG;
     if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED) return RBC_ERR_INVALID_ARG;
+    if (p->field_ops & ~(RBC_FIELD_FREEZE | RBC_FIELD_HEAT)) return RBC_ERR_INVALID_ARG;
     if (!L_supported(p->nz, p->form == RBC_FORM_MIXED)) return RBC_ERR_UNSUPPORTED;
     rbc_handle* h = new rbc_handle;
     h->prm = *p;
@@ -902,6 +977,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
             RBC_DISPATCH_L(setup_contract, double, G.L, h);
         }
         tracer_setup(h);
+        field_ops_setup(h);
         RBC_CUDA(cudaDeviceSynchronize());
         if (p->tune) autotune(h);
     } catch (const CudaError& e) {
@@ -2030,3 +2106,61 @@ rbc_status nu_wall(rbc_handle* h, double* nu)
 }
 
 } // namespace rbcint
+
+// ------------------------------------------------------------------ field operators
+rbc_status rbc_freeze_mask(rbc_handle* h, int shape, double size)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (!h->frozen) return fail(h, RBC_ERR_INVALID_ARG, "handle created without RBC_FIELD_FREEZE");
+    if ((shape != RBC_MASK_CIRCLE && shape != RBC_MASK_RECTANGLE) || !std::isfinite(size))
+        return fail(h, RBC_ERR_INVALID_ARG, "bad mask shape or size");
+    RBC_GUARD(h)
+    make_mask(h, h->fmask, shape, 0.5, 0.5, size);
+    mask_pass(h, 3, MASK_SNAPSHOT, h->fmask, 0.0);
+    h->frozen_set = true;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_freeze_apply(rbc_handle* h)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (!h->frozen_set) return RBC_OK; // freeze_operator::calculate_operator before a freeze
+    RBC_GUARD(h)
+    flush_tracers(h); // a pending tracer advance uses the velocity of the state before the change
+    mask_pass(h, 3, MASK_FREEZE, h->fmask, 0.0);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_heat_mask(rbc_handle* h, int shape, double size, double increment)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (!h->hmask) return fail(h, RBC_ERR_INVALID_ARG, "handle created without RBC_FIELD_HEAT");
+    if ((shape != RBC_MASK_CIRCLE && shape != RBC_MASK_RECTANGLE) || !std::isfinite(size) || !std::isfinite(increment))
+        return fail(h, RBC_ERR_INVALID_ARG, "bad mask shape, size or increment");
+    RBC_GUARD(h)
+    make_mask(h, h->hmask, shape, 0.2, 0.3, size);
+    h->heat_set = true;
+    h->heat_inc = increment;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_heat_apply(rbc_handle* h)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (!h->heat_set) return RBC_OK; // masktemp::calculate_operator before the mask is set
+    RBC_GUARD(h)
+    flush_tracers(h);
+    mask_pass(h, 1, MASK_HEAT, h->hmask, h->heat_inc);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_field_ops_reset(rbc_handle* h)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    h->frozen_set = h->heat_set = false;
+    return RBC_OK;
+}

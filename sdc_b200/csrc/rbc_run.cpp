@@ -18,10 +18,16 @@
 //   -form fp64|mixed     precision form
 //   -diag n              print Nu_wall, Nu_vol, KE every n steps
 //   -real_bytes 4|8      element size of the written dumps (4 = the reference's default)
+//   -freeze_circle N     from iteration N on, hold the field inside the circle of radius 0.8
+//                        (freeze_operator, main.cu:222-223, 569-577)
+//   -temp_circle N       from iteration N + 1 on, heat theta inside the frame of width 0.1 by
+//                        1.5/100 per iteration (masktemp, main.cu:228-229, 580-589)
 // Writes simulation.log (main.cu:402-426) and returns non-zero on any library error.
 #include "rbc.h"
 
+#include <algorithm>
 #include <cmath>
+#include <initializer_list>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -94,6 +100,9 @@ int main(int argc, char** argv)
     const unsigned long long seed = (unsigned long long)a.num("-seed", 1);
     const int diag_every = (int)a.num("-diag", 0);
     const int real_bytes = (int)a.num("-real_bytes", 4);
+    const long long freeze_at = (long long)a.num("-freeze_circle", 0);
+    const long long heat_at = (long long)a.num("-temp_circle", 0);
+    p.field_ops = (freeze_at > 0 ? RBC_FIELD_FREEZE : 0) | (heat_at > 0 ? RBC_FIELD_HEAT : 0);
     const char* dir = a.str("-dir");
     std::string out = dir ? dir : ".";
     if (dir) mkdir(dir, 0755);
@@ -146,7 +155,21 @@ int main(int argc, char** argv)
 
     long long done = 0;
     while (done < iters && !rc) {
+        // iteration i of main.cu:556; the field operators run before its step (main.cu:569-589)
+        const long long i = done + 1;
+        if (freeze_at > 0) {
+            rc |= check(rbc_freeze_apply(h), h, "rbc_freeze_apply");
+            if (i == freeze_at) rc |= check(rbc_freeze_mask(h, RBC_MASK_CIRCLE, 0.8), h, "rbc_freeze_mask");
+        }
+        if (heat_at > 0) {
+            rc |= check(rbc_heat_apply(h), h, "rbc_heat_apply");
+            if (i == heat_at) rc |= check(rbc_heat_mask(h, RBC_MASK_RECTANGLE, 0.1, 1.5 / 100), h, "rbc_heat_mask");
+        }
+        if (rc) break;
         long long chunk = iters - done;
+        // steps run in one call only while no operator acts at their iterations
+        for (long long at : {freeze_at, heat_at})
+            if (at > 0) chunk = std::min(chunk, at > i ? at - i : 1);
         if (write_every > 0) chunk = std::min(chunk, write_every - done % write_every);
         if (diag_every > 0) chunk = std::min(chunk, diag_every - done % diag_every);
         rc |= check(rbc_step(h, (int)chunk), h, "rbc_step");
