@@ -68,7 +68,23 @@ typedef struct {
     int track_period;  /* steps between recorded frames (0 or 1: every step) */
     int field_ops;     /* buffers of the field operators: RBC_FIELD_FREEZE | RBC_FIELD_HEAT
                           (0: none; see rbc_freeze_mask and rbc_heat_mask) */
+    double penalization_eta; /* eta > 0: the penalized nonlinear operator of the reference's
+                          PENALIZED builds (-eta, main.cu:117-123; 0.01 there by default);
+                          0: none */
+    int penalization_mask;   /* rbc_pen_mask: the build target's mask */
 } rbc_params;
+
+/* Masks of the penalized operator (nonlinear_operator_rayleigh_noslip.cu:1653-1738; 1 in
+ * the penalized region, integer arithmetic on the Nx x Ny grid):
+ *   RECTANGLE   a frame 3 points wide (make rectangle, the default)
+ *   CIRCLE      outside the centred circle of radius min(Nx, Ny)/2 - 3 (make circle)
+ *   DISK_ARRAY  3 x 2 disks at the cell centres where the squared distance is below
+ *               min(Nx/6, Ny/4) (make diskarray; the reference compares a squared distance
+ *               with that length)
+ *   EVERYWHERE  every point (the reference's unused init_mask_physical_space_everywhere) */
+typedef enum {
+    RBC_PEN_RECTANGLE = 0, RBC_PEN_CIRCLE = 1, RBC_PEN_DISK_ARRAY = 2, RBC_PEN_EVERYWHERE = 3
+} rbc_pen_mask;
 
 #define RBC_FIELD_FREEZE 1 /* frozen planes [3][L][Ny][Nx] and their mask */
 #define RBC_FIELD_HEAT 2   /* heating mask [Ny][Nx] */

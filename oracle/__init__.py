@@ -84,6 +84,10 @@ def lib():
         L.oracle_freeze_mask.restype = None
         L.oracle_heat_mask.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         L.oracle_heat_mask.restype = None
+        L.oracle_pen_mask.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
+        L.oracle_pen_mask.restype = None
+        L.oracle_set_penalization.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.oracle_set_penalization.restype = None
         for name in ("oracle_freeze_apply", "oracle_heat_apply"):
             getattr(L, name).argtypes = [ctypes.c_void_p]
             getattr(L, name).restype = None
@@ -131,6 +135,16 @@ def field_mask(nx, ny, shape, cx, cy, size):
     out = np.zeros((ny, nx), np.int32)
     lib().oracle_field_mask(nx, ny, MASK_SHAPES[shape], cx, cy, size,
                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    return out
+
+
+PEN_MASKS = {"rectangle": 0, "circle": 1, "disk_array": 2, "everywhere": 3}
+
+
+def pen_mask(nx, ny, kind):
+    """Penalization mask [Ny][Nx] of the PENALIZED builds (1 inside the penalized region)."""
+    out = np.zeros((ny, nx))
+    lib().oracle_pen_mask(nx, ny, PEN_MASKS[kind], _ptr(out))
     return out
 
 
@@ -232,6 +246,10 @@ class Oracle:
 
     def step(self, n=1):
         lib().oracle_step(self.h, n)
+
+    def set_penalization(self, eta, kind="rectangle"):
+        """Penalized nonlinear operator (eta > 0) with the named mask; eta = 0 turns it off."""
+        lib().oracle_set_penalization(self.h, eta, PEN_MASKS[kind])
 
     # freeze_operator / masktemp of the reference's iteration loop
     def freeze_mask(self, shape, size):

@@ -116,7 +116,7 @@ static void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w
 // 2-index tables at i + j*L, 3-index at i + j*L + k*L*L (coeff.h getter order).
 struct Tables {
     int L = 0;
-    std::vector<double> Iac, Ia1;
+    std::vector<double> Iac, Ia1, Ia2;
     std::vector<double> Ibb1, Ib11, I111, Iabc, Iac1, Iaab, Iaa1, Iab2, Ia12;
     double ibbb(int i, int j, int k) const { return -Iabc[i + j * L + k * L * L] - Iabc[i + k * L + j * L * L]; }
     double t3(const std::vector<double>& t, int i, int j, int k) const { return t[i + j * L + k * L * L]; }
@@ -184,6 +184,19 @@ static void build_tables(int L, Tables& T)
     };
     two("ac", T.Iac);
     two("a1", T.Ia1);
+    // Ia2 = int C_i S'_j (penalization terms), closed form with the tabulated lambda
+    // (coeff.cu:143-180): z = lambda_i / pi, tau = 2 z tan(lambda_i / 2) for odd 1-based i,
+    // 2 z cot(lambda_i / 2) for even i; 2 j z^2 tau / (j^4 - z^4) for opposite parities.
+    T.Ia2.assign(L * L, 0.0);
+    for (int i = 1; i <= L; ++i) {
+        const double li = lambda_of(i), zi = li / PI, zi2 = zi * zi;
+        const double tau = (i % 2) ? zi * 2.0 * std::tan(0.5 * li) : zi * 2.0 / std::tan(0.5 * li);
+        for (int j = 1; j <= L; ++j) {
+            if (i % 2 == j % 2) continue;
+            const int j2 = j * j;
+            T.Ia2[(i - 1) + (j - 1) * L] = 2.0 * j * zi2 * tau / (j2 * j2 - zi2 * zi2);
+        }
+    }
     // Iac = int C_i C_j'' has closed forms that follow from C(+-1/2) = C'(+-1/2) = 0
     // (coeff.cu:76-122). The reference evaluates them with the tabulated lambda, which
     // is not an exact root, so they differ from the quadrature of the same functions by
@@ -402,6 +415,9 @@ struct Solver {
     std::vector<cd> th, f, g, F, G;
     std::vector<cd> r_th, r_f, r_g, r_F, r_G; // AB2 history (B^-1 N of previous step)
     bool have_hist = false;
+    // penalization (PENALIZED builds of the reference): eta > 0 turns it on
+    double pen_eta = 0.0;
+    std::vector<double> pen_mask; // [Ny][Nx]
     // per-wavenumber tables [L*L][Ny][mox] as in the reference (row-major m*L+m1)
     std::vector<double> binv_ff, imp_tt, imp_tf, imp_ft, imp_ff;
     long long steps = 0;
@@ -675,6 +691,8 @@ struct Solver {
                 const int j = pair / L, i = pair % L;
                 auto Q = [&](int pi) { return &spec[((size_t)pb * nprod + pi) * S]; };
                 accumulate_pair(i, j, Q, buf, oth, of, og, oF, oG);
+                // the penalized parts follow the products of mode j (:1097-1335)
+                if (pen_eta > 0 && i == L - 1) penalize(j, fld, buf, oth, of, og, oF, oG);
             }
         }
         for (auto& v : oth) v *= -1.0;
@@ -683,6 +701,63 @@ struct Solver {
         for (auto& v : og) v *= s;
         for (auto& v : oF) v *= s;
         for (auto& v : oG) v *= s;
+    }
+
+    // Penalized parts of mode j (nonlinear_operator_rayleigh_noslip.cu:1097-1335): the
+    // spectra of mask * u_j / P for u = u11, u21, u31, u12, u22, theta enter f (all eight
+    // summands, including the four the reference computes under "g" and adds to f as
+    // well, with d_y in its fourth), F, G and theta.
+    void penalize(int j, const std::vector<double>* const* fld, std::vector<cd>& buf, std::vector<cd>& oth,
+                  std::vector<cd>& of, std::vector<cd>& og, std::vector<cd>& oF, std::vector<cd>& oG) const
+    {
+        (void)og;
+        const int L = p.L;
+        const double scale = 1.0 / P, pe = p.pr / pen_eta;
+        // 0 u11, 1 u21, 2 u31, 3 u12, 4 u22, 5 theta
+        static const int src[6] = {0, 1, 2, 3, 4, 5};
+        std::vector<cd> ms((size_t)6 * S);
+        std::vector<double> prd(P);
+        for (int a = 0; a < 6; ++a) {
+            const double* u = &(*fld[src[a]])[(size_t)P * j];
+            for (int x = 0; x < P; ++x) prd[x] = pen_mask[x] * u[x] * scale;
+            fft.r2c(prd.data(), &ms[(size_t)a * S]);
+        }
+        auto M = [&](int a) { return &ms[(size_t)a * S]; };
+        cd* b = buf.data();
+        auto axpy = [&](std::vector<cd>& acc, int k, const cd* x, double C) {
+            cd* q = &acc[(size_t)S * k];
+            for (int e = 0; e < S; ++e) q[e] += x[e] * C;
+        };
+        const Tables& t = T;
+        auto Iac = [&](int a, int c) { return t.Iac[a + c * L]; };
+        auto Ia2 = [&](int a, int c) { return t.Ia2[a + c * L]; };
+        // f
+        d_x(M(0), b, 1);
+        for (int k = 0; k < L; ++k) { double C = Iac(j, k); if (C != 0.0) axpy(of, k, b, pe * C); }
+        d_x(M(3), b, 1);
+        for (int k = 0; k < L; ++k) { double C = Ia2(k, j); if (C != 0.0) axpy(of, k, b, pe * C); }
+        d_y(M(1), b, 1);
+        for (int k = 0; k < L; ++k) { double C = Iac(j, k); if (C != 0.0) axpy(of, k, b, pe * C); }
+        d_y(M(4), b, 1);
+        for (int k = 0; k < L; ++k) { double C = Ia2(k, j); if (C != 0.0) axpy(of, k, b, pe * C); }
+        lap(M(2), b, 1);
+        axpy(of, j, b, -1.0 * pe);
+        // the "g" summands, added to f by the reference
+        d_y(M(0), b, 1);
+        for (int k = 0; k < L; ++k) { double C = -Ia2(j, k); if (C != 0.0) axpy(of, k, b, pe * C); }
+        d_y(M(3), b, 1);
+        axpy(of, j, b, 0.5 * pe);
+        d_x(M(1), b, 1);
+        for (int k = 0; k < L; ++k) { double C = -Ia2(j, k); if (C != 0.0) axpy(of, k, b, -1.0 * pe * C); }
+        d_y(M(4), b, 1);
+        axpy(of, j, b, -0.5 * pe);
+        // F and G: the mean (q = 0) entries
+        for (int k = 0; k < L; ++k) { double C = -Ia2(j, k); if (C != 0.0) oF[k] += M(0)[0] * (pe * C); }
+        oF[j] += M(3)[0] * (0.5 * pe);
+        for (int k = 0; k < L; ++k) { double C = -Ia2(j, k); if (C != 0.0) oG[k] += M(1)[0] * (pe * C); }
+        oG[j] += M(4)[0] * (0.5 * pe);
+        // theta
+        axpy(oth, j, M(5), 0.5 / pen_eta);
     }
 
     template <class QF>
@@ -1244,6 +1319,50 @@ oracle_handle* oracle_create(int nx, int ny, int L, double lx, double ly, double
 }
 void oracle_destroy(oracle_handle* h) { delete h; }
 
+// Penalization masks of the PENALIZED builds (nonlinear_operator_rayleigh_noslip.cu:1653-1738)
+// on [Ny][Nx], col = index % Nx, 1 inside the penalized region:
+//   0 rectangle   a frame 3 points wide (the default build)
+//   1 circle      outside the centred circle of radius min(Nx, Ny)/2 - 3 (-DCIRCLE)
+//   2 disk array  3 x 2 disks, squared distance below min(Nx/6, Ny/4) (-DDISKARRAY)
+//   3 everywhere  1 at every point
+// All in integer arithmetic, as the reference's kernels.
+void oracle_pen_mask(int nx, int ny, int kind, double* out)
+{
+    for (int i = 0; i < nx * ny; ++i) {
+        const int col = i % nx, row = (i % (nx * ny)) / nx;
+        double m = 0.0;
+        if (kind == 0) {
+            if (col < 3 || col > nx - 4 || row < 3 || row > ny - 4) m = 1.0;
+        } else if (kind == 1) {
+            const int d = (col - nx / 2) * (col - nx / 2) + (row - ny / 2) * (row - ny / 2);
+            const int mn = ny < nx ? ny : nx;
+            if (d > (mn / 2 - 3) * (mn / 2 - 3)) m = 1.0;
+        } else if (kind == 2) {
+            const int ndx = 3, ndy = 2;
+            for (int a = 0; a < ndx; ++a)
+                for (int b = 0; b < ndy; ++b) {
+                    const int cx = a * nx / ndx + nx / (ndx * 2), cy = b * ny / ndy + ny / (ndy * 2);
+                    const int d = (cx - col) * (cx - col) + (cy - row) * (cy - row);
+                    int r = nx / (ndx * 2);
+                    if (r > ny / (ndy * 2)) r = ny / (ndy * 2);
+                    if (d < r) m = 1.0;
+                }
+        } else {
+            m = 1.0;
+        }
+        out[i] = m;
+    }
+}
+
+// Turns the penalized operator on (eta > 0, mask kind as oracle_pen_mask) or off (eta 0).
+void oracle_set_penalization(oracle_handle* h, double eta, int kind)
+{
+    Solver& s = h->s;
+    s.pen_eta = eta > 0 ? eta : 0.0;
+    s.pen_mask.assign(s.P, 0.0);
+    if (eta > 0) oracle_pen_mask(s.p.nx, s.p.ny, kind, s.pen_mask.data());
+}
+
 // freeze_operator::freeze_circle / freeze_rectangle -> freeze_mask (freeze_operator.cu:34-111):
 // the mask and the unnormalised C2R of every vertical mode of theta, f and g. The state is
 // not changed here (cuFFT's out-of-place C2R leaves its input unspecified).
@@ -1407,6 +1526,7 @@ int oracle_table(int L, const char* name, double* out)
     const std::vector<double>* v = nullptr;
     if (!strcmp(name, "Iac")) v = &T.Iac;
     else if (!strcmp(name, "Ia1")) v = &T.Ia1;
+    else if (!strcmp(name, "Ia2")) v = &T.Ia2;
     else if (!strcmp(name, "Ibb1")) v = &T.Ibb1;
     else if (!strcmp(name, "Ib11")) v = &T.Ib11;
     else if (!strcmp(name, "I111")) v = &T.I111;

@@ -31,7 +31,8 @@ class _Params(ctypes.Structure):
                 ("pr", ctypes.c_double), ("dt", ctypes.c_double), ("form", ctypes.c_int),
                 ("n_tracers", ctypes.c_int), ("device", ctypes.c_int), ("diag_capacity", ctypes.c_int),
                 ("tune", ctypes.c_int), ("tracer_diffusivity", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong),
-                ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int), ("field_ops", ctypes.c_int)]
+                ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int), ("field_ops", ctypes.c_int),
+                ("penalization_eta", ctypes.c_double), ("penalization_mask", ctypes.c_int)]
 
 
 class _Diag(ctypes.Structure):
@@ -80,6 +81,7 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_heat_mask", "rbc_heat_apply", "rbc_field_ops_reset"]
 FIELD_OPS = {"freeze": 1, "heat": 2}
 MASK_SHAPES = {"circle": 0, "rectangle": 1}
+PEN_MASKS = {"rectangle": 0, "circle": 1, "disk_array": 2, "everywhere": 3}
 INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
 TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
@@ -227,12 +229,15 @@ def dump_write(path, arr, real_bytes=8):
 
 
 def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False,
-                tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=()):
+                tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
+                penalization=None):
+    """penalization: None, or (eta, mask) with mask one of PEN_MASKS."""
     ops = 0
     for name in field_ops:
         ops |= FIELD_OPS[name]
+    eta, kind = penalization if penalization else (0.0, "rectangle")
     return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)),
-                   tracer_diffusivity, noise_seed, track_frames, track_period, ops)
+                   tracer_diffusivity, noise_seed, track_frames, track_period, ops, eta, PEN_MASKS[kind])
 
 
 def track_write(path, frames, times, description=""):
@@ -287,7 +292,7 @@ class Solver:
 
     def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0,
                  tune=False, tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
-                 _handle=None):
+                 penalization=None, _handle=None):
         self.nx, self.ny, self.L = nx, ny, nz
         self.mox = nx // 2 + 1
         self.n_tracers = n_tracers
@@ -298,7 +303,7 @@ class Solver:
             self.h = _handle
             return
         p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune,
-                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops)
+                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops, penalization)
         h = ctypes.c_void_p()
         st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
         if st != RBC_OK:

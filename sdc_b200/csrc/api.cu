@@ -10,6 +10,7 @@
 #include "update_kernel.cuh"
 #include "colloc_kernels.cuh"
 #include "mask_kernels.cuh"
+#include "pen_kernels.cuh"
 #include "solver_internal.h"
 
 #include <algorithm>
@@ -119,6 +120,10 @@ struct rbc_handle {
     bool frozen_set = false, heat_set = false;
     double heat_inc = 0.0;
     int mask_nb = 1;                                 // row pairs per k_mask_rows CTA
+    // penalized operator (rbc_params.penalization_eta > 0)
+    bool penalized = false;
+    double *pen_mask = nullptr, *pen_cf = nullptr, *pen_ia2 = nullptr, *pen_partial = nullptr;
+    int pen_blocks = 0;
     // CUDA graphs of one steady-state (AB2) step: [0] without, [1] with the pending
     // tracer advance at its start
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -435,6 +440,9 @@ static void snapshot_step(rbc_handle* h)
 // pending tracer advance the tracer kernel is forked onto the side stream right after
 // the contraction that wrote its node records; defer_join leaves the join to the caller
 // (run_step joins after the update), otherwise it is joined here.
+template <typename R, int L> static void launch_penalize(rbc_handle* h);
+template <typename R, int L> static void launch_penalize_fg(rbc_handle* h);
+
 template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, bool defer_join = false)
 {
     typedef typename cplx_t<R>::type C;
@@ -454,6 +462,7 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
             launch_tracer_from_synthesis<R>(h);
         }
     }
+    if (h->penalized) RBC_DISPATCH_L(launch_penalize, R, G.L, h);
     const int rows = 13 * G.L * G.ny;
     {
     StageScope sc(h, ST_R2C);
@@ -478,6 +487,7 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     RBC_CUDA(cudaGetLastError());
     }
     h->launches += 2;
+    if (h->penalized) RBC_DISPATCH_L(launch_penalize_fg, R, G.L, h);
     if (!defer_join) join_tracer(h);
 }
 
@@ -713,6 +723,88 @@ static void autotune(rbc_handle* h)
     h->launches = 0;
 }
 
+// ------------------------------------------------------------------ penalization
+// Mask of the reference's PENALIZED builds (see rbc_pen_mask), [Ny][Nx], col = index % Nx.
+static void pen_mask_host(int nx, int ny, int kind, std::vector<double>& m)
+{
+    m.assign((size_t)nx * ny, 0.0);
+    for (int row = 0; row < ny; ++row)
+        for (int col = 0; col < nx; ++col) {
+            bool in = false;
+            if (kind == RBC_PEN_RECTANGLE) {
+                in = col < 3 || col > nx - 4 || row < 3 || row > ny - 4;
+            } else if (kind == RBC_PEN_CIRCLE) {
+                const int mn = std::min(nx, ny);
+                in = (col - nx / 2) * (col - nx / 2) + (row - ny / 2) * (row - ny / 2) > (mn / 2 - 3) * (mn / 2 - 3);
+            } else if (kind == RBC_PEN_DISK_ARRAY) {
+                const int r = std::min(nx / 6, ny / 4);
+                for (int a = 0; a < 3 && !in; ++a)
+                    for (int b = 0; b < 2 && !in; ++b) {
+                        const int cx = a * nx / 3 + nx / 6, cy = b * ny / 2 + ny / 4;
+                        in = (cx - col) * (cx - col) + (cy - row) * (cy - row) < r;
+                    }
+            } else {
+                in = true;
+            }
+            m[(size_t)row * nx + col] = in ? 1.0 : 0.0;
+        }
+}
+
+// Mask, group coefficients (layout of k_penalize) and the partial-sum buffer.
+static void penalization_setup(rbc_handle* h)
+{
+    const rbc_params& p = h->prm;
+    if (!(p.penalization_eta > 0)) return;
+    const Geom& G = h->G;
+    const int L = G.L;
+    std::vector<double> m;
+    pen_mask_host(G.nx, G.ny, p.penalization_mask, m);
+    const double pe = p.pr / p.penalization_eta;
+    const auto& T = h->tab;
+    auto Iac = [&](int a, int c) { return T.Iac[a + c * L]; };
+    auto Ia2 = [&](int a, int c) { return T.Ia2[a + c * L]; };
+    std::vector<double> cf((size_t)2 * L * 4 * L, 0.0);
+    auto at = [&](int g, int k, int f, int j) -> double& { return cf[((size_t)g * L + k) * 4 * L + f * L + j]; };
+    for (int k = 0; k < L; ++k)
+        for (int j = 0; j < L; ++j) {
+            const double d = j == k ? 0.5 * pe : 0.0;
+            at(0, k, 0, j) = pe * Iac(j, k);  // d_x: u11
+            at(0, k, 1, j) = pe * Ia2(j, k);  //      u21 (the reference's third "g" summand)
+            at(0, k, 2, j) = pe * Ia2(k, j);  //      u12
+            at(1, k, 0, j) = -pe * Ia2(j, k); // d_y: u11 (first "g" summand)
+            at(1, k, 1, j) = pe * Iac(j, k);  //      u21
+            at(1, k, 2, j) = d;               //      u12 (second "g" summand)
+            at(1, k, 3, j) = pe * Ia2(k, j) - d; //   u22 (and the fourth "g" summand)
+        }
+    h->pen_mask = dalloc<double>(m.size(), h->owned);
+    RBC_CUDA(cudaMemcpy(h->pen_mask, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->pen_cf = dalloc<double>(cf.size(), h->owned);
+    RBC_CUDA(cudaMemcpy(h->pen_cf, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->pen_ia2 = dalloc<double>(T.Ia2.size(), h->owned);
+    RBC_CUDA(cudaMemcpy(h->pen_ia2, T.Ia2.data(), T.Ia2.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->pen_blocks = (G.P + kPenThreads - 1) / kPenThreads;
+    h->pen_partial = dalloc<double>((size_t)h->pen_blocks * 4 * L, h->owned);
+    h->penalized = true;
+}
+
+template <typename R, int L> static void launch_penalize(rbc_handle* h)
+{
+    const rbc_params& p = h->prm;
+    k_penalize<R, L><<<h->pen_blocks, kPenThreads, 0, h->stream>>>((const R*)h->phys, (R*)h->grp, h->pen_mask,
+                                                                    h->pen_cf, h->G.P, p.pr / p.penalization_eta,
+                                                                    0.5 / p.penalization_eta, h->pen_partial);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
+template <typename R, int L> static void launch_penalize_fg(rbc_handle* h)
+{
+    k_penalize_fg<L><<<1, 64, 0, h->stream>>>(h->pen_partial, h->pen_blocks, h->pen_ia2,
+                                              1.0 / (h->prm.penalization_eta * h->G.P), h->NFG);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -849,6 +941,9 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         return RBC_ERR_INVALID_ARG;
     if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED) return RBC_ERR_INVALID_ARG;
     if (p->field_ops & ~(RBC_FIELD_FREEZE | RBC_FIELD_HEAT)) return RBC_ERR_INVALID_ARG;
+    if (!(p->penalization_eta >= 0 && std::isfinite(p->penalization_eta)) || p->penalization_mask < 0 ||
+        p->penalization_mask > RBC_PEN_EVERYWHERE)
+        return RBC_ERR_INVALID_ARG;
     if (!L_supported(p->nz, p->form == RBC_FORM_MIXED)) return RBC_ERR_UNSUPPORTED;
     rbc_handle* h = new rbc_handle;
     h->prm = *p;
@@ -978,6 +1073,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         }
         tracer_setup(h);
         field_ops_setup(h);
+        penalization_setup(h);
         RBC_CUDA(cudaDeviceSynchronize());
         if (p->tune) autotune(h);
     } catch (const CudaError& e) {
@@ -1519,6 +1615,7 @@ static rbc_status table_by_name(const rbchost::Tables& T, const char* name, doub
     const std::vector<double>* v = nullptr;
     if (!std::strcmp(name, "Iac")) v = &T.Iac;
     else if (!std::strcmp(name, "Ia1")) v = &T.Ia1;
+    else if (!std::strcmp(name, "Ia2")) v = &T.Ia2;
     else if (!std::strcmp(name, "Ibb1")) v = &T.Ibb1;
     else if (!std::strcmp(name, "Ib11")) v = &T.Ib11;
     else if (!std::strcmp(name, "I111")) v = &T.I111;

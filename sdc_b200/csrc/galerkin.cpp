@@ -130,6 +130,22 @@ void build_tables(int L, Tables& T)
             if (std::fabs(e) < 1e-13 * mx) e = 0.0;
     };
     int2(0, 3, T.Ia1);
+    // Ia2 = int C_i S'_j (penalization terms only), in the closed form that follows from
+    // C(+-1/2) = 0, evaluated with the tabulated lambda as the reference does (coeff.cu:143-180):
+    // with z = lambda_i / pi and tau = 2 z tan(lambda_i/2) (odd 1-based i) or 2 z cot(lambda_i/2)
+    // (even i), Ia2(i, j) = 2 j z^2 tau / (j^4 - z^4) for i, j of opposite parity, else 0.
+    T.Ia2.assign(L * L, 0.0);
+    for (int i = 0; i < L; ++i) {
+        const int mi = i + 1;
+        const double li = T.lambda[i], zi = li / kPi, zi2 = zi * zi;
+        const double tau = (mi & 1) ? zi * 2.0 * std::tan(0.5 * li) : zi * 2.0 / std::tan(0.5 * li);
+        for (int j = 0; j < L; ++j) {
+            const int mj = j + 1;
+            if ((mi & 1) == (mj & 1)) continue;
+            const int j2 = mj * mj;
+            T.Ia2[i + j * L] = 2.0 * mj * zi2 * tau / (j2 * j2 - zi2 * zi2);
+        }
+    }
     T.CS = T.Ia1;
     int2(1, 1, T.CpCp);
     int2(0, 0, T.CC);

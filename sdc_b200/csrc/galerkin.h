@@ -11,7 +11,7 @@ namespace rbchost {
 struct Tables {
     int L = 0;
     std::vector<double> lambda;                 // lambda_{m+1}
-    std::vector<double> Iac, Ia1;               // as the reference uses them (Iac closed forms)
+    std::vector<double> Iac, Ia1, Ia2;          // as the reference uses them (Iac closed forms)
     std::vector<double> Ibb1, Ib11, I111, Iabc, Iac1, Iaab, Iaa1, Iab2, Ia12;
     std::vector<double> CpCp, CC, CS;           // exact int C'_i C'_j, int C_i C_j, int C_i S_j (diagnostics)
     double t3(const std::vector<double>& t, int i, int j, int k) const { return t[i + j * L + k * L * L]; }

@@ -22,6 +22,9 @@
 //                        (freeze_operator, main.cu:222-223, 569-577)
 //   -temp_circle N       from iteration N + 1 on, heat theta inside the frame of width 0.1 by
 //                        1.5/100 per iteration (masktemp, main.cu:228-229, 580-589)
+//   -penalized rectangle|circle|diskarray|everywhere   the penalized operator with that mask
+//                        (the reference's PENALIZED build targets)
+//   -eta e               its eta (main.cu:117-123; default 0.01)
 // Writes simulation.log (main.cu:402-426) and returns non-zero on any library error.
 #include "rbc.h"
 
@@ -103,6 +106,17 @@ int main(int argc, char** argv)
     const long long freeze_at = (long long)a.num("-freeze_circle", 0);
     const long long heat_at = (long long)a.num("-temp_circle", 0);
     p.field_ops = (freeze_at > 0 ? RBC_FIELD_FREEZE : 0) | (heat_at > 0 ? RBC_FIELD_HEAT : 0);
+    if (const char* pen = a.str("-penalized")) {
+        static const char* kMasks[] = {"rectangle", "circle", "diskarray", "everywhere"};
+        p.penalization_mask = -1;
+        for (int i = 0; i < 4; ++i)
+            if (!std::strcmp(pen, kMasks[i])) p.penalization_mask = i;
+        if (p.penalization_mask < 0) {
+            std::fprintf(stderr, "unknown -penalized mask %s\n", pen);
+            return 2;
+        }
+        p.penalization_eta = a.num("-eta", 0.01);
+    }
     const char* dir = a.str("-dir");
     std::string out = dir ? dir : ".";
     if (dir) mkdir(dir, 0755);
@@ -144,9 +158,9 @@ int main(int argc, char** argv)
         if (log) {
             std::fprintf(log, "Simulation of Rayleigh-Benard convection (sm_100a)\nRayleigh-Number: %g\nPrandtl-Number: %g\n"
                               "delta t: %g\nfinal t: %g\nnumber of files: %d\nnumber of iterations: %lld\n"
-                              "cube length x direction: %g\ncube length y direction: %g\ncube length z direction: 1\n"
+                              "eta(penalization): %g\ncube length x direction: %g\ncube length y direction: %g\ncube length z direction: 1\n"
                               "number of x modes: %d\nnumber of y modes: %d\nnumber of z modes: %d\ncommand string: ",
-                         p.ra, p.pr, p.dt, tfinal, nfiles, iters, p.lx, p.ly, p.nx, p.ny, p.nz);
+                         p.ra, p.pr, p.dt, tfinal, nfiles, iters, p.penalization_eta, p.lx, p.ly, p.nx, p.ny, p.nz);
             for (int i = 0; i < argc; ++i) std::fprintf(log, "%s ", argv[i]);
             std::fprintf(log, "\n");
             std::fclose(log);

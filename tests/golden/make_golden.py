@@ -14,7 +14,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-NAMES2 = ["Iac", "Ia1"]
+NAMES2 = ["Iac", "Ia1", "Ia2"]
 NAMES3 = ["Ibbb", "Ibb1", "Ib11", "I111", "Iabc", "Iac1", "Iaab", "Iaa1", "Iab2", "Ia12"]
 
 

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 
 @pytest.mark.parametrize("L", [4, 8, 12])
-@pytest.mark.parametrize("name", ["Iac", "Ia1", "Ibbb", "Ibb1", "Ib11", "I111", "Iabc", "Iac1",
+@pytest.mark.parametrize("name", ["Iac", "Ia1", "Ia2", "Ibbb", "Ibb1", "Ib11", "I111", "Iabc", "Iac1",
                                   "Iaab", "Iaa1", "Iab2", "Ia12", "lambda"])
 def test_library_tables_match_reference_golden(L, name):
     ref = np.load(os.path.join(GOLD, f"coeff_L{L}.npz"))[name]

@@ -11,7 +11,7 @@ import oracle
 from tests.helpers import random_state, rel_err
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-NAMES = ["Iac", "Ia1", "Ibbb", "Ibb1", "Ib11", "I111", "Iabc", "Iac1", "Iaab", "Iaa1", "Iab2", "Ia12", "lambda"]
+NAMES = ["Iac", "Ia1", "Ia2", "Ibbb", "Ibb1", "Ib11", "I111", "Iabc", "Iac1", "Iaab", "Iaa1", "Iab2", "Ia12", "lambda"]
 
 
 @pytest.mark.parametrize("L", [4, 8, 12])
