@@ -234,6 +234,64 @@ def mixed_form(s64, stream, args, local, world):
             "fp64_nu_wall": d64["nu_wall"], "nu_err_le_1e-3": bool(err["nu_wall"] <= 1e-3)}
 
 
+def optional_physics_forms(s64, stream, local, steps=2000):
+    """The reference's optional physics on the same workload and state: the penalized
+    operator (PENALIZED build, circle mask, eta = 0.01) as plain steps, and the iteration
+    loop with the freeze (circle 0.8) and the heating (frame 0.1, +1.5/100) before every
+    step, as main.cu:569-616 runs them. ms per iteration against the plain step."""
+    import torch
+    import sdc_b200
+    state = s64.get_state()
+    tr = s64.tracers_get()
+    out = {}
+
+    def timed(run):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    s64.set_state(*state)
+    s64.tracers_set(tr)
+    s64.step(10)
+    plain = timed(lambda: s64.step_async(steps))
+    p = sdc_b200.Solver(**WORK, n_tracers=NTRACERS, device=local, penalization=(0.01, "circle"))
+    p.set_stream(stream.cuda_stream)
+    p.set_state(*state)
+    p.tracers_set(tr)
+    p.step(10)
+    pen = timed(lambda: p.step_async(steps))
+    dp = p.diagnostics()
+    p.close()
+    out["penalized"] = {"ms_per_step": pen, "plain_ms_per_step": plain, "overhead": pen / plain - 1.0,
+                        "mask": "circle", "eta": 0.01, "nu_wall_after": dp["nu_wall"], "steps": steps}
+    f = sdc_b200.Solver(**WORK, n_tracers=NTRACERS, device=local, field_ops=("freeze", "heat"))
+    f.set_stream(stream.cuda_stream)
+    f.set_state(*state)
+    f.tracers_set(tr)
+    f.step(10)
+    f.freeze_mask("circle", 0.8)
+    f.heat_mask("rectangle", 0.1, 1.5 / 100)
+
+    def loop():
+        for _ in range(steps):
+            f.freeze_apply()
+            f.heat_apply()
+            f.step_async(1)
+
+    it = timed(loop)
+    df = f.diagnostics()
+    f.close()
+    out["freeze_heat"] = {"ms_per_iteration": it, "plain_ms_per_step": plain, "overhead": it / plain - 1.0,
+                          "freeze": "circle 0.8", "heat": "frame 0.1, +0.015", "nu_wall_after": df["nu_wall"],
+                          "steps": steps}
+    return out
+
+
 # Learned surrogate (north_star form 4): Fourier neural operator on (theta, u, v, w) at
 # 12 Gauss-Legendre levels of the 128 x 128 x 6 grid (Lx = Ly = 16), one surrogate
 # interval = 40 plain steps of dt = 5e-4 (0.02 time units).
@@ -608,6 +666,7 @@ def main():
     forms = None
     if args.form == "fp64" and not args.no_forms and world == 1:
         forms = {"mixed": mixed_form(s, stream, args, local, world)}
+        forms.update(optional_physics_forms(s, stream, local))
         if not args.no_batched:
             forms["batched"] = batched_form(local)
         if not args.no_surrogate:

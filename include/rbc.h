@@ -88,6 +88,7 @@ typedef enum {
 
 #define RBC_FIELD_FREEZE 1 /* frozen planes [3][L][Ny][Nx] and their mask */
 #define RBC_FIELD_HEAT 2   /* heating mask [Ny][Nx] */
+#define RBC_FIELD_SCALE 4  /* mask of rbc_masker [Ny][Nx] */
 
 /* Diagnostics of the state after a step (no reference counterpart). */
 typedef struct {
@@ -373,6 +374,13 @@ rbc_status rbc_heat_mask(rbc_handle* h, int shape, double size, double increment
 /* theta = R2C(mask ? C2R(theta) : C2R(theta) + increment) / (Nx Ny), every vertical mode.
  * No-op before rbc_heat_mask. Replaces masktemp::calculate_operator (masktemp.cu:104-157). */
 rbc_status rbc_heat_apply(rbc_handle* h);
+/* The interactive temperature mask: theta = R2C(mask ? C2R(theta) : factor C2R(theta)) / (Nx Ny)
+ * for every vertical mode, with mask 1 outside the circle of radius radius/2 min(Nx, Ny)
+ * centred at column y Nx and row x Ny (the reference swaps x and y there). Replaces
+ * masking::set_mask_parameters + masking::masker (gpu_flow/code/operator/masking.cu:24-29,
+ * 78-118), which main.cu calls with the UDP viewer's input (main.cu:676-683; defaults
+ * x = y = 0.5, radius 0.15, factor 1.1). Needs RBC_FIELD_SCALE. */
+rbc_status rbc_masker(rbc_handle* h, double x, double y, double radius, double factor);
 /* Drops the frozen planes and the heating mask (later applies are no-ops again). */
 rbc_status rbc_field_ops_reset(rbc_handle* h);
 

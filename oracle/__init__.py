@@ -88,6 +88,8 @@ def lib():
         L.oracle_pen_mask.restype = None
         L.oracle_set_penalization.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.oracle_set_penalization.restype = None
+        L.oracle_masker.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 4
+        L.oracle_masker.restype = None
         for name in ("oracle_freeze_apply", "oracle_heat_apply"):
             getattr(L, name).argtypes = [ctypes.c_void_p]
             getattr(L, name).restype = None
@@ -263,6 +265,9 @@ class Oracle:
 
     def heat_apply(self):
         lib().oracle_heat_apply(self.h)
+
+    def masker(self, x=0.5, y=0.5, radius=0.15, factor=1.1):
+        lib().oracle_masker(self.h, x, y, radius, factor)
 
     def nonlinear(self):
         b = self._bufs()

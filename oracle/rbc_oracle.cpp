@@ -1381,7 +1381,8 @@ void oracle_freeze_mask(oracle_handle* h, int shape, double size)
 
 // The per-point operation of apply_mask (freeze_operator.cu:242-257, masktemp.cu:191-208)
 // between the C2R and the R2C of every vertical mode of the field.
-static void mask_field(Solver& s, std::vector<cd>& a, const std::vector<int>& mask, const double* frozen, double inc)
+static void mask_field(Solver& s, std::vector<cd>& a, const std::vector<int>& mask, const double* frozen, double inc,
+                       bool scale = false)
 {
     const int L = s.p.L, P = s.P;
     std::vector<double> x(P);
@@ -1389,6 +1390,10 @@ static void mask_field(Solver& s, std::vector<cd>& a, const std::vector<int>& ma
     for (int k = 0; k < L; ++k) {
         s.fft.c2r(&a[(size_t)s.S * k], x.data());
         for (int i = 0; i < P; ++i) {
+            if (scale) { // masking.cu:49-56 (julie_do_the_thing)
+                x[i] = mask[i] == 0 ? factor * x[i] * inc : x[i] * factor;
+                continue;
+            }
             double entry;
             if (mask[i] == 1) entry = x[i];
             else entry = frozen ? frozen[(size_t)k * P + i] : x[i] + inc;
@@ -1418,6 +1423,17 @@ void oracle_heat_mask(oracle_handle* h, int shape, double size, double increment
     oracle_field_mask(s.p.nx, s.p.ny, shape, 0.2, 0.3, size, h->hmask.data());
     h->heat_inc = increment;
     h->heat_set = true;
+}
+
+// masking::set_mask_parameters + masker (masking.cu:24-29, 78-118): theta scaled by `factor`
+// inside the circle of radius `radius` (fraction of min(Nx, Ny)/2) whose centre is column
+// y Nx, row x Ny (init_mask_physical_space_circle there takes c_y for the columns).
+void oracle_masker(oracle_handle* h, double x, double y, double radius, double factor)
+{
+    Solver& s = h->s;
+    std::vector<int> m(s.P);
+    oracle_field_mask(s.p.nx, s.p.ny, 0, y, x, radius, m.data());
+    mask_field(s, s.th, m, nullptr, factor, true);
 }
 
 // masktemp::calculate_operator (masktemp.cu:104-157); nothing before the mask is set.

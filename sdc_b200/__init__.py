@@ -78,8 +78,8 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_fno_loss_grad", "rbc_fno_colloc_get", "rbc_fno_colloc_add", "rbc_fno_dataset_reserve",
            "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run",
            "rbc_fno_set_train_options", "rbc_structure_function", "rbc_freeze_mask", "rbc_freeze_apply",
-           "rbc_heat_mask", "rbc_heat_apply", "rbc_field_ops_reset"]
-FIELD_OPS = {"freeze": 1, "heat": 2}
+           "rbc_heat_mask", "rbc_heat_apply", "rbc_field_ops_reset", "rbc_masker"]
+FIELD_OPS = {"freeze": 1, "heat": 2, "scale": 4}
 MASK_SHAPES = {"circle": 0, "rectangle": 1}
 PEN_MASKS = {"rectangle": 0, "circle": 1, "disk_array": 2, "everywhere": 3}
 INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
@@ -158,6 +158,7 @@ def lib():
     L.rbc_heat_mask.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
     L.rbc_heat_apply.argtypes = [vp]
     L.rbc_field_ops_reset.argtypes = [vp]
+    L.rbc_masker.argtypes = [vp] + [ctypes.c_double] * 4
     L.rbc_fno_create.argtypes = [ctypes.POINTER(_FnoParams), ctypes.POINTER(vp)]
     L.rbc_fno_destroy.argtypes = [vp]
     L.rbc_fno_destroy.restype = None
@@ -488,6 +489,10 @@ class Solver:
 
     def heat_apply(self):
         self._check(lib().rbc_heat_apply(self.h))
+
+    def masker(self, x=0.5, y=0.5, radius=0.15, factor=1.1):
+        """Scales theta by factor inside a circle (masking::masker; field_ops "scale")."""
+        self._check(lib().rbc_masker(self.h, x, y, radius, factor))
 
     def field_ops_reset(self):
         self._check(lib().rbc_field_ops_reset(self.h))

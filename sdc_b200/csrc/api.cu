@@ -115,7 +115,7 @@ struct rbc_handle {
     int contract_grid = 0, contract_smem = 0;
     // field operators of the iteration loop (freeze, heating), when rbc_params.field_ops
     // asks for their buffers
-    unsigned char *fmask = nullptr, *hmask = nullptr; // [Ny][Nx], 1 keeps the current value
+    unsigned char *fmask = nullptr, *hmask = nullptr, *smask = nullptr; // [Ny][Nx], 1 keeps the value
     double* frozen = nullptr;                        // [3][L][Ny][Nx] C2R of theta, f, g
     bool frozen_set = false, heat_set = false;
     double heat_inc = 0.0;
@@ -886,6 +886,7 @@ static void field_ops_setup(rbc_handle* h)
         h->frozen = dalloc<double>((size_t)3 * G.L * G.P, h->owned);
     }
     if (ops & RBC_FIELD_HEAT) h->hmask = dalloc<unsigned char>((size_t)G.P, h->owned);
+    if (ops & RBC_FIELD_SCALE) h->smask = dalloc<unsigned char>((size_t)G.P, h->owned);
     int dev = 0, optin = 0;
     RBC_CUDA(cudaGetDevice(&dev));
     RBC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -940,7 +941,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         p->track_period < 0 || (p->track_frames > 0 && p->n_tracers == 0))
         return RBC_ERR_INVALID_ARG;
     if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED) return RBC_ERR_INVALID_ARG;
-    if (p->field_ops & ~(RBC_FIELD_FREEZE | RBC_FIELD_HEAT)) return RBC_ERR_INVALID_ARG;
+    if (p->field_ops & ~(RBC_FIELD_FREEZE | RBC_FIELD_HEAT | RBC_FIELD_SCALE)) return RBC_ERR_INVALID_ARG;
     if (!(p->penalization_eta >= 0 && std::isfinite(p->penalization_eta)) || p->penalization_mask < 0 ||
         p->penalization_mask > RBC_PEN_EVERYWHERE)
         return RBC_ERR_INVALID_ARG;
@@ -2251,6 +2252,20 @@ rbc_status rbc_heat_apply(rbc_handle* h)
     RBC_GUARD(h)
     flush_tracers(h);
     mask_pass(h, 1, MASK_HEAT, h->hmask, h->heat_inc);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_masker(rbc_handle* h, double x, double y, double radius, double factor)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (!h->smask) return fail(h, RBC_ERR_INVALID_ARG, "handle created without RBC_FIELD_SCALE");
+    if (!std::isfinite(x) || !std::isfinite(y) || !std::isfinite(radius) || !std::isfinite(factor))
+        return fail(h, RBC_ERR_INVALID_ARG, "bad mask position, radius or factor");
+    RBC_GUARD(h)
+    flush_tracers(h); // a pending tracer advance uses the velocity of the state before the change
+    make_mask(h, h->smask, RBC_MASK_CIRCLE, y, x, radius); // column centre y Nx, row centre x Ny
+    mask_pass(h, 1, MASK_SCALE, h->smask, factor);
     return RBC_OK;
     RBC_GUARD_END(h)
 }

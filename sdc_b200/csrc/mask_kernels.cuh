@@ -8,6 +8,7 @@
 // 1/(Nx Ny) and returns with the unnormalised R2C:
 //   freeze   v = mask ? v : frozen        (freeze_operator.cu:242-257)
 //   heating  v = mask ? v : v + increment (masktemp.cu:191-208, increment 1.5/100)
+//   scaling  v = mask ? v : v factor      (masking.cu:43-58, factor 1.1 by default)
 // The frozen planes are the C2R of the state when the freeze was taken
 // (freeze_operator.cu:60-111).
 //
@@ -27,7 +28,7 @@
 
 namespace rbck {
 
-enum MaskOp { MASK_SNAPSHOT = 0, MASK_FREEZE = 1, MASK_HEAT = 2 };
+enum MaskOp { MASK_SNAPSHOT = 0, MASK_FREEZE = 1, MASK_HEAT = 2, MASK_SCALE = 3 };
 
 // Up to three fields of L planes each; plane pl is vertical mode pl % L of field pl / L.
 struct MaskFields {
@@ -95,7 +96,8 @@ __global__ void __launch_bounds__(kThreads) k_mask_cols(Geom G, int W, rbcfft::P
 // rows ya = 2 (blockIdx.x NB + t) and ya + 1 as z = x_a + i x_b. Shared: twiddles [Nx],
 // NB padded transforms, and the staged kept coefficients [ckeep][2 NB].
 // op: MASK_SNAPSHOT writes the C2R of the planes to `frozen` and leaves S alone;
-// MASK_FREEZE / MASK_HEAT apply the operation and write the R2C back into S.
+// MASK_FREEZE / MASK_HEAT / MASK_SCALE apply the operation (increment is the factor of
+// MASK_SCALE) and write the R2C back into S.
 __global__ void __launch_bounds__(kThreads) k_mask_rows(Geom G, int NB, rbcfft::Plan px, const double2* __restrict__ twx,
                                                         double2* __restrict__ S, int op,
                                                         const unsigned char* __restrict__ mask,
@@ -149,6 +151,12 @@ __global__ void __launch_bounds__(kThreads) k_mask_rows(Geom G, int NB, rbcfft::
             continue;
         }
         double va = z.x, vb = z.y;
+        if (op == MASK_SCALE) { // masking.cu:49-56: (1/P) v factor inside the circle
+            va = mask[ia] ? invP * va : invP * va * increment;
+            vb = mask[ib] ? invP * vb : invP * vb * increment;
+            z = make_double2(va, vb);
+            continue;
+        }
         if (!mask[ia]) va = op == MASK_FREEZE ? fr[ia] : va + increment;
         if (!mask[ib]) vb = op == MASK_FREEZE ? fr[ib] : vb + increment;
         z = make_double2(invP * va, invP * vb);

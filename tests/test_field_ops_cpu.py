@@ -130,3 +130,21 @@ def test_freeze_holds_the_inside_of_the_circle_over_steps():
     inside = m == 0
     assert drift_free[inside].mean() < 0.5 * drift_plain[inside].mean()
     assert one > 0
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("x,y,radius,factor", [(0.5, 0.5, 0.15, 1.1), (0.3, 0.7, 0.4, 0.5)])
+def test_masker_matches_numpy(case, x, y, radius, factor):
+    """masking::masker: theta scaled by factor inside the circle whose centre is column
+    y Nx, row x Ny (the reference's kernel takes c_y for the columns)."""
+    nx, ny, L = case[:3]
+    o, st = make(case, 8)
+    o.masker(x, y, radius, factor)
+    got = o.get_state()
+    m = np_mask(nx, ny, "circle", y, x, radius)
+    for k in range(L):
+        xk = c2r(st[0][k], nx)
+        ref = r2c(np.where(m == 0, (1.0 / (nx * ny)) * xk * factor, xk * (1.0 / (nx * ny))))
+        assert rel_err(got[0][k], ref) < 1e-13, k
+    for a, b in zip(got[1:], st[1:]):
+        assert np.array_equal(a, b)

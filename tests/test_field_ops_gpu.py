@@ -186,3 +186,20 @@ def test_cli_driver_field_operators_match_library(tmp_path):
     for name, w in zip(NAMES, s.get_state()):
         got = sdc_b200.dump_read(tmp_path / f"{name}_{12:08d}.bin")
         assert np.array_equal(got.reshape(w.shape), w), name
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("x,y,radius,factor", [(0.5, 0.5, 0.15, 1.1), (0.3, 0.7, 0.4, 0.5)])
+def test_masker_matches_oracle(case, x, y, radius, factor):
+    nx, ny, L = case[:3]
+    s = sdc_b200.Solver(*case, field_ops=("scale",))
+    o = oracle.Oracle(*case, threads=8)
+    st = random_state(nx, ny, L, seed=31, amp=0.05)
+    s.set_state(*st)
+    o.set_state(*st)
+    s.masker(x, y, radius, factor)
+    o.masker(x, y, radius, factor)
+    for name, a, b in zip(NAMES, s.get_state(), dealiased(o.get_state(), nx, ny)):
+        assert rel_err(a, b) < 1e-12, (name, rel_err(a, b))
+    with pytest.raises(sdc_b200.RBCError):
+        sdc_b200.Solver(*case).masker()
