@@ -488,6 +488,29 @@ def profile_surrogate(local):
     print(json.dumps({"profile_surrogate": "done", "nu_wall": s.diagnostics()["nu_wall"]}))
 
 
+def profile_field_ops(local, iters=5):
+    """Small workload for kernel profiling of the optional physics on the plain step's
+    256 x 256 x 8 grid without tracers: `iters` iterations of freeze (circle 0.8) + heating
+    (frame 0.1) + one step, then `iters` penalized nonlinear operators (circle mask,
+    eta = 0.01; the standalone operator launches its kernels outside CUDA graphs)."""
+    import sdc_b200
+    s = sdc_b200.Solver(**WORK, device=local, field_ops=("freeze", "heat"))
+    s.init_fields(SEED, 1e-3, 8.0)
+    s.step(20)
+    s.freeze_mask("circle", 0.8)
+    s.heat_mask("rectangle", 0.1, 1.5 / 100)
+    for _ in range(iters):
+        s.freeze_apply()
+        s.heat_apply()
+        s.step(1)
+    p = sdc_b200.Solver(**WORK, device=local, penalization=(0.01, "circle"))
+    state = s.get_state()
+    for _ in range(iters):
+        n = p.nonlinear(*state)
+    print(json.dumps({"profile_field_ops": "done", "nu_wall": s.diagnostics()["nu_wall"],
+                      "n_theta_00": abs(n[0][0, 0, 0])}))
+
+
 def ensemble_configs(n=64, seed=4):
     """The uneven ensemble: per member a grid from {64, 128, 192, 256}^2, Nz from {4, 6, 8},
     Ra ~ U[2000, 8000], Pr from {0.7, 1, 7}, Lx = Ly = grid / 8, dt = 5e-4 (drawn by seed)."""
@@ -559,10 +582,15 @@ def main():
     ap.add_argument("--surrogate-epochs", type=int, default=80)
     ap.add_argument("--profile-surrogate", action="store_true",
                     help="run only a small surrogate workload (for kernel profiling) and exit")
+    ap.add_argument("--profile-field-ops", action="store_true",
+                    help="run only a small freeze/heating/penalization workload (for kernel profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_surrogate:
         profile_surrogate(int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.profile_field_ops:
+        profile_field_ops(int(os.environ.get("LOCAL_RANK", "0")))
         return
 
     world, rank, local = dist_env()

@@ -317,6 +317,14 @@ template <typename R, int L> static void launch_contract(rbc_handle* h)
     ++h->launches;
 }
 
+template <typename R, int L> static void launch_node_records(rbc_handle* h)
+{
+    const int grid = std::min((h->G.P + 255) / 256, 148 * 8);
+    k_node_records<R, L><<<grid, 256, 0, h->stream>>>((const R*)h->phys, h->G.P, (R*)h->nv);
+    RBC_CUDA(cudaGetLastError());
+    ++h->launches;
+}
+
 template <typename R, int L> static void launch_update(rbc_handle* h)
 {
     UpdateArgs A;
@@ -627,7 +635,7 @@ template <typename R> static void flush_tracers_t(rbc_handle* h)
 {
     if (!h->tracer_pending) return;
     run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
-    RBC_DISPATCH_L(launch_contract, R, h->G.L, h); // writes the node records
+    RBC_DISPATCH_L(launch_node_records, R, h->G.L, h); // no step starts from this synthesis
     snapshot_step(h);
     launch_tracer_from_synthesis<R>(h);
     h->tracer_pending = false;
@@ -890,8 +898,9 @@ static void field_ops_setup(rbc_handle* h)
     int dev = 0, optin = 0;
     RBC_CUDA(cudaGetDevice(&dev));
     RBC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    // row pairs per CTA: the most that leave room for two CTAs per SM
     int nb = h->px.chunk;
-    while (nb > 1 && smem_mask_rows(h, nb) > (size_t)optin) nb /= 2;
+    while (nb > 1 && smem_mask_rows(h, nb) > (size_t)optin / 2) nb /= 2;
     if (smem_mask_rows(h, nb) > (size_t)optin || smem_mask_cols(h) > (size_t)optin)
         throw ArgError{"grid too large for the field operators' shared memory"};
     h->mask_nb = nb;

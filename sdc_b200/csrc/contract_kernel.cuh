@@ -65,6 +65,31 @@ RBC_D void contract_mode(const R (&in)[rbcprog::NFIELD][L], const R* __restrict_
 // u11, u21, u31, u12, u22 of a grid point, padded to an even count (16-byte records).
 template <int L> struct NodeRec { static constexpr int value = (5 * L + 1) & ~1; };
 
+// The node records alone (no contraction): the tracer advance that runs on a state no
+// step will start from (a state about to be changed between steps) needs only these.
+template <typename R, int L>
+__global__ void __launch_bounds__(256) k_node_records(const R* __restrict__ phys, int P, R* __restrict__ nv)
+{
+    constexpr int NR = NodeRec<L>::value;
+    typedef typename cplx_t<R>::type R2;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < P; x += gridDim.x * blockDim.x) {
+        R rec[NR];
+#pragma unroll
+        for (int f = 0; f < 5; ++f)
+#pragma unroll
+            for (int i = 0; i < L; ++i) rec[f * L + i] = phys[((size_t)f * L + i) * P + x];
+        if (NR > 5 * L) rec[NR - 1] = 0;
+        R2* dst = reinterpret_cast<R2*>(nv + (size_t)x * NR);
+#pragma unroll
+        for (int q = 0; q < NR / 2; ++q) {
+            R2 v;
+            v.x = rec[2 * q];
+            v.y = rec[2 * q + 1];
+            dst[q] = v;
+        }
+    }
+}
+
 // Grid-stride over points; coef (global) is the packed array of pack_contraction,
 // copied once per CTA into shared memory. When nv is not null the kernel also writes
 // every point's node record nv[x * NodeRec] (the tracers gather those records).
