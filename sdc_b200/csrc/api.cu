@@ -631,19 +631,32 @@ template <typename R> static void run_step(rbc_handle* h)
     ++h->host_steps;
 }
 
-template <typename R> static void flush_tracers_t(rbc_handle* h)
+// overlap: the advance goes to the side stream and the caller calls join_tracer(h) once
+// the work it overlaps (which must leave the tracer data and node records alone) is enqueued.
+template <typename R> static void flush_tracers_t(rbc_handle* h, bool overlap)
 {
     if (!h->tracer_pending) return;
     run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
     RBC_DISPATCH_L(launch_node_records, R, h->G.L, h); // no step starts from this synthesis
     snapshot_step(h);
-    launch_tracer_from_synthesis<R>(h);
+    if (overlap && h->side && !h->profiling) {
+        RBC_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+        RBC_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+        cudaStream_t main_stream = h->stream;
+        h->stream = h->side;
+        launch_tracer_from_synthesis<R>(h);
+        h->stream = main_stream;
+        RBC_CUDA(cudaEventRecord(h->ev_join, h->side));
+        h->join_pending = true;
+    } else {
+        launch_tracer_from_synthesis<R>(h);
+    }
     h->tracer_pending = false;
 }
-static void flush_tracers(rbc_handle* h)
+static void flush_tracers(rbc_handle* h, bool overlap = false)
 {
-    if (h->mixed) flush_tracers_t<float>(h);
-    else flush_tracers_t<double>(h);
+    if (h->mixed) flush_tracers_t<float>(h, overlap);
+    else flush_tracers_t<double>(h, overlap);
 }
 
 // The dynamic shared-memory limit is an attribute of the kernel, shared by every handle
@@ -807,7 +820,7 @@ template <typename R, int L> static void launch_penalize(rbc_handle* h)
 
 template <typename R, int L> static void launch_penalize_fg(rbc_handle* h)
 {
-    k_penalize_fg<L><<<1, 64, 0, h->stream>>>(h->pen_partial, h->pen_blocks, h->pen_ia2,
+    k_penalize_fg<L><<<1, kPenFgThreads, 0, h->stream>>>(h->pen_partial, h->pen_blocks, h->pen_ia2,
                                               1.0 / (h->prm.penalization_eta * h->G.P), h->NFG);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
@@ -873,9 +886,9 @@ static void twiddles(int n, std::vector<double2>& tw)
 }
 
 // ------------------------------------------------------------------ field operators
-static size_t smem_mask_cols(const rbc_handle* h)
+static size_t smem_mask_cols(const rbc_handle* h, int W)
 {
-    return (size_t)(h->G.ny + h->py.chunk * h->py.stride) * sizeof(double2);
+    return (size_t)(h->G.ny + W * h->py.stride) * sizeof(double2);
 }
 static size_t smem_mask_rows(const rbc_handle* h, int nb)
 {
@@ -901,7 +914,7 @@ static void field_ops_setup(rbc_handle* h)
     // row pairs per CTA: the most that leave room for two CTAs per SM
     int nb = h->px.chunk;
     while (nb > 1 && smem_mask_rows(h, nb) > (size_t)optin / 2) nb /= 2;
-    if (smem_mask_rows(h, nb) > (size_t)optin || smem_mask_cols(h) > (size_t)optin)
+    if (smem_mask_rows(h, nb) > (size_t)optin || smem_mask_cols(h, h->py.chunk) > (size_t)optin)
         throw ArgError{"grid too large for the field operators' shared memory"};
     h->mask_nb = nb;
     RBC_CUDA(cudaFuncSetAttribute(k_mask_cols<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
@@ -917,9 +930,14 @@ static void mask_pass(rbc_handle* h, int nfields, int op, const unsigned char* m
     MaskFields fl{{h->th, h->f, h->g}};
     const int planes = nfields * G.L;
     double2* S = static_cast<double2*>(h->H);
-    const int W = h->py.chunk;
+    // column CTAs: about four per SM over all planes, each with a thread per butterfly
+    int rmin = 1 << 30;
+    for (int i = 0; i < h->py.npass; ++i) rmin = std::min(rmin, h->py.radix[i]);
+    const int W = std::max(1, std::min(h->py.chunk, (G.ckeep * planes + 4 * 148 - 1) / (4 * 148)));
+    const int tc = std::min(kThreads, std::max(32, (W * G.ny / rmin + 31) / 32 * 32));
     const dim3 gc((G.ckeep + W - 1) / W, planes);
-    k_mask_cols<1><<<gc, kThreads, smem_mask_cols(h), h->stream>>>(G, W, h->py, h->twy, fl, S);
+    const size_t smc = smem_mask_cols(h, W);
+    k_mask_cols<1><<<gc, tc, smc, h->stream>>>(G, W, h->py, h->twy, fl, S);
     RBC_CUDA(cudaGetLastError());
     const int nb = h->mask_nb;
     k_mask_rows<<<dim3((G.ny + 2 * nb - 1) / (2 * nb), planes), kThreads, smem_mask_rows(h, nb), h->stream>>>(
@@ -927,7 +945,7 @@ static void mask_pass(rbc_handle* h, int nfields, int op, const unsigned char* m
     RBC_CUDA(cudaGetLastError());
     h->launches += 2;
     if (op == MASK_SNAPSHOT) return;
-    k_mask_cols<-1><<<gc, kThreads, smem_mask_cols(h), h->stream>>>(G, W, h->py, h->twy, fl, S);
+    k_mask_cols<-1><<<gc, tc, smc, h->stream>>>(G, W, h->py, h->twy, fl, S);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -2234,8 +2252,11 @@ rbc_status rbc_freeze_apply(rbc_handle* h)
     if (!h) return RBC_ERR_INVALID_ARG;
     if (!h->frozen_set) return RBC_OK; // freeze_operator::calculate_operator before a freeze
     RBC_GUARD(h)
-    flush_tracers(h); // a pending tracer advance uses the velocity of the state before the change
+    // a pending tracer advance uses the velocity of the state before the change; it runs
+    // beside the operator, which leaves the tracer data alone
+    flush_tracers(h, true);
     mask_pass(h, 3, MASK_FREEZE, h->fmask, 0.0);
+    join_tracer(h);
     return RBC_OK;
     RBC_GUARD_END(h)
 }
@@ -2259,8 +2280,9 @@ rbc_status rbc_heat_apply(rbc_handle* h)
     if (!h) return RBC_ERR_INVALID_ARG;
     if (!h->heat_set) return RBC_OK; // masktemp::calculate_operator before the mask is set
     RBC_GUARD(h)
-    flush_tracers(h);
+    flush_tracers(h, true);
     mask_pass(h, 1, MASK_HEAT, h->hmask, h->heat_inc);
+    join_tracer(h);
     return RBC_OK;
     RBC_GUARD_END(h)
 }
@@ -2272,9 +2294,10 @@ rbc_status rbc_masker(rbc_handle* h, double x, double y, double radius, double f
     if (!std::isfinite(x) || !std::isfinite(y) || !std::isfinite(radius) || !std::isfinite(factor))
         return fail(h, RBC_ERR_INVALID_ARG, "bad mask position, radius or factor");
     RBC_GUARD(h)
-    flush_tracers(h); // a pending tracer advance uses the velocity of the state before the change
+    flush_tracers(h, true); // beside the operator, as in rbc_freeze_apply
     make_mask(h, h->smask, RBC_MASK_CIRCLE, y, x, radius); // column centre y Nx, row centre x Ny
     mask_pass(h, 1, MASK_SCALE, h->smask, factor);
+    join_tracer(h);
     return RBC_OK;
     RBC_GUARD_END(h)
 }

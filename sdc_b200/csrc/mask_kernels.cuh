@@ -62,8 +62,9 @@ __global__ void k_field_mask(unsigned char* __restrict__ mask, int nx, int ny, i
     mask[i] = m;
 }
 
-// KM1 / KM3. Grid (ceil(ckeep / W), planes), kThreads threads; W <= py.chunk columns of
-// one plane per CTA. Shared: twiddles [Ny] + W padded transforms.
+// KM1 / KM3. Grid (ceil(ckeep / W), planes); W <= py.chunk columns of one plane per CTA
+// and at least W Ny / (smallest radix) threads (every butterfly of a pass has a thread).
+// Shared: twiddles [Ny] + W padded transforms.
 template <int SIGN>
 __global__ void __launch_bounds__(kThreads) k_mask_cols(Geom G, int W, rbcfft::Plan py, const double2* __restrict__ twy,
                                                         MaskFields fl, double2* __restrict__ S)
@@ -79,8 +80,9 @@ __global__ void __launch_bounds__(kThreads) k_mask_cols(Geom G, int W, rbcfft::P
     const double2* src = SIGN > 0 ? state : scr;
     for (int e = threadIdx.x; e < nc * ny; e += blockDim.x) {
         const int j = e / ny, r = e - j * ny;
-        buf[j * py.stride + rbcfft::pad(r)] = src[(size_t)(c0 + j) * ny + r];
+        cp_async<sizeof(double2)>(buf + j * py.stride + rbcfft::pad(r), src + (size_t)(c0 + j) * ny + r);
     }
+    cp_async_wait_all();
     __syncthreads();
     fft_batched<double>(buf, py, nc, tw, SIGN);
     double2* dst = SIGN > 0 ? scr : state;
@@ -115,8 +117,9 @@ __global__ void __launch_bounds__(kThreads) k_mask_rows(Geom G, int NB, rbcfft::
     double2* scr = S + (size_t)pl * G.ckp * ny;
     for (int e = threadIdx.x; e < ck * nrow; e += blockDim.x) {
         const int c = e / nrow, y = e - c * nrow;
-        stg[c * 2 * NB + y] = scr[(size_t)c * ny + y0 + y];
+        cp_async<sizeof(double2)>(stg + c * 2 * NB + y, scr + (size_t)c * ny + y0 + y);
     }
+    cp_async_wait_all();
     __syncthreads();
     // Hermitian extension of rows a and b, packed: Z[j] = A[j] + i B[j] and
     // Z[Nx - j] = conj(A[j]) + i conj(B[j]); the imaginary parts of A and B at j = 0
@@ -139,27 +142,53 @@ __global__ void __launch_bounds__(kThreads) k_mask_rows(Geom G, int NB, rbcfft::
     __syncthreads();
     fft_batched<double>(buf, px, nt, tw, +1);
     const double invP = 1.0 / ((double)nx * ny);
-    for (int e = threadIdx.x; e < nt * nx; e += blockDim.x) {
-        const int t = e / nx, x = e - t * nx;
-        const int ya = y0 + 2 * t;
-        double2& z = buf[t * px.stride + rbcfft::pad(x)];
-        const size_t ia = (size_t)ya * nx + x, ib = ia + nx;
-        double* fr = frozen ? frozen + (size_t)pl * G.P : nullptr;
-        if (op == MASK_SNAPSHOT) {
-            fr[ia] = z.x;
-            fr[ib] = z.y;
-            continue;
+    double* fr = frozen ? frozen + (size_t)pl * G.P : nullptr;
+    // four elements per thread and round: their mask and frozen values are loaded before
+    // any of them is used
+    const int tot = nt * nx;
+    for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
+        unsigned char ma[4], mb[4];
+        double fa[4], fb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = e0 + u * blockDim.x;
+            ma[u] = mb[u] = 1;
+            fa[u] = fb[u] = 0.0;
+            if (e < tot && op != MASK_SNAPSHOT) {
+                const int t = e / nx, x = e - t * nx;
+                const size_t ia = (size_t)(y0 + 2 * t) * nx + x;
+                ma[u] = mask[ia];
+                mb[u] = mask[ia + nx];
+                if (op == MASK_FREEZE) {
+                    fa[u] = fr[ia];
+                    fb[u] = fr[ia + nx];
+                }
+            }
         }
-        double va = z.x, vb = z.y;
-        if (op == MASK_SCALE) { // masking.cu:49-56: (1/P) v factor inside the circle
-            va = mask[ia] ? invP * va : invP * va * increment;
-            vb = mask[ib] ? invP * vb : invP * vb * increment;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e >= tot) continue;
+            const int t = e / nx, x = e - t * nx;
+            const size_t ia = (size_t)(y0 + 2 * t) * nx + x;
+            double2& z = buf[t * px.stride + rbcfft::pad(x)];
+            if (op == MASK_SNAPSHOT) {
+                fr[ia] = z.x;
+                fr[ia + nx] = z.y;
+                continue;
+            }
+            double va = z.x, vb = z.y;
+            if (op == MASK_SCALE) { // masking.cu:49-56: (1/P) v factor inside the circle
+                va = ma[u] ? invP * va : invP * va * increment;
+                vb = mb[u] ? invP * vb : invP * vb * increment;
+            } else {
+                if (!ma[u]) va = op == MASK_FREEZE ? fa[u] : va + increment;
+                if (!mb[u]) vb = op == MASK_FREEZE ? fb[u] : vb + increment;
+                va *= invP;
+                vb *= invP;
+            }
             z = make_double2(va, vb);
-            continue;
         }
-        if (!mask[ia]) va = op == MASK_FREEZE ? fr[ia] : va + increment;
-        if (!mask[ib]) vb = op == MASK_FREEZE ? fr[ib] : vb + increment;
-        z = make_double2(invP * va, invP * vb);
     }
     if (op == MASK_SNAPSHOT) return; // uniform over the CTA
     __syncthreads();

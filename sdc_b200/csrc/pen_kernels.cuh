@@ -46,26 +46,40 @@ __global__ void __launch_bounds__(kPenThreads) k_penalize(const R* __restrict__ 
 #pragma unroll
         for (int j = 0; j < L; ++j) v[f][j] = m != 0.0 ? (double)phys[((size_t)fidx[f] * L + j) * sP + p] : 0.0;
     if (m != 0.0) {
+        // modes in pairs: every load of a pair is issued before its stores
+        constexpr int KB = L < 2 ? L : 2;
 #pragma unroll
-        for (int k = 0; k < L; ++k) {
-            double a3 = 0.0, a4 = 0.0;
+        for (int k0 = 0; k0 < L; k0 += KB) {
+            double u31[KB], th[KB], g[4][KB];
+            const int gid[4] = {3, 4, 7, 12};
 #pragma unroll
-            for (int f = 0; f < 4; ++f)
+            for (int kk = 0; kk < KB; ++kk) {
+                const int k = k0 + kk;
+                if (k < L) {
+                    u31[kk] = (double)phys[((size_t)2 * L + k) * sP + p];
+                    th[kk] = (double)phys[((size_t)5 * L + k) * sP + p];
 #pragma unroll
-                for (int j = 0; j < L; ++j) {
-                    a3 += scf[(0 * L + k) * 4 * L + f * L + j] * v[f][j];
-                    a4 += scf[(1 * L + k) * 4 * L + f * L + j] * v[f][j];
+                    for (int q = 0; q < 4; ++q) g[q][kk] = (double)grp[((size_t)gid[q] * L + k) * sP + p];
                 }
-            const double u31 = (double)phys[((size_t)2 * L + k) * sP + p];
-            const double th = (double)phys[((size_t)5 * L + k) * sP + p];
-            R* g3 = grp + ((size_t)3 * L + k) * sP + p;
-            R* g4 = grp + ((size_t)4 * L + k) * sP + p;
-            R* g7 = grp + ((size_t)7 * L + k) * sP + p;
-            R* g12 = grp + ((size_t)12 * L + k) * sP + p;
-            *g3 = (R)((double)*g3 + m * a3);
-            *g4 = (R)((double)*g4 + m * a4);
-            *g7 = (R)((double)*g7 - m * pe * u31);
-            *g12 = (R)((double)*g12 + m * theta_fac * th);
+            }
+#pragma unroll
+            for (int kk = 0; kk < KB; ++kk) {
+                const int k = k0 + kk;
+                if (k < L) {
+                    double a3 = 0.0, a4 = 0.0;
+#pragma unroll
+                    for (int f = 0; f < 4; ++f)
+#pragma unroll
+                        for (int j = 0; j < L; ++j) {
+                            a3 += scf[(0 * L + k) * 4 * L + f * L + j] * v[f][j];
+                            a4 += scf[(1 * L + k) * 4 * L + f * L + j] * v[f][j];
+                        }
+                    grp[((size_t)3 * L + k) * sP + p] = (R)(g[0][kk] + m * a3);
+                    grp[((size_t)4 * L + k) * sP + p] = (R)(g[1][kk] + m * a4);
+                    grp[((size_t)7 * L + k) * sP + p] = (R)(g[2][kk] - m * pe * u31[kk]);
+                    grp[((size_t)12 * L + k) * sP + p] = (R)(g[3][kk] + m * theta_fac * th[kk]);
+                }
+            }
         }
     }
     // fixed-order block sums of mask * u for the means of F and G
@@ -88,16 +102,24 @@ __global__ void __launch_bounds__(kPenThreads) k_penalize(const R* __restrict__ 
 }
 
 // After the column pass has written NFG (F of mode k at k, G at L + k): adds the
-// penalized means. One CTA; ia2[j + k L] = Ia2(j, k); inv = 1 / (eta P).
+// penalized means. One CTA of kPenFgThreads; warp w sums the partials of values
+// w, w + 32, ... (lane l takes blocks l, l + 32, ..., then a fixed shuffle tree);
+// ia2[j + k L] = Ia2(j, k); inv = 1 / (eta P).
+constexpr int kPenFgThreads = 1024;
 template <int L>
-__global__ void k_penalize_fg(const double* __restrict__ partial, int nblocks, const double* __restrict__ ia2,
-                              double inv, double* __restrict__ NFG)
+__global__ void __launch_bounds__(kPenFgThreads) k_penalize_fg(const double* __restrict__ partial, int nblocks,
+                                                               const double* __restrict__ ia2, double inv,
+                                                               double* __restrict__ NFG)
 {
     __shared__ double S[4 * L];
-    for (int t = threadIdx.x; t < 4 * L; t += blockDim.x) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int t = warp; t < 4 * L; t += nwarp) {
         double s = 0.0;
-        for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * 4 * L + t];
-        S[t] = s;
+#pragma unroll 8
+        for (int b = lane; b < nblocks; b += 32) s += partial[(size_t)b * 4 * L + t];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) S[t] = s;
     }
     __syncthreads();
     if (threadIdx.x < L) {
