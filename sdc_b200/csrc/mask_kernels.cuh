@@ -66,7 +66,7 @@ __global__ void k_field_mask(unsigned char* __restrict__ mask, int nx, int ny, i
 // and at least W Ny / (smallest radix) threads (every butterfly of a pass has a thread).
 // Shared: twiddles [Ny] + W padded transforms.
 template <int SIGN>
-__global__ void __launch_bounds__(kThreads) k_mask_cols(Geom G, int W, rbcfft::Plan py, const double2* __restrict__ twy,
+__global__ void __launch_bounds__(kThreads, 2) k_mask_cols(Geom G, int W, rbcfft::Plan py, const double2* __restrict__ twy,
                                                         MaskFields fl, double2* __restrict__ S)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) k_mask_cols(Geom G, int W, rbcfft::P
 // op: MASK_SNAPSHOT writes the C2R of the planes to `frozen` and leaves S alone;
 // MASK_FREEZE / MASK_HEAT / MASK_SCALE apply the operation (increment is the factor of
 // MASK_SCALE) and write the R2C back into S.
-__global__ void __launch_bounds__(kThreads) k_mask_rows(Geom G, int NB, rbcfft::Plan px, const double2* __restrict__ twx,
+__global__ void __launch_bounds__(kThreads, 2) k_mask_rows(Geom G, int NB, rbcfft::Plan px, const double2* __restrict__ twx,
                                                         double2* __restrict__ S, int op,
                                                         const unsigned char* __restrict__ mask,
                                                         double* __restrict__ frozen, double increment)
