@@ -259,6 +259,17 @@ rbc_status rbc_diagnostics(rbc_handle* h, rbc_diag* out);
 /* The last min(n, steps, capacity) per-step entries, oldest first; *count receives the
  * number written. */
 rbc_status rbc_diag_history(rbc_handle* h, rbc_diag* out, int n, int* count);
+/* Pipelined reads of the per-step diagnostics (no reference counterpart): ..._async
+ * enqueues, on the handle's stream, a copy of the newest entry and the error word into one
+ * of RBC_DIAG_SLOTS pinned host slots and returns its ticket without waiting; ..._get waits
+ * for that copy only (not for work enqueued after it) and returns the entry, or
+ * RBC_ERR_NAN as rbc_diagnostics does. A loop of rbc_step_async(h, 1), rbc_diagnostics_async
+ * and rbc_diagnostics_get of the previous ticket keeps the next step queued while the host
+ * reads the last one. Tickets older than the last RBC_DIAG_SLOTS are rejected. Before the
+ * first step the entry has step 0 and NaN values. */
+#define RBC_DIAG_SLOTS 8
+rbc_status rbc_diagnostics_async(rbc_handle* h, long long* ticket);
+rbc_status rbc_diagnostics_get(rbc_handle* h, long long ticket, rbc_diag* out);
 /* Radial shell spectrum of theta(x, y, z): sum of |theta_hat|^2 over the half spectrum
  * in nbins shells of width |q_max| / nbins, as energy_spectrum_2d::reduce_spectrum
  * (gpu_flow/code/postProcessing/energy_spectrum_2d.cu:85-129). */

@@ -78,7 +78,8 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_fno_loss_grad", "rbc_fno_colloc_get", "rbc_fno_colloc_add", "rbc_fno_dataset_reserve",
            "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run",
            "rbc_fno_set_train_options", "rbc_structure_function", "rbc_freeze_mask", "rbc_freeze_apply",
-           "rbc_heat_mask", "rbc_heat_apply", "rbc_field_ops_reset", "rbc_masker"]
+           "rbc_heat_mask", "rbc_heat_apply", "rbc_field_ops_reset", "rbc_masker",
+           "rbc_diagnostics_async", "rbc_diagnostics_get"]
 FIELD_OPS = {"freeze": 1, "heat": 2, "scale": 4}
 MASK_SHAPES = {"circle": 0, "rectangle": 1}
 PEN_MASKS = {"rectangle": 0, "circle": 1, "disk_array": 2, "everywhere": 3}
@@ -159,6 +160,8 @@ def lib():
     L.rbc_heat_apply.argtypes = [vp]
     L.rbc_field_ops_reset.argtypes = [vp]
     L.rbc_masker.argtypes = [vp] + [ctypes.c_double] * 4
+    L.rbc_diagnostics_async.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.rbc_diagnostics_get.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(_Diag)]
     L.rbc_fno_create.argtypes = [ctypes.POINTER(_FnoParams), ctypes.POINTER(vp)]
     L.rbc_fno_destroy.argtypes = [vp]
     L.rbc_fno_destroy.restype = None
@@ -457,6 +460,18 @@ class Solver:
     def diagnostics(self):
         d = _Diag()
         self._check(lib().rbc_diagnostics(self.h, ctypes.byref(d)))
+        return {"nu_wall": d.nu_wall, "nu_vol": d.nu_vol, "ke": d.ke, "step": d.step}
+
+    def diagnostics_async(self):
+        """Enqueues a read of the newest diagnostics entry; returns its ticket."""
+        t = ctypes.c_longlong(0)
+        self._check(lib().rbc_diagnostics_async(self.h, ctypes.byref(t)))
+        return t.value
+
+    def diagnostics_get(self, ticket):
+        """Waits for the read of `ticket` only and returns its entry."""
+        d = _Diag()
+        self._check(lib().rbc_diagnostics_get(self.h, ticket, ctypes.byref(d)))
         return {"nu_wall": d.nu_wall, "nu_vol": d.nu_vol, "ke": d.ke, "step": d.step}
 
     def diag_history(self, n):

@@ -120,6 +120,11 @@ struct rbc_handle {
     bool frozen_set = false, heat_set = false;
     double heat_inc = 0.0;
     int mask_nb = 1;                                 // row pairs per k_mask_rows CTA
+    // pipelined diagnostics: pinned slots of [4] doubles + the error word, one event each
+    struct DiagSlot { double v[4]; int err; int pad; };
+    DiagSlot* dslot = nullptr;
+    cudaEvent_t dev_ev[RBC_DIAG_SLOTS] = {};
+    long long dticket = 0;                           // tickets issued
     // penalized operator (rbc_params.penalization_eta > 0)
     bool penalized = false;
     double *pen_mask = nullptr, *pen_cf = nullptr, *pen_ia2 = nullptr, *pen_partial = nullptr;
@@ -861,6 +866,10 @@ static void free_all(rbc_handle* h)
     if (h->ev_join) cudaEventDestroy(h->ev_join);
     h->side = nullptr;
     h->ev_fork = h->ev_join = nullptr;
+    for (auto& e : h->dev_ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    if (h->dslot) cudaFreeHost(h->dslot);
+    h->dslot = nullptr;
 }
 
 void rbc_destroy(rbc_handle* h)
@@ -1100,6 +1109,8 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
             RBC_DISPATCH_L(setup_contract, double, G.L, h);
         }
         tracer_setup(h);
+        RBC_CUDA(cudaHostAlloc((void**)&h->dslot, RBC_DIAG_SLOTS * sizeof(rbc_handle::DiagSlot), cudaHostAllocDefault));
+        for (auto& e : h->dev_ev) RBC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         field_ops_setup(h);
         penalization_setup(h);
         RBC_CUDA(cudaDeviceSynchronize());
@@ -1567,6 +1578,50 @@ rbc_status rbc_diagnostics(rbc_handle* h, rbc_diag* out)
     out->nu_vol = NAN;
     out->ke = NAN;
     out->step = 0;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_diagnostics_async(rbc_handle* h, long long* ticket)
+{
+    if (!ticket) return fail(h, RBC_ERR_INVALID_ARG, "null ticket");
+    RBC_GUARD(h)
+    const long long t = h->dticket;
+    const int sl = (int)(t % RBC_DIAG_SLOTS);
+    rbc_handle::DiagSlot* d = h->dslot + sl;
+    // the slot's previous copy must be done before it is overwritten
+    RBC_CUDA(cudaEventSynchronize(h->dev_ev[sl]));
+    RBC_CUDA(cudaMemcpyAsync(d->v, h->ring + 4 * (size_t)h->ring_cap, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                             h->stream));
+    RBC_CUDA(cudaMemcpyAsync(&d->err, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaEventRecord(h->dev_ev[sl], h->stream));
+    h->dticket = t + 1;
+    *ticket = t;
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_diagnostics_get(rbc_handle* h, long long ticket, rbc_diag* out)
+{
+    if (!out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (ticket < 0 || ticket >= h->dticket || ticket < h->dticket - RBC_DIAG_SLOTS)
+        return fail(h, RBC_ERR_INVALID_ARG, "ticket not among the last RBC_DIAG_SLOTS issued");
+    RBC_GUARD(h)
+    const int sl = (int)(ticket % RBC_DIAG_SLOTS);
+    RBC_CUDA(cudaEventSynchronize(h->dev_ev[sl]));
+    const rbc_handle::DiagSlot& d = h->dslot[sl];
+    if (d.err & RBC_DEVERR_NAN) return fail(h, RBC_ERR_NAN, "non-finite value in the state");
+    if (d.err) return fail(h, RBC_ERR_CUDA, "device error word set");
+    if (d.v[3] > 0) {
+        out->nu_wall = d.v[0];
+        out->nu_vol = d.v[1];
+        out->ke = d.v[2];
+        out->step = (long long)d.v[3];
+    } else {
+        out->nu_wall = out->nu_vol = out->ke = NAN;
+        out->step = 0;
+    }
     return RBC_OK;
     RBC_GUARD_END(h)
 }

@@ -181,6 +181,45 @@ def test_diag_history_ring_wraps():
     assert s.diag_history(3).shape == (3, 4)
 
 
+def test_pipelined_diagnostics_match_history():
+    """rbc_diagnostics_async / _get: each ticket returns the entry of the step it was
+    enqueued after, read while later steps are queued; stale tickets are rejected."""
+    case = SMALL_CASES[2]
+    s = sdc_b200.Solver(*case)
+    nx, ny, L = case[:3]
+    s.set_state(*random_state(nx, ny, L, seed=24, amp=0.05))
+    t_init = s.diagnostics_async()
+    d = s.diagnostics_get(t_init)
+    assert d["step"] == 0 and np.isnan(d["nu_wall"])
+    got = []
+    prev = None
+    for _ in range(20):
+        s.step_async(1)
+        t = s.diagnostics_async()
+        if prev is not None:
+            got.append(s.diagnostics_get(prev))
+        prev = t
+    got.append(s.diagnostics_get(prev))
+    hist = s.diag_history(20)
+    assert [g["step"] for g in got] == list(range(1, 21))
+    for g, h in zip(got, hist):
+        assert (g["nu_wall"], g["nu_vol"], g["ke"]) == (h[0], h[1], h[2])
+    with pytest.raises(sdc_b200.RBCError):
+        s.diagnostics_get(prev - 8)
+    with pytest.raises(sdc_b200.RBCError):
+        s.diagnostics_get(prev + 1)
+    # a non-finite state is reported through the pipelined read too
+    st = random_state(nx, ny, L, seed=1, amp=0.01)
+    st[0][0, 3, 2] = np.nan
+    s2 = sdc_b200.Solver(*case)
+    s2.set_state(*st)
+    s2.step_async(2)
+    t = s2.diagnostics_async()
+    with pytest.raises(sdc_b200.RBCError) as e:
+        s2.diagnostics_get(t)
+    assert e.value.status == 3
+
+
 @pytest.mark.parametrize("z", [0.0, 0.23])
 def test_spectrum_matches_oracle(z):
     case = SMALL_CASES[4]
