@@ -17,6 +17,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -298,6 +299,31 @@ __global__ void k_structure_function(const double2* __restrict__ th, const doubl
 }
 
 // ------------------------------------------------------------------ dispatch
+// Launch of a step kernel that follows another kernel of the step on the same stream: with
+// programmatic stream serialization, so that its CTAs start and load their constant tables
+// while the predecessor drains (the kernel fences with pdl_wait before it touches step data).
+// A kernel launched this way reads step data written by its immediate predecessor only:
+// pdl_wait makes the predecessor's writes visible, and the chain of waits orders the
+// kernels, but a kernel that also read data written two launches back (the penalization
+// kernels, reading the synthesis) saw stale values when both links were programmatic.
+// Those kernels are launched plainly, which also covers the kernel after them. Plain
+// launches too while stage timing brackets every kernel with events.
+template <typename... KArgs, typename... Args>
+static void launch_dep(rbc_handle* h, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = h->profiling ? 0 : 1;
+    RBC_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
 template <typename R, int L> static void setup_contract(rbc_handle* h)
 {
     const int smem = (int)(rbcprog::NUNIT * L * L * rbcprog::half_len(L) * sizeof(R));
@@ -316,8 +342,8 @@ template <typename R, int L> static void launch_contract(rbc_handle* h)
 {
     StageScope sc(h, ST_CONTRACT);
     R* nv = h->tracer_pending ? (R*)h->nv : nullptr; // node records for the tracer advance
-    k_contract<R, L><<<h->contract_grid, 128, h->contract_smem, h->stream>>>((const R*)h->phys, (R*)h->grp,
-                                                                             (const R*)h->coef, h->G.P, nv);
+    launch_dep(h, k_contract<R, L>, dim3(h->contract_grid), dim3(128), (size_t)h->contract_smem, (const R*)h->phys,
+               (R*)h->grp, (const R*)h->coef, h->G.P, nv);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -355,7 +381,7 @@ template <typename R, int L> static void launch_update(rbc_handle* h)
     A.step_counter = h->step_counter;
     A.err = h->err;
     StageScope sc(h, ST_UPDATE);
-    k_update<R, L><<<h->upd_blocks, kThreads, 0, h->stream>>>(A);
+    launch_dep(h, k_update<R, L>, dim3(h->upd_blocks), dim3(kThreads), 0, A);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -425,9 +451,9 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     const int nb = rows / (2 * h->NP);
     const size_t sm = smem_rows<R>(h);
     switch (rx_x(h)) {
-    case 16: k_rows_c2r_tp<R, 16><<<nb, h->NP * 16, sm, h->stream>>>(G, h->NP, h->twx, (const C*)h->H, (R*)h->phys); break;
-    case 8: k_rows_c2r_tp<R, 8><<<nb, h->NP * 8, sm, h->stream>>>(G, h->NP, h->twx, (const C*)h->H, (R*)h->phys); break;
-    default: k_rows_c2r<R><<<nb, kThreads, sm, h->stream>>>(G, h->NP, h->px, h->twx, (const C*)h->H, (R*)h->phys);
+    case 16: launch_dep(h, k_rows_c2r_tp<R, 16>, dim3(nb), dim3(h->NP * 16), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
+    case 8: launch_dep(h, k_rows_c2r_tp<R, 8>, dim3(nb), dim3(h->NP * 8), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
+    default: launch_dep(h, k_rows_c2r<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const C*)h->H, (R*)h->phys);
     }
     RBC_CUDA(cudaGetLastError());
     h->launches += 2;
@@ -482,9 +508,9 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     const int nb = rows / (2 * h->NP);
     const size_t sm = smem_rows<R>(h);
     switch (rx_x(h)) {
-    case 16: k_rows_r2c_tp<R, 16><<<nb, h->NP * 16, sm, h->stream>>>(G, h->NP, h->twx, (const R*)h->grp, (C*)h->gh); break;
-    case 8: k_rows_r2c_tp<R, 8><<<nb, h->NP * 8, sm, h->stream>>>(G, h->NP, h->twx, (const R*)h->grp, (C*)h->gh); break;
-    default: k_rows_r2c<R><<<nb, kThreads, sm, h->stream>>>(G, h->NP, h->px, h->twx, (const R*)h->grp, (C*)h->gh);
+    case 16: launch_dep(h, k_rows_r2c_tp<R, 16>, dim3(nb), dim3(h->NP * 16), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 8: launch_dep(h, k_rows_r2c_tp<R, 8>, dim3(nb), dim3(h->NP * 8), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    default: launch_dep(h, k_rows_r2c<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh);
     }
     RBC_CUDA(cudaGetLastError());
     }
@@ -493,9 +519,9 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     StageScope sc(h, ST_COMBINE);
     const size_t sm = smem_combine<R>(h);
     switch (rx_y(h)) {
-    case 16: k_columns_combine_tp<R, 16><<<g5, 13 * 16, sm, h->stream>>>(G, h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
-    case 8: k_columns_combine_tp<R, 8><<<g5, 13 * 8, sm, h->stream>>>(G, h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
-    default: k_columns_combine<R><<<g5, kThreads, sm, h->stream>>>(G, h->py, h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
+    case 16: launch_dep(h, k_columns_combine_tp<R, 16>, g5, dim3(13 * 16), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    case 8: launch_dep(h, k_columns_combine_tp<R, 8>, g5, dim3(13 * 8), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    default: launch_dep(h, k_columns_combine<R>, g5, dim3(kThreads), sm, G, h->py, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
     }
     RBC_CUDA(cudaGetLastError());
     }
@@ -816,6 +842,7 @@ static void penalization_setup(rbc_handle* h)
 template <typename R, int L> static void launch_penalize(rbc_handle* h)
 {
     const rbc_params& p = h->prm;
+    // a plain launch: this kernel reads the synthesis, written two launches back
     k_penalize<R, L><<<h->pen_blocks, kPenThreads, 0, h->stream>>>((const R*)h->phys, (R*)h->grp, h->pen_mask,
                                                                     h->pen_cf, h->G.P, p.pr / p.penalization_eta,
                                                                     0.5 / p.penalization_eta, h->pen_partial);
@@ -825,8 +852,9 @@ template <typename R, int L> static void launch_penalize(rbc_handle* h)
 
 template <typename R, int L> static void launch_penalize_fg(rbc_handle* h)
 {
+    // a plain launch: this kernel reads k_penalize's partial sums, three launches back
     k_penalize_fg<L><<<1, kPenFgThreads, 0, h->stream>>>(h->pen_partial, h->pen_blocks, h->pen_ia2,
-                                              1.0 / (h->prm.penalization_eta * h->G.P), h->NFG);
+                                                         1.0 / (h->prm.penalization_eta * h->G.P), h->NFG);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }

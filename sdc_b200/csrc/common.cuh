@@ -40,3 +40,12 @@ template <int BYTES> RBC_D void cp_async(void* smem_dst, const void* gmem_src)
         asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem_src), "n"(BYTES) : "memory");
 }
 RBC_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Programmatic dependent launch (sm_90+). A kernel launched with the programmatic
+// stream-serialization attribute may start once every CTA of its predecessor in the stream
+// has called pdl_trigger (or exited), i.e. while the predecessor drains. Before pdl_wait
+// such a kernel may read only data no kernel of the step writes (twiddles, coefficient
+// tables, class indices) and write nothing; pdl_wait returns when the predecessor has
+// completed and its writes are visible. Both are no-ops for an ordinary launch.
+RBC_D void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+RBC_D void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }

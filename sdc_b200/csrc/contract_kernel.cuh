@@ -100,7 +100,9 @@ __global__ void __launch_bounds__(128) k_contract(const R* __restrict__ phys, R*
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* coef = reinterpret_cast<R*>(smem_raw);
     constexpr int NC = rbcprog::NUNIT * L * L * rbcprog::half_len(L);
+    pdl_trigger();
     for (int e = threadIdx.x; e < NC; e += blockDim.x) coef[e] = coef_g[e];
+    pdl_wait(); // the synthesis is complete
     __syncthreads();
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < P; x += gridDim.x * blockDim.x) {
         R in[rbcprog::NFIELD][L];

@@ -34,7 +34,9 @@ __global__ void __launch_bounds__(kPenThreads) k_penalize(const R* __restrict__ 
 {
     __shared__ double scf[2 * L * 4 * L];
     __shared__ double red[kPenThreads / 32][4 * L];
+    pdl_trigger();
     for (int i = threadIdx.x; i < 2 * L * 4 * L; i += blockDim.x) scf[i] = cf[i];
+    pdl_wait(); // the contraction is complete
     __syncthreads();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const double m = p < P ? mask[p] : 0.0;
@@ -112,6 +114,8 @@ __global__ void __launch_bounds__(kPenFgThreads) k_penalize_fg(const double* __r
                                                                double* __restrict__ NFG)
 {
     __shared__ double S[4 * L];
+    pdl_trigger();
+    pdl_wait(); // the column pass has written NFG
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int t = warp; t < 4 * L; t += nwarp) {
         double s = 0.0;

@@ -153,7 +153,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r(
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + G.nx;
+    pdl_trigger();
     load_twiddles<R>(tw, twx, G.nx);
+    pdl_wait();
     const int nx = G.nx, st = px.stride;
     const int row0 = 2 * NP * blockIdx.x;           // first row (plane * Ny + y)
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
@@ -209,7 +211,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c(
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + G.nx;
+    pdl_trigger();
     load_twiddles<R>(tw, twx, G.nx);
+    pdl_wait();
     const int nx = G.nx, st = px.stride;
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
@@ -259,7 +263,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + G.ny;
     const int c = blockIdx.x, k = blockIdx.y, ny = G.ny;
+    pdl_trigger();
     load_twiddles<R>(tw, twy, ny);
+    pdl_wait();
     const size_t cstride = (size_t)G.L * G.ckp * ny; // between groups
     const C* src = gh + ((size_t)k * G.ckp + c) * ny;
     for (int e = threadIdx.x; e < 13 * ny; e += blockDim.x) {
@@ -400,6 +406,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
     const int st = tp_stride(N, RX);
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
+    pdl_trigger();
+    load_twiddles<R>(tw, twx, N);
+    pdl_wait();
     // A[n] to slot n, B[n] to slot N - n (B[0] to the spare last slot st - 1 > pad(N - 1))
     const C* src = H + (size_t)plane * G.ckp * G.ny + y0;
     for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
@@ -412,7 +421,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
         const int pp = e / N, n = e - pp * N;
         if (n >= G.ckeep && n <= N - G.ckeep) buf[pp * st + rbcfft::pad(n)] = cmk<C>(0, 0);
     }
-    load_twiddles<R>(tw, twx, N);
     cp_async_wait_all();
     __syncthreads();
     for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
@@ -460,13 +468,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     const int pp = threadIdx.x / RX, t = threadIdx.x - pp * RX;
     const R* src = grp + (size_t)(row0 + 2 * pp) * N;
+    pdl_trigger();
+    load_twiddles<R>(tw, twx, N);
+    pdl_wait();
     C v[RX];
 #pragma unroll
     for (int a = 0; a < RX; ++a) {
         v[a].x = src[t + RX * a];
         v[a].y = src[N + t + RX * a];
     }
-    load_twiddles<R>(tw, twx, N);
     __syncthreads();
     C* S = buf + pp * st;
     rbcfft::two_pass<RX, R>(v, t, S, tw, -1);
@@ -507,10 +517,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     const size_t cstride = (size_t)G.L * G.ckp * N; // between groups
     const int gq = threadIdx.x / RX, t = threadIdx.x - gq * RX;
     const C* src = gh + ((size_t)k * G.ckp + c) * N + gq * cstride;
+    pdl_trigger();
+    load_twiddles<R>(tw, twy, N);
+    pdl_wait();
     C v[RX];
 #pragma unroll
     for (int a = 0; a < RX; ++a) v[a] = src[t + RX * a];
-    load_twiddles<R>(tw, twy, N);
     __syncthreads();
     C* S = buf + gq * st;
     rbcfft::two_pass<RX, R>(v, t, S, tw, -1);

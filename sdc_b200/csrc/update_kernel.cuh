@@ -69,6 +69,8 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
     const double mpi = (k + 1) * kPi;
     double esum = 0.0, wsum = 0.0;
     const long long nwave = (long long)G.ckeep * ny;
+    pdl_trigger();
+    pdl_wait(); // N and the mean-flow terms come from the column pass
     {
         const long long e = (long long)blockIdx.x * (blockDim.x / T) + threadIdx.x / T; // wavenumber c * ny + r
         const int c = (int)(e / ny), r = (int)(e - (long long)c * ny);
