@@ -133,6 +133,13 @@ struct rbc_handle {
     // CUDA graphs of one steady-state (AB2) step: [0] without, [1] with the pending
     // tracer advance at its start
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // kChainSteps steady steps with pending tracer advances in one graph: each advance is
+    // joined just before the next step's contraction (which rewrites the node records it
+    // reads) instead of at the end of its own step, so it also overlaps the next synthesis
+    cudaGraphExec_t graph_chain = nullptr;
+    cudaStream_t graph_chain_stream = nullptr;
+    int graph_chain_launches = 0;
+    bool chain_tracers = false;   // while capturing that graph
     cudaStream_t graph_stream[2] = {nullptr, nullptr};
     int graph_launches[2] = {0, 0};
     bool use_graphs = true;
@@ -485,6 +492,7 @@ template <typename R, int L> static void launch_penalize_fg(rbc_handle* h);
 template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, bool defer_join = false)
 {
     typedef typename cplx_t<R>::type C;
+    join_tracer(h); // an advance still reading the node records ends before they are rewritten
     RBC_DISPATCH_L(launch_contract, R, G.L, h);
     if (h->tracer_pending) {
         snapshot_step(h);
@@ -656,7 +664,7 @@ template <typename R> static void run_step(rbc_handle* h)
     run_analysis<R>(h, h->G, true); // the contraction also writes the tracers' node records
     h->tracer_pending = false;
     RBC_DISPATCH_L(launch_update, R, h->G.L, h);
-    join_tracer(h);
+    if (!h->chain_tracers) join_tracer(h); // in a chain the next step's analysis joins it
     h->have_hist = true;
     h->tracer_pending = h->ntr > 0;
     ++h->host_steps;
@@ -883,6 +891,8 @@ static void free_all(rbc_handle* h)
 {
     for (int v = 0; v < 2; ++v)
         if (h->graph[v]) cudaGraphExecDestroy(h->graph[v]);
+    if (h->graph_chain) cudaGraphExecDestroy(h->graph_chain);
+    h->graph_chain = nullptr;
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
     h->evpool.clear();
     for (void* p : h->owned) cudaFree(p);
@@ -1301,6 +1311,48 @@ static void capture_step(rbc_handle* h, int variant)
     h->host_steps = hs;
 }
 
+constexpr int kChainSteps = 8;
+
+// Captures kChainSteps steady steps, each with a pending tracer advance, into one graph.
+static void capture_chain(rbc_handle* h)
+{
+    if (h->graph_chain) {
+        cudaGraphExecDestroy(h->graph_chain);
+        h->graph_chain = nullptr;
+    }
+    const long long launches = h->launches, hs = h->host_steps;
+    cudaGraph_t g = nullptr;
+    RBC_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->launches = 0;
+    h->chain_tracers = true;
+    try {
+        for (int i = 0; i < kChainSteps; ++i) {
+            h->have_hist = true;
+            h->tracer_pending = true;
+            if (h->mixed) run_step<float>(h);
+            else run_step<double>(h);
+        }
+        join_tracer(h); // the last advance
+    } catch (...) {
+        h->chain_tracers = false;
+        h->join_pending = false;
+        cudaStreamEndCapture(h->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    h->chain_tracers = false;
+    RBC_CUDA(cudaStreamEndCapture(h->stream, &g));
+    h->graph_chain_launches = (int)h->launches;
+    cudaError_t e = cudaGraphInstantiate(&h->graph_chain, g, 0);
+    cudaGraphDestroy(g);
+    RBC_CUDA(e);
+    h->graph_chain_stream = h->stream;
+    h->have_hist = true;
+    h->tracer_pending = true;
+    h->launches = launches;
+    h->host_steps = hs;
+}
+
 rbc_status rbc_step_async(rbc_handle* h, int nsteps)
 {
     if (nsteps < 0) return fail(h, RBC_ERR_INVALID_ARG, "negative step count");
@@ -1310,6 +1362,15 @@ rbc_status rbc_step_async(rbc_handle* h, int nsteps)
     for (int s = 0; s < nsteps; ++s) {
         // graphs need a real stream (the legacy default stream cannot be captured)
         if (h->use_graphs && h->have_hist && !h->profiling && h->stream != nullptr) {
+            if (h->tracer_pending && h->ntr > 0 && nsteps - s >= kChainSteps) {
+                if (!h->graph_chain || h->graph_chain_stream != h->stream) capture_chain(h);
+                RBC_CUDA(cudaGraphLaunch(h->graph_chain, h->stream));
+                h->launches += h->graph_chain_launches;
+                h->tracer_pending = true;
+                h->host_steps += kChainSteps;
+                s += kChainSteps - 1;
+                continue;
+            }
             const int v = h->tracer_pending ? 1 : 0;
             if (!h->graph[v] || h->graph_stream[v] != h->stream) capture_step(h, v);
             RBC_CUDA(cudaGraphLaunch(h->graph[v], h->stream));
