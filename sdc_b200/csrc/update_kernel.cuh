@@ -70,14 +70,14 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
     double esum = 0.0, wsum = 0.0;
     const long long nwave = (long long)G.ckeep * ny;
     pdl_trigger();
-    pdl_wait(); // N and the mean-flow terms come from the column pass
     {
         const long long e = (long long)blockIdx.x * (blockDim.x / T) + threadIdx.x / T; // wavenumber c * ny + r
         const int c = (int)(e / ny), r = (int)(e - (long long)c * ny);
-        // the class index and the vectors are fetched together: the vector loads are
-        // predicated on the kept band by its formula (always in bounds), the tables wait
-        // for the class index
+        // the class index is constant and is fetched before the wait; after it the
+        // vectors and the class's table rows are fetched together (the vector loads are
+        // predicated on the kept band by its formula, always in bounds)
         const int cl = (e < nwave) ? __ldg(A.cls + e) : -1;   // uniform over the team
+        pdl_wait(); // N and the mean-flow terms come from the column pass
         const bool geo = e < nwave && k < L && c < G.ckeep && row_kept(r, ny);
         const size_t o = (size_t)e;
         const int ry = wrap_row(r, ny);
