@@ -140,6 +140,10 @@ struct rbc_handle {
     cudaStream_t graph_chain_stream = nullptr;
     int graph_chain_launches = 0;
     bool chain_tracers = false;   // while capturing that graph
+    // programmatic dependent launches off: set for ensemble members, whose steps run as
+    // concurrent graph branches (CTAs waiting at griddepcontrol.wait would hold SM
+    // resources the other branches can use)
+    bool no_pdl = false;
     cudaStream_t graph_stream[2] = {nullptr, nullptr};
     int graph_launches[2] = {0, 0};
     bool use_graphs = true;
@@ -327,7 +331,7 @@ static void launch_dep(rbc_handle* h, void (*kern)(KArgs...), dim3 grid, dim3 bl
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = h->profiling ? 0 : 1;
+    cfg.numAttrs = (h->profiling || h->no_pdl) ? 0 : 1;
     RBC_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
 }
 
@@ -1977,6 +1981,7 @@ rbc_status rbc_ensemble_create(const rbc_params* members, int n, int nstreams, r
             rbc_ensemble_destroy(e);
             return s;
         }
+        h->no_pdl = true;
         e->members.push_back(h);
     }
     // longest-processing-time-first assignment of members to worker streams

@@ -35,6 +35,19 @@ RBC_D void load_twiddles(typename cplx_t<R>::type* tw, const double2* twg, int n
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = cmk<C>(twg[t].x, twg[t].y);
 }
 
+// The same table copy issued asynchronously where no conversion is needed (FP64): it
+// completes at the kernel's next cp_async_wait_all(), so its latency overlaps the data loads
+// that follow (and the predecessor's tail under programmatic launch).
+template <typename R>
+RBC_D void load_twiddles_async(typename cplx_t<R>::type* tw, const double2* twg, int n)
+{
+    if constexpr (sizeof(typename cplx_t<R>::type) == sizeof(double2)) {
+        for (int t = threadIdx.x; t < n; t += blockDim.x) cp_async<sizeof(double2)>(tw + t, twg + t);
+    } else {
+        load_twiddles<R>(tw, twg, n);
+    }
+}
+
 template <typename R>
 RBC_D void fft_batched(typename cplx_t<R>::type* buf, const rbcfft::Plan& p, int nb,
                        const typename cplx_t<R>::type* tw, int sign)
@@ -407,7 +420,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     pdl_trigger();
-    load_twiddles<R>(tw, twx, N);
+    load_twiddles_async<R>(tw, twx, N);
     pdl_wait();
     // A[n] to slot n, B[n] to slot N - n (B[0] to the spare last slot st - 1 > pad(N - 1))
     const C* src = H + (size_t)plane * G.ckp * G.ny + y0;
@@ -469,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     const int pp = threadIdx.x / RX, t = threadIdx.x - pp * RX;
     const R* src = grp + (size_t)(row0 + 2 * pp) * N;
     pdl_trigger();
-    load_twiddles<R>(tw, twx, N);
+    load_twiddles_async<R>(tw, twx, N);
     pdl_wait();
     C v[RX];
 #pragma unroll
@@ -477,6 +490,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
         v[a].x = src[t + RX * a];
         v[a].y = src[N + t + RX * a];
     }
+    cp_async_wait_all();
     __syncthreads();
     C* S = buf + pp * st;
     rbcfft::two_pass<RX, R>(v, t, S, tw, -1);
@@ -518,11 +532,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     const int gq = threadIdx.x / RX, t = threadIdx.x - gq * RX;
     const C* src = gh + ((size_t)k * G.ckp + c) * N + gq * cstride;
     pdl_trigger();
-    load_twiddles<R>(tw, twy, N);
+    load_twiddles_async<R>(tw, twy, N);
     pdl_wait();
     C v[RX];
 #pragma unroll
     for (int a = 0; a < RX; ++a) v[a] = src[t + RX * a];
+    cp_async_wait_all();
     __syncthreads();
     C* S = buf + gq * st;
     rbcfft::two_pass<RX, R>(v, t, S, tw, -1);
