@@ -292,7 +292,7 @@ def optional_physics_forms(s64, stream, local, steps=2000):
     return out
 
 
-# Learned surrogate (north_star form 4): Fourier neural operator on (theta, u, v, w) at
+# Learned surrogate (the fourth form): Fourier neural operator on (theta, u, v, w) at
 # 12 Gauss-Legendre levels of the 128 x 128 x 6 grid (Lx = Ly = 16), one surrogate
 # interval = 40 plain steps of dt = 5e-4 (0.02 time units).
 SURR = dict(nx=128, ny=128, nz=6, lx=16.0, ly=16.0, pr=1.0, dt=5e-4)
@@ -695,7 +695,7 @@ def main():
     d = s.diagnostics()
     assert np.isfinite(d["ke"]) and np.all(np.isfinite(out_tr)) and all(np.all(np.isfinite(a)) for a in out_state)
 
-    # ---- the mixed form on the same workload (north_star form 1): throughput from the
+    # ---- the mixed form on the same workload (the first form): throughput from the
     # convective FP64 state reached above, and its diagnostics error against the FP64 form
     # over the same 2000 steps from that state
     forms = None
