@@ -72,6 +72,9 @@ typedef struct {
                           PENALIZED builds (-eta, main.cu:117-123; 0.01 there by default);
                           0: none */
     int penalization_mask;   /* rbc_pen_mask: the build target's mask */
+    double mean_F;     /* nonzero: before every step F of the lowest vertical mode is set to
+                          (mean_F, 0), the reference's -mean_F (force_mean, util.cu:74-81,
+                          main.cu:139-140, 566-568); 0: no forcing */
 } rbc_params;
 
 /* Masks of the penalized operator (nonlinear_operator_rayleigh_noslip.cu:1653-1738; 1 in

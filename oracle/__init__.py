@@ -88,6 +88,8 @@ def lib():
         L.oracle_pen_mask.restype = None
         L.oracle_set_penalization.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.oracle_set_penalization.restype = None
+        L.oracle_set_force_mean.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.oracle_set_force_mean.restype = None
         L.oracle_masker.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 4
         L.oracle_masker.restype = None
         for name in ("oracle_freeze_apply", "oracle_heat_apply"):
@@ -248,6 +250,10 @@ class Oracle:
 
     def step(self, n=1):
         lib().oracle_step(self.h, n)
+
+    def set_force_mean(self, mean_F):
+        """F of the lowest mode set to mean_F before every step (0: off)."""
+        lib().oracle_set_force_mean(self.h, mean_F)
 
     def set_penalization(self, eta, kind="rectangle"):
         """Penalized nonlinear operator (eta > 0) with the named mask; eta = 0 turns it off."""

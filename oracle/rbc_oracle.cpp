@@ -1168,8 +1168,10 @@ struct Solver {
     }
 
     // main.cu:612-637: step_time, make_real, tracers
+    double force_mean = 0.0; // the reference's -mean_F (force_mean, util.cu:74-81)
     void step()
     {
+        if (force_mean != 0.0) F[0] = cd(force_mean, 0.0); // main.cu:566-568, before step_time
         step_time();
         make_real(th);
         make_real(f);
@@ -1353,6 +1355,9 @@ void oracle_pen_mask(int nx, int ny, int kind, double* out)
         out[i] = m;
     }
 }
+
+// F of the lowest mode set to (mean_F, 0) before every step (0: off).
+void oracle_set_force_mean(oracle_handle* h, double mean_F) { h->s.force_mean = mean_F; }
 
 // Turns the penalized operator on (eta > 0, mask kind as oracle_pen_mask) or off (eta 0).
 void oracle_set_penalization(oracle_handle* h, double eta, int kind)

@@ -32,7 +32,8 @@ class _Params(ctypes.Structure):
                 ("n_tracers", ctypes.c_int), ("device", ctypes.c_int), ("diag_capacity", ctypes.c_int),
                 ("tune", ctypes.c_int), ("tracer_diffusivity", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong),
                 ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int), ("field_ops", ctypes.c_int),
-                ("penalization_eta", ctypes.c_double), ("penalization_mask", ctypes.c_int)]
+                ("penalization_eta", ctypes.c_double), ("penalization_mask", ctypes.c_int),
+                ("mean_F", ctypes.c_double)]
 
 
 class _Diag(ctypes.Structure):
@@ -234,14 +235,14 @@ def dump_write(path, arr, real_bytes=8):
 
 def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False,
                 tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
-                penalization=None):
+                penalization=None, mean_F=0.0):
     """penalization: None, or (eta, mask) with mask one of PEN_MASKS."""
     ops = 0
     for name in field_ops:
         ops |= FIELD_OPS[name]
     eta, kind = penalization if penalization else (0.0, "rectangle")
     return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)),
-                   tracer_diffusivity, noise_seed, track_frames, track_period, ops, eta, PEN_MASKS[kind])
+                   tracer_diffusivity, noise_seed, track_frames, track_period, ops, eta, PEN_MASKS[kind], mean_F)
 
 
 def track_write(path, frames, times, description=""):
@@ -296,7 +297,7 @@ class Solver:
 
     def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0,
                  tune=False, tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
-                 penalization=None, _handle=None):
+                 penalization=None, mean_F=0.0, _handle=None):
         self.nx, self.ny, self.L = nx, ny, nz
         self.mox = nx // 2 + 1
         self.n_tracers = n_tracers
@@ -307,7 +308,7 @@ class Solver:
             self.h = _handle
             return
         p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune,
-                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops, penalization)
+                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops, penalization, mean_F)
         h = ctypes.c_void_p()
         st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
         if st != RBC_OK:

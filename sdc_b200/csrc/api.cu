@@ -662,8 +662,20 @@ template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h)
 // One iteration of the reference loop (main.cu:612-637). The tracer advance of a step
 // needs the velocity of the state after it, which is exactly the synthesis the next
 // step starts with; it is therefore run there (or by flush_tracers).
+__global__ void k_force_mean(double2* __restrict__ FG, double v) { FG[0] = make_double2(v, 0.0); }
+
+template <typename R> static void flush_tracers_t(rbc_handle* h, bool overlap);
+
 template <typename R> static void run_step(rbc_handle* h)
 {
+    if (h->prm.mean_F != 0.0) {
+        // force_mean comes before the step, after the previous step's tracer advance, which
+        // must see the unforced mean flow: a pending advance runs on its own synthesis first
+        flush_tracers_t<R>(h, false);
+        k_force_mean<<<1, 1, 0, h->stream>>>(h->FG, h->prm.mean_F);
+        RBC_CUDA(cudaGetLastError());
+        ++h->launches;
+    }
     run_synthesis<R>(h, h->th, h->f, h->g, h->FG);
     run_analysis<R>(h, h->G, true); // the contraction also writes the tracers' node records
     h->tracer_pending = false;
@@ -1020,6 +1032,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         return RBC_ERR_INVALID_ARG;
     if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED) return RBC_ERR_INVALID_ARG;
     if (p->field_ops & ~(RBC_FIELD_FREEZE | RBC_FIELD_HEAT | RBC_FIELD_SCALE)) return RBC_ERR_INVALID_ARG;
+    if (!std::isfinite(p->mean_F)) return RBC_ERR_INVALID_ARG;
     if (!(p->penalization_eta >= 0 && std::isfinite(p->penalization_eta)) || p->penalization_mask < 0 ||
         p->penalization_mask > RBC_PEN_EVERYWHERE)
         return RBC_ERR_INVALID_ARG;

@@ -25,6 +25,8 @@
 //   -penalized rectangle|circle|diskarray|everywhere   the penalized operator with that mask
 //                        (the reference's PENALIZED build targets)
 //   -eta e               its eta (main.cu:117-123; default 0.01)
+//   -mean_F F            force the mean flow F of the lowest mode to F before every step
+//                        (main.cu:139-140, 566-568)
 // Writes simulation.log (main.cu:402-426) and returns non-zero on any library error.
 #include "rbc.h"
 
@@ -117,6 +119,7 @@ int main(int argc, char** argv)
         }
         p.penalization_eta = a.num("-eta", 0.01);
     }
+    p.mean_F = a.num("-mean_F", 0.0);
     const char* dir = a.str("-dir");
     std::string out = dir ? dir : ".";
     if (dir) mkdir(dir, 0755);
