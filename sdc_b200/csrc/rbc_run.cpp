@@ -27,6 +27,17 @@
 //   -eta e               its eta (main.cu:117-123; default 0.01)
 //   -mean_F F            force the mean flow F of the lowest mode to F before every step
 //                        (main.cu:139-140, 566-568)
+// Tracers the reference's way (main.cu:150-199, 490-532, 620-660, 719-726):
+//   -npart n -le D       n tracers with diffusivity D. As in the reference, one tracer set is
+//                        made per -le value and none without it; one value only here
+//                        (-le_count 1), a run with several sets needs one process per value
+//   -part_center | -part_center_sigma | -part_diagonal | -part_pairs |
+//   -part_coord_sigma x y  start patterns (sigma 0.125), -part_sigma s overrides sigma
+//   -write_tracks_every p  record every p-th step; at each state dump the recorded frames
+//                        go to particles_le<D>_<step>.trkss
+//   -calc_secondmoment   second moment of the positions after every step, secondmoment_0.dat
+//   -no_step_time        advance the tracers only, on the fixed initial flow
+//   -snapshot_freq n     accepted; the reference's snapshot output is disabled, so is ours
 // Writes simulation.log (main.cu:402-426) and returns non-zero on any library error.
 #include "rbc.h"
 
@@ -120,6 +131,41 @@ int main(int argc, char** argv)
         p.penalization_eta = a.num("-eta", 0.01);
     }
     p.mean_F = a.num("-mean_F", 0.0);
+    // tracers as main.cu configures them
+    const int npart = (int)a.num("-npart", 0);
+    double lewis = 0.0;
+    if (a.has("-le")) {
+        if ((int)a.num("-le_count", 1) != 1) {
+            std::fprintf(stderr, "several Lewis numbers (tracer sets) need one process per -le value\n");
+            return 2;
+        }
+        lewis = a.num("-le", 0.0);
+        if (npart > 0) {
+            p.n_tracers = npart;
+            p.tracer_diffusivity = lewis;
+        }
+    }
+    int part_type = RBC_TRACERS_RANDOM;
+    double part_sigma = 0.0, part_cx = 0.0, part_cy = 0.0;
+    if (a.has("-part_center")) part_type = RBC_TRACERS_CENTER;
+    if (a.has("-part_center_sigma")) { part_type = RBC_TRACERS_CENTER_SIGMA; part_sigma = 0.125; }
+    if (a.has("-part_diagonal")) part_type = RBC_TRACERS_DIAGONAL;
+    if (a.has("-part_pairs")) part_type = RBC_TRACERS_PAIRS;
+    if (a.has("-part_coord_sigma")) {
+        part_type = RBC_TRACERS_COORD_SIGMA;
+        part_cx = a.num("-part_coord_sigma", 0.0, 0, true);
+        part_cy = a.num("-part_coord_sigma", 0.0, 1, true);
+        part_sigma = 0.125;
+    }
+    if (a.has("-part_sigma")) part_sigma = a.num("-part_sigma", 0.0, 0, true);
+    const bool write_tracks = a.has("-write_tracks_every") && p.n_tracers > 0;
+    const int track_every = std::max(1, (int)a.num("-write_tracks_every", 1));
+    if (write_tracks) {
+        p.track_frames = 256;
+        p.track_period = track_every;
+    }
+    const bool moments = a.has("-calc_secondmoment") && p.n_tracers > 0;
+    const bool do_step = !a.has("-no_step_time");
     const char* dir = a.str("-dir");
     std::string out = dir ? dir : ".";
     if (dir) mkdir(dir, 0755);
@@ -150,7 +196,12 @@ int main(int argc, char** argv)
             rc |= check(rbc_init_fields(h, seed, a.num("-init_amp", 1e-3), a.num("-init_kmax", 4.0)), h,
                         "rbc_init_fields");
     }
-    if (!rc && p.n_tracers > 0) rc |= check(rbc_tracers_seed(h, seed), h, "rbc_tracers_seed");
+    if (!rc && p.n_tracers > 0) {
+        if (npart > 0)
+            rc |= check(rbc_tracers_init(h, part_type, seed, part_cx, part_cy, 0.0, part_sigma), h, "rbc_tracers_init");
+        else
+            rc |= check(rbc_tracers_seed(h, seed), h, "rbc_tracers_seed");
+    }
     if (rc) {
         rbc_destroy(h);
         return 1;
@@ -168,6 +219,21 @@ int main(int argc, char** argv)
             std::fprintf(log, "\n");
             std::fclose(log);
         }
+    }
+
+    // tracer outputs: recorded frames since the last dump, the second-moment file
+    std::vector<float> frames, ring(write_tracks ? (size_t)256 * 3 * p.n_tracers : 0);
+    std::vector<unsigned int> frame_steps, ring_steps(write_tracks ? 256 : 0);
+    char track_desc[512];
+    std::snprintf(track_desc, sizeof track_desc,
+                  "Particle tracks.  Simulation: Ra=%.1lf Pr=%.1lf Size=%.1lfx%.1lfx1.0  Technical: Modes=%dx%dx%d "
+                  "dt=%.3lf  Tracks: Le=%.0le ",
+                  p.ra, p.pr, p.lx, p.ly, p.nx, p.ny, p.nz, p.dt, lewis);
+    FILE* m2 = nullptr;
+    if (moments) {
+        // datapoint_writer's format (output/datapoint_writer.cu:21-45)
+        m2 = std::fopen((out + "/secondmoment_0.dat").c_str(), "w");
+        if (m2) std::fprintf(m2, "# Data point writer\n# Le %.9f\n# Data ordering: t, val\n", lewis);
     }
 
     long long done = 0;
@@ -189,9 +255,23 @@ int main(int argc, char** argv)
             if (at > 0) chunk = std::min(chunk, at > i ? at - i : 1);
         if (write_every > 0) chunk = std::min(chunk, write_every - done % write_every);
         if (diag_every > 0) chunk = std::min(chunk, diag_every - done % diag_every);
-        rc |= check(rbc_step(h, (int)chunk), h, "rbc_step");
+        if (write_tracks) chunk = std::min(chunk, (long long)255 * track_every); // ring of 256 frames
+        if (moments || !do_step) chunk = 1;
+        if (do_step) rc |= check(rbc_step(h, (int)chunk), h, "rbc_step");
+        else rc |= check(rbc_tracers_advance(h), h, "rbc_tracers_advance");
         done += chunk;
         if (rc) break;
+        if (write_tracks) {
+            int n = 0;
+            rc |= check(rbc_tracks_read(h, ring.data(), ring_steps.data(), 256, &n), h, "rbc_tracks_read");
+            frames.insert(frames.end(), ring.begin(), ring.begin() + (size_t)n * 3 * p.n_tracers);
+            frame_steps.insert(frame_steps.end(), ring_steps.begin(), ring_steps.begin() + n);
+        }
+        if (m2) {
+            double mo[4];
+            rc |= check(rbc_tracer_moments(h, mo), h, "rbc_tracer_moments");
+            std::fprintf(m2, "%g\t%g\n", done * p.dt, mo[2]);
+        }
         if (diag_every > 0 && done % diag_every == 0) {
             rbc_diag d;
             rc |= check(rbc_diagnostics(h, &d), h, "rbc_diagnostics");
@@ -201,9 +281,18 @@ int main(int argc, char** argv)
             rc |= check(rbc_save_state(h, out.c_str(), done, real_bytes), h, "rbc_save_state");
             char path[4096];
             std::snprintf(path, sizeof path, "%s/history_%08lld.bin", out.c_str(), done);
-            rc |= check(rbc_save_history(h, path), h, "rbc_save_history");
+            if (do_step) rc |= check(rbc_save_history(h, path), h, "rbc_save_history"); // none without steps
+            if (write_tracks && !frame_steps.empty()) {
+                std::snprintf(path, sizeof path, "%s/particles_le%.0le_%08lld.trkss", out.c_str(), lewis, done);
+                rc |= check(rbc_track_write(path, track_desc, frames.data(), frame_steps.data(),
+                                            (int)frame_steps.size(), p.n_tracers),
+                            nullptr, "rbc_track_write");
+                frames.clear();
+                frame_steps.clear();
+            }
         }
     }
+    if (m2) std::fclose(m2);
     rbc_destroy(h);
     return rc;
 }
