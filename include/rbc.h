@@ -72,6 +72,11 @@ typedef struct {
                           PENALIZED builds (-eta, main.cu:117-123; 0.01 there by default);
                           0: none */
     int penalization_mask;   /* rbc_pen_mask: the build target's mask */
+    int tracer_sets;   /* the tracers form this many equal consecutive sets (0 or 1: one),
+                          as the reference makes one particle_tracer per Lewis number
+                          (main.cu:490-505); each set has its own diffusivity
+                          (rbc_tracer_set_diffusivity), start pattern (rbc_tracers_init_set)
+                          and moments (rbc_tracer_moments_set) */
     double mean_F;     /* nonzero: before every step F of the lowest vertical mode is set to
                           (mean_F, 0), the reference's -mean_F (force_mean, util.cu:74-81,
                           main.cu:139-140, 566-568); 0: no forcing */
@@ -236,6 +241,15 @@ rbc_status rbc_tracers_advance(rbc_handle* h);
  *   out[3] = sum over pairs (2i, 2i+1) of dx^2 + dy^2, each |d| above half the box
  *            replaced by box - |d| (PERIODIC), divided by n/2 (integer division). */
 rbc_status rbc_tracer_moments(rbc_handle* h, double* out);
+/* Tracer sets (rbc_params.tracer_sets): set s holds tracers [s n/sets, (s + 1) n/sets).
+ * rbc_tracer_set_diffusivity sets the D of one set (params.tracer_diffusivity is every set's
+ * initial value; takes effect from the next advance, captured step graphs included);
+ * rbc_tracers_init_set gives one set the start pattern of rbc_tracers_init (n/sets tracers);
+ * rbc_tracer_moments_set returns rbc_tracer_moments of one set. */
+rbc_status rbc_tracer_set_diffusivity(rbc_handle* h, int set, double D);
+rbc_status rbc_tracers_init_set(rbc_handle* h, int set, int type, unsigned long long seed, double cx, double cy,
+                                double cz, double sigma);
+rbc_status rbc_tracer_moments_set(rbc_handle* h, int set, double* out);
 /* Recorded tracks (the reference's position buffer, get_particle_positions and
  * track_writer::append, particle_tracer.cu:273-309, output/track_writer.cu:21-70).
  * With track_frames > 0 the positions of every step m with m % track_period == 0 are

@@ -88,6 +88,8 @@ def lib():
         L.oracle_pen_mask.restype = None
         L.oracle_set_penalization.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.oracle_set_penalization.restype = None
+        L.oracle_set_tracer_sets.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.oracle_set_tracer_sets.restype = None
         L.oracle_set_force_mean.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.oracle_set_force_mean.restype = None
         L.oracle_masker.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 4
@@ -250,6 +252,11 @@ class Oracle:
 
     def step(self, n=1):
         lib().oracle_step(self.h, n)
+
+    def set_tracer_sets(self, diffusivities):
+        """Equal consecutive tracer sets with their own diffusivities."""
+        d = np.ascontiguousarray(diffusivities, dtype=np.float64)
+        lib().oracle_set_tracer_sets(self.h, d.size, _ptr(d))
 
     def set_force_mean(self, mean_F):
         """F of the lowest mode set to mean_F before every step (0: off)."""

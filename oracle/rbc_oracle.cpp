@@ -1123,12 +1123,17 @@ struct Solver {
     // Tracer diffusion (D, the reference's -le value) and the seed of its noise.
     double tr_diff = 0.0;
     uint64_t noise_seed = 0;
+    // several tracer sets (main.cu:490-505: one particle_tracer per Lewis number): equal
+    // consecutive ranges of the particles, each with its own D (empty: tr_diff for all)
+    std::vector<double> set_diff;
 
     // particle_tracer::step_particles for the positions of step m.
     void step_tracers(long long m)
     {
         if (tx.empty()) return;
-        const double sig = tr_diff > 0 ? std::sqrt(2.0 * tr_diff * p.dt) : 0.0;
+        const double sig0 = tr_diff > 0 ? std::sqrt(2.0 * tr_diff * p.dt) : 0.0;
+        const int nsets = set_diff.empty() ? 1 : (int)set_diff.size();
+        const int per_set = (int)tx.size() / nsets;
         std::vector<double> ux, uy, uz;
         velocity_grid(ux, uy, uz);
         const double dt = p.dt;
@@ -1149,6 +1154,8 @@ struct Solver {
             x += (dx1 + 2 * (dx2 + dx3) + dx4) / 6.;
             y += (dy1 + 2 * (dy2 + dy3) + dy4) / 6.;
             z += (dz1 + 2 * (dz2 + dz3) + dz4) / 6.;
+            const double Dt = set_diff.empty() ? -1.0 : set_diff[t / per_set];
+            const double sig = Dt < 0 ? sig0 : (Dt > 0 ? std::sqrt(2.0 * Dt * p.dt) : 0.0);
             if (sig > 0) {
                 x += sig * diffusion_normal(noise_seed, m, n, t, 0);
                 y += sig * diffusion_normal(noise_seed, m, n, t, 1);
@@ -1513,6 +1520,11 @@ void oracle_tracers_get(oracle_handle* h, double* xyz)
 }
 // Advances tracers with the current velocity field only (no fluid step).
 void oracle_tracers_advance(oracle_handle* h) { h->s.step_tracers(h->s.steps); }
+// Splits the tracers into `sets` equal consecutive ranges with diffusivities D[set].
+void oracle_set_tracer_sets(oracle_handle* h, int sets, const double* D)
+{
+    h->s.set_diff.assign(D, D + sets);
+}
 void oracle_set_diffusion(oracle_handle* h, double D, uint64_t seed)
 {
     h->s.tr_diff = D;

@@ -33,7 +33,7 @@ class _Params(ctypes.Structure):
                 ("tune", ctypes.c_int), ("tracer_diffusivity", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong),
                 ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int), ("field_ops", ctypes.c_int),
                 ("penalization_eta", ctypes.c_double), ("penalization_mask", ctypes.c_int),
-                ("mean_F", ctypes.c_double)]
+                ("tracer_sets", ctypes.c_int), ("mean_F", ctypes.c_double)]
 
 
 class _Diag(ctypes.Structure):
@@ -80,7 +80,8 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run",
            "rbc_fno_set_train_options", "rbc_structure_function", "rbc_freeze_mask", "rbc_freeze_apply",
            "rbc_heat_mask", "rbc_heat_apply", "rbc_field_ops_reset", "rbc_masker",
-           "rbc_diagnostics_async", "rbc_diagnostics_get"]
+           "rbc_diagnostics_async", "rbc_diagnostics_get",
+           "rbc_tracer_set_diffusivity", "rbc_tracers_init_set", "rbc_tracer_moments_set"]
 FIELD_OPS = {"freeze": 1, "heat": 2, "scale": 4}
 MASK_SHAPES = {"circle": 0, "rectangle": 1}
 PEN_MASKS = {"rectangle": 0, "circle": 1, "disk_array": 2, "everywhere": 3}
@@ -162,6 +163,9 @@ def lib():
     L.rbc_field_ops_reset.argtypes = [vp]
     L.rbc_masker.argtypes = [vp] + [ctypes.c_double] * 4
     L.rbc_diagnostics_async.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.rbc_tracer_set_diffusivity.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.rbc_tracers_init_set.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong] + [ctypes.c_double] * 4
+    L.rbc_tracer_moments_set.argtypes = [vp, ctypes.c_int, _dp]
     L.rbc_diagnostics_get.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(_Diag)]
     L.rbc_fno_create.argtypes = [ctypes.POINTER(_FnoParams), ctypes.POINTER(vp)]
     L.rbc_fno_destroy.argtypes = [vp]
@@ -235,14 +239,14 @@ def dump_write(path, arr, real_bytes=8):
 
 def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False,
                 tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
-                penalization=None, mean_F=0.0):
+                penalization=None, mean_F=0.0, tracer_sets=1):
     """penalization: None, or (eta, mask) with mask one of PEN_MASKS."""
     ops = 0
     for name in field_ops:
         ops |= FIELD_OPS[name]
     eta, kind = penalization if penalization else (0.0, "rectangle")
     return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)),
-                   tracer_diffusivity, noise_seed, track_frames, track_period, ops, eta, PEN_MASKS[kind], mean_F)
+                   tracer_diffusivity, noise_seed, track_frames, track_period, ops, eta, PEN_MASKS[kind], tracer_sets, mean_F)
 
 
 def track_write(path, frames, times, description=""):
@@ -297,7 +301,7 @@ class Solver:
 
     def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0,
                  tune=False, tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
-                 penalization=None, mean_F=0.0, _handle=None):
+                 penalization=None, mean_F=0.0, tracer_sets=1, _handle=None):
         self.nx, self.ny, self.L = nx, ny, nz
         self.mox = nx // 2 + 1
         self.n_tracers = n_tracers
@@ -308,7 +312,7 @@ class Solver:
             self.h = _handle
             return
         p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune,
-                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops, penalization, mean_F)
+                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops, penalization, mean_F, tracer_sets)
         h = ctypes.c_void_p()
         st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
         if st != RBC_OK:
@@ -431,6 +435,17 @@ class Solver:
     def tracers_init(self, pattern, seed=0, coord=(0.0, 0.0, 0.0), sigma=0.0):
         """Start positions by pattern (random, center, center_sigma, diagonal, pairs, coord_sigma)."""
         self._check(lib().rbc_tracers_init(self.h, TRACER_PATTERNS[pattern], seed, *coord, sigma))
+
+    def tracer_set_diffusivity(self, set_index, D):
+        self._check(lib().rbc_tracer_set_diffusivity(self.h, set_index, D))
+
+    def tracers_init_set(self, set_index, pattern, seed=0, coord=(0.0, 0.0, 0.0), sigma=0.0):
+        self._check(lib().rbc_tracers_init_set(self.h, set_index, TRACER_PATTERNS[pattern], seed, *coord, sigma))
+
+    def tracer_moments_set(self, set_index):
+        out = np.zeros(4)
+        self._check(lib().rbc_tracer_moments_set(self.h, set_index, _p(out)))
+        return out
 
     def tracer_moments(self):
         """(<x>, <y>, second moment, pair second moment) of the current positions."""

@@ -102,6 +102,9 @@ struct rbc_handle {
     void* nv = nullptr;           // [Ny*Nx][NodeRec] node records for the tracers (R)
     bool tracer_pending = false;  // a fluid step ran whose tracer advance is not done yet
     double tr_sigma = 0.0;        // sqrt(2 D dt) of the diffusion step
+    int tr_sets = 1, tr_per_set = 0;  // equal consecutive tracer sets
+    double* set_sig = nullptr;    // [tr_sets] sqrt(2 D dt) of each set (device)
+    std::vector<double> set_sig_host;
     float* trk = nullptr;         // [trk_cap][3][ntr] recorded frames
     int trk_cap = 0, trk_period = 1;
     long long trk_next = 0;       // step of the oldest unread frame (a multiple of trk_period)
@@ -588,6 +591,11 @@ static void tracer_setup(rbc_handle* h)
     RBC_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     const double D = h->prm.tracer_diffusivity;
     h->tr_sigma = D > 0 ? std::sqrt(2.0 * D * h->G.dt) : 0.0;
+    h->tr_sets = h->prm.tracer_sets > 1 ? h->prm.tracer_sets : 1;
+    h->tr_per_set = h->ntr / h->tr_sets;
+    h->set_sig_host.assign(h->tr_sets, h->tr_sigma);
+    h->set_sig = dalloc<double>(h->tr_sets, h->owned);
+    RBC_CUDA(cudaMemcpy(h->set_sig, h->set_sig_host.data(), h->tr_sets * sizeof(double), cudaMemcpyHostToDevice));
     h->trk_period = h->prm.track_period > 1 ? h->prm.track_period : 1;
     h->trk_cap = h->prm.track_frames;
     if (h->trk_cap > 0) {
@@ -640,7 +648,8 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.ly = h->G.ly;
     A.dt = h->G.dt;
     A.zmax = 0.5f - 1e-3;
-    A.sigma = h->tr_sigma;
+    A.set_sigma = h->set_sig;
+    A.per_set = h->tr_per_set;
     A.noise_seed = h->prm.noise_seed;
     A.step_counter = h->tr_step;
     A.track = h->trk;
@@ -1027,6 +1036,8 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
     *out = nullptr;
     if (!fft_len_ok(p->nx) || !fft_len_ok(p->ny)) return RBC_ERR_INVALID_ARG;
     if (!(p->lx > 0 && p->ly > 0 && p->pr > 0 && p->dt > 0) || p->n_tracers < 0) return RBC_ERR_INVALID_ARG;
+    if (p->tracer_sets < 0 || (p->tracer_sets > 1 && (p->n_tracers == 0 || p->n_tracers % p->tracer_sets)))
+        return RBC_ERR_INVALID_ARG;
     if (!(p->tracer_diffusivity >= 0 && std::isfinite(p->tracer_diffusivity)) || p->track_frames < 0 ||
         p->track_period < 0 || (p->track_frames > 0 && p->n_tracers == 0))
         return RBC_ERR_INVALID_ARG;
@@ -1896,7 +1907,7 @@ rbc_status rbc_tracer_moments(rbc_handle* h, double* out)
     RBC_GUARD(h)
     if (h->ntr == 0) return fail(h, RBC_ERR_INVALID_ARG, "no tracers");
     flush_tracers(h);
-    k_tracer_sums<<<1, 1024, 0, h->stream>>>(h->trpos, h->ntr, h->prm.lx, h->prm.ly, h->trsums);
+    k_tracer_sums<<<1, 1024, 0, h->stream>>>(h->trpos, h->ntr, h->ntr, h->prm.lx, h->prm.ly, h->trsums);
     RBC_CUDA(cudaGetLastError());
     double s[4];
     RBC_CUDA(cudaMemcpyAsync(s, h->trsums, sizeof s, cudaMemcpyDeviceToHost, h->stream));
@@ -1906,6 +1917,60 @@ rbc_status rbc_tracer_moments(rbc_handle* h, double* out)
     out[1] = s[1] / n;
     out[2] = s[2] / n - out[0] * out[0] - out[1] * out[1];
     out[3] = s[3] / (double)(h->ntr / 2);
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_tracer_set_diffusivity(rbc_handle* h, int set, double D)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (h->ntr == 0 || set < 0 || set >= h->tr_sets || !(D >= 0 && std::isfinite(D)))
+        return fail(h, RBC_ERR_INVALID_ARG, "bad tracer set or diffusivity");
+    RBC_GUARD(h)
+    h->set_sig_host[set] = D > 0 ? std::sqrt(2.0 * D * h->G.dt) : 0.0;
+    RBC_CUDA(cudaMemcpyAsync(h->set_sig + set, &h->set_sig_host[set], sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream)); // the host value may change again right after
+    return RBC_OK;
+    RBC_GUARD_END(h)
+}
+
+rbc_status rbc_tracers_init_set(rbc_handle* h, int set, int type, unsigned long long seed, double cx, double cy,
+                                double cz, double sigma)
+{
+    if (!h) return RBC_ERR_INVALID_ARG;
+    if (h->ntr == 0 || set < 0 || set >= h->tr_sets) return fail(h, RBC_ERR_INVALID_ARG, "bad tracer set");
+    if (type < RBC_TRACERS_RANDOM || type > RBC_TRACERS_COORD_SIGMA || !(sigma >= 0))
+        return fail(h, RBC_ERR_INVALID_ARG, "unknown tracer pattern or negative sigma");
+    const int ns = h->tr_per_set, n = h->ntr;
+    if (type == RBC_TRACERS_PAIRS && (ns & 1))
+        return fail(h, RBC_ERR_INVALID_ARG, "position pairs need an even number of tracers per set");
+    std::vector<double> all(3 * (size_t)n), part(3 * (size_t)ns);
+    rbc_status st = rbc_tracers_get(h, all.data(), n);
+    if (st != RBC_OK) return st;
+    rbchost::tracer_pattern(type, seed, ns, h->prm.lx, h->prm.ly, cx, cy, cz, sigma, part.data());
+    for (int d = 0; d < 3; ++d)
+        std::memcpy(&all[(size_t)d * n + (size_t)set * ns], &part[(size_t)d * ns], ns * sizeof(double));
+    return rbc_tracers_set(h, all.data(), n);
+}
+
+rbc_status rbc_tracer_moments_set(rbc_handle* h, int set, double* out)
+{
+    if (!out) return fail(h, RBC_ERR_INVALID_ARG, "null output");
+    RBC_GUARD(h)
+    if (h->ntr == 0 || set < 0 || set >= h->tr_sets) return fail(h, RBC_ERR_INVALID_ARG, "bad tracer set");
+    flush_tracers(h);
+    const int ns = h->tr_per_set;
+    k_tracer_sums<<<1, 1024, 0, h->stream>>>(h->trpos + (size_t)set * ns, ns, h->ntr, h->prm.lx, h->prm.ly,
+                                             h->trsums);
+    RBC_CUDA(cudaGetLastError());
+    double s[4];
+    RBC_CUDA(cudaMemcpyAsync(s, h->trsums, sizeof s, cudaMemcpyDeviceToHost, h->stream));
+    RBC_CUDA(cudaStreamSynchronize(h->stream));
+    out[0] = s[0] / ns;
+    out[1] = s[1] / ns;
+    out[2] = s[2] / ns - out[0] * out[0] - out[1] * out[1];
+    out[3] = s[3] / (double)(ns / 2);
     return RBC_OK;
     RBC_GUARD_END(h)
 }

@@ -28,14 +28,13 @@
 //   -mean_F F            force the mean flow F of the lowest mode to F before every step
 //                        (main.cu:139-140, 566-568)
 // Tracers the reference's way (main.cu:150-199, 490-532, 620-660, 719-726):
-//   -npart n -le D       n tracers with diffusivity D. As in the reference, one tracer set is
-//                        made per -le value and none without it; one value only here
-//                        (-le_count 1), a run with several sets needs one process per value
+//   -npart n -le_count k -le D1 .. Dk   k tracer sets of n tracers, set s with diffusivity
+//                        Ds; as in the reference, no tracers without -le
 //   -part_center | -part_center_sigma | -part_diagonal | -part_pairs |
 //   -part_coord_sigma x y  start patterns (sigma 0.125), -part_sigma s overrides sigma
 //   -write_tracks_every p  record every p-th step; at each state dump the recorded frames
-//                        go to particles_le<D>_<step>.trkss
-//   -calc_secondmoment   second moment of the positions after every step, secondmoment_0.dat
+//                        of set s go to particles_le<Ds>_<step>.trkss
+//   -calc_secondmoment   second moment of each set after every step, secondmoment_<s>.dat
 //   -no_step_time        advance the tracers only, on the fixed initial flow
 //   -snapshot_freq n     accepted; the reference's snapshot output is disabled, so is ours
 // Writes simulation.log (main.cu:402-426) and returns non-zero on any library error.
@@ -133,18 +132,18 @@ int main(int argc, char** argv)
     p.mean_F = a.num("-mean_F", 0.0);
     // tracers as main.cu configures them
     const int npart = (int)a.num("-npart", 0);
-    double lewis = 0.0;
+    std::vector<double> lewis;
     if (a.has("-le")) {
-        if ((int)a.num("-le_count", 1) != 1) {
-            std::fprintf(stderr, "several Lewis numbers (tracer sets) need one process per -le value\n");
-            return 2;
-        }
-        lewis = a.num("-le", 0.0);
+        const int le_count = std::max(1, (int)a.num("-le_count", 1));
+        for (int k = 0; k < le_count; ++k) lewis.push_back(a.num("-le", 0.0, k, true));
         if (npart > 0) {
-            p.n_tracers = npart;
-            p.tracer_diffusivity = lewis;
+            p.n_tracers = npart * le_count;
+            p.tracer_sets = le_count;
+            p.tracer_diffusivity = lewis[0];
         }
     }
+    const int nsets = p.tracer_sets > 1 ? p.tracer_sets : 1;
+    if (lewis.empty()) lewis.assign(nsets, p.tracer_diffusivity); // -particles: one set, no -le
     int part_type = RBC_TRACERS_RANDOM;
     double part_sigma = 0.0, part_cx = 0.0, part_cy = 0.0;
     if (a.has("-part_center")) part_type = RBC_TRACERS_CENTER;
@@ -197,10 +196,17 @@ int main(int argc, char** argv)
                         "rbc_init_fields");
     }
     if (!rc && p.n_tracers > 0) {
-        if (npart > 0)
-            rc |= check(rbc_tracers_init(h, part_type, seed, part_cx, part_cy, 0.0, part_sigma), h, "rbc_tracers_init");
-        else
+        if (npart > 0) {
+            // one particle_tracer per Lewis number (main.cu:494-500), each with its own draws
+            for (int k = 0; k < nsets && !rc; ++k) {
+                rc |= check(rbc_tracer_set_diffusivity(h, k, lewis[k]), h, "rbc_tracer_set_diffusivity");
+                rc |= check(rbc_tracers_init_set(h, k, part_type, seed + (unsigned long long)k, part_cx, part_cy, 0.0,
+                                                 part_sigma),
+                            h, "rbc_tracers_init_set");
+            }
+        } else {
             rc |= check(rbc_tracers_seed(h, seed), h, "rbc_tracers_seed");
+        }
     }
     if (rc) {
         rbc_destroy(h);
@@ -224,16 +230,21 @@ int main(int argc, char** argv)
     // tracer outputs: recorded frames since the last dump, the second-moment file
     std::vector<float> frames, ring(write_tracks ? (size_t)256 * 3 * p.n_tracers : 0);
     std::vector<unsigned int> frame_steps, ring_steps(write_tracks ? 256 : 0);
-    char track_desc[512];
-    std::snprintf(track_desc, sizeof track_desc,
-                  "Particle tracks.  Simulation: Ra=%.1lf Pr=%.1lf Size=%.1lfx%.1lfx1.0  Technical: Modes=%dx%dx%d "
-                  "dt=%.3lf  Tracks: Le=%.0le ",
-                  p.ra, p.pr, p.lx, p.ly, p.nx, p.ny, p.nz, p.dt, lewis);
-    FILE* m2 = nullptr;
+    std::vector<FILE*> m2;
     if (moments) {
-        // datapoint_writer's format (output/datapoint_writer.cu:21-45)
-        m2 = std::fopen((out + "/secondmoment_0.dat").c_str(), "w");
-        if (m2) std::fprintf(m2, "# Data point writer\n# Le %.9f\n# Data ordering: t, val\n", lewis);
+        // one datapoint_writer per set (main.cu:521-529, output/datapoint_writer.cu:21-45)
+        for (int k = 0; k < nsets; ++k) {
+            char name[64];
+            std::snprintf(name, sizeof name, "/secondmoment_%d.dat", k);
+            FILE* f = std::fopen((out + name).c_str(), "w");
+            if (!f) {
+                std::fprintf(stderr, "cannot open %s%s\n", out.c_str(), name);
+                rc = 1;
+                break;
+            }
+            std::fprintf(f, "# Data point writer\n# Le %.9f\n# Data ordering: t, val\n", lewis[k]);
+            m2.push_back(f);
+        }
     }
 
     long long done = 0;
@@ -267,10 +278,10 @@ int main(int argc, char** argv)
             frames.insert(frames.end(), ring.begin(), ring.begin() + (size_t)n * 3 * p.n_tracers);
             frame_steps.insert(frame_steps.end(), ring_steps.begin(), ring_steps.begin() + n);
         }
-        if (m2) {
+        for (int k = 0; k < (int)m2.size(); ++k) {
             double mo[4];
-            rc |= check(rbc_tracer_moments(h, mo), h, "rbc_tracer_moments");
-            std::fprintf(m2, "%g\t%g\n", done * p.dt, mo[2]);
+            rc |= check(rbc_tracer_moments_set(h, k, mo), h, "rbc_tracer_moments_set");
+            std::fprintf(m2[k], "%g\t%g\n", done * p.dt, mo[2]);
         }
         if (diag_every > 0 && done % diag_every == 0) {
             rbc_diag d;
@@ -283,16 +294,29 @@ int main(int argc, char** argv)
             std::snprintf(path, sizeof path, "%s/history_%08lld.bin", out.c_str(), done);
             if (do_step) rc |= check(rbc_save_history(h, path), h, "rbc_save_history"); // none without steps
             if (write_tracks && !frame_steps.empty()) {
-                std::snprintf(path, sizeof path, "%s/particles_le%.0le_%08lld.trkss", out.c_str(), lewis, done);
-                rc |= check(rbc_track_write(path, track_desc, frames.data(), frame_steps.data(),
-                                            (int)frame_steps.size(), p.n_tracers),
-                            nullptr, "rbc_track_write");
+                // one track file per set (main.cu:719-725): its columns of every frame
+                const int nf = (int)frame_steps.size(), ns = p.n_tracers / nsets;
+                std::vector<float> part((size_t)nf * 3 * ns);
+                for (int k = 0; k < nsets; ++k) {
+                    for (int fr = 0; fr < nf; ++fr)
+                        for (int d = 0; d < 3; ++d)
+                            std::memcpy(&part[((size_t)fr * 3 + d) * ns],
+                                        &frames[((size_t)fr * 3 + d) * p.n_tracers + (size_t)k * ns], ns * sizeof(float));
+                    char desc[512];
+                    std::snprintf(desc, sizeof desc,
+                                  "Particle tracks.  Simulation: Ra=%.1lf Pr=%.1lf Size=%.1lfx%.1lfx1.0  Technical: "
+                                  "Modes=%dx%dx%d dt=%.3lf  Tracks: Le=%.0le ",
+                                  p.ra, p.pr, p.lx, p.ly, p.nx, p.ny, p.nz, p.dt, lewis[k]);
+                    std::snprintf(path, sizeof path, "%s/particles_le%.0le_%08lld.trkss", out.c_str(), lewis[k], done);
+                    rc |= check(rbc_track_write(path, desc, part.data(), frame_steps.data(), nf, ns), nullptr,
+                                "rbc_track_write");
+                }
                 frames.clear();
                 frame_steps.clear();
             }
         }
     }
-    if (m2) std::fclose(m2);
+    for (FILE* f : m2) std::fclose(f);
     rbc_destroy(h);
     return rc;
 }

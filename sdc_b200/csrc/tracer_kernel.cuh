@@ -25,7 +25,8 @@ struct TracerArgs {
     double* pos;          // [3][n] x, y, z
     int n, nx, ny, L;
     double lx, ly, dt, zmax;
-    double sigma;                     // sqrt(2 D dt) of the diffusion step (0: none)
+    const double* set_sigma;          // [sets] sqrt(2 D dt) of each tracer set (0: no diffusion)
+    int per_set;                      // tracers per set (consecutive ranges)
     unsigned long long noise_seed;
     const long long* step_counter;    // completed fluid steps = step m of the new positions
     float* track;                     // [track_cap][3][n] FP32 frames, or null
@@ -149,11 +150,12 @@ __global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
     z += (dz1 + 2 * (dz2 + dz3) + dz4) / 6.;
     if (!(live && q == 0)) return;
     const long long m = *A.step_counter;
-    if (A.sigma > 0.0) {
+    const double sg = A.set_sigma[t / A.per_set];
+    if (sg > 0.0) {
         // diffuse_particles (particle_tracer.cu:690-716) before the lid reflection
-        x += A.sigma * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 0);
-        y += A.sigma * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 1);
-        z += A.sigma * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 2);
+        x += sg * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 0);
+        y += sg * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 1);
+        z += sg * rbcrng::diffusion_normal(A.noise_seed, m, A.n, t, 2);
     }
     const double zm = A.zmax;
     if (!(z <= zm)) z = (z < 2 * zm) ? 2 * zm - z : zm;  // also sends NaN to the lid
@@ -179,19 +181,20 @@ __global__ void k_track_frame(const double* __restrict__ pos, float* __restrict_
 // Sums for the tracer moments in FP64, one CTA of 1024 threads: thread i sums particles
 // i, i + 1024, ... (and pairs likewise), then a fixed shared-memory tree; deterministic.
 // out[0..3] = sum x, sum y, sum x^2 + y^2, sum over pairs of the squared periodic separation.
-__global__ void __launch_bounds__(1024) k_tracer_sums(const double* __restrict__ pos, int n, double lx, double ly,
-                                                      double* __restrict__ out)
+// n positions of one set starting at pos: x at pos[i], y at pos[stride + i].
+__global__ void __launch_bounds__(1024) k_tracer_sums(const double* __restrict__ pos, int n, int stride, double lx,
+                                                      double ly, double* __restrict__ out)
 {
     __shared__ double red[4][1024];
     double sx = 0, sy = 0, s2 = 0, sp = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const double x = pos[i], y = pos[n + i];
+        const double x = pos[i], y = pos[stride + i];
         sx += x;
         sy += y;
         s2 += x * x + y * y;
     }
     for (int i = 2 * threadIdx.x; i < n - 1; i += 2 * blockDim.x) {
-        double dx = fabs(pos[i + 1] - pos[i]), dy = fabs(pos[n + i + 1] - pos[n + i]);
+        double dx = fabs(pos[i + 1] - pos[i]), dy = fabs(pos[stride + i + 1] - pos[stride + i]);
         if (dx > 0.5 * lx) dx = lx - dx;
         if (dy > 0.5 * ly) dy = ly - dy;
         sp += dx * dx + dy * dy;

@@ -71,8 +71,27 @@ def test_npart_without_le_has_no_tracers(tmp_path):
     assert not any(f.endswith(".trkss") for f in os.listdir(tmp_path))
 
 
-def test_several_lewis_numbers_rejected(tmp_path):
-    exe = os.path.join(os.path.dirname(sdc_b200.LIB_PATH), "rbc_run")
-    r = subprocess.run([exe] + BASE + ["-t", "0.002", "-npart", "64", "-le_count", "2", "-le", "1", "0.1",
-                                       "-dir", str(tmp_path)], capture_output=True, text=True, timeout=120)
-    assert r.returncode == 2 and "one process per -le value" in r.stderr
+def test_several_lewis_numbers_give_one_set_each(tmp_path):
+    """-le_count 2 -le D1 D2: two sets of -npart tracers (one particle_tracer per Lewis
+    number), each with its tracks file and second-moment file."""
+    run(tmp_path, "-t", "0.006", "-npart", "128", "-le_count", "2", "-le", "1e-3", "1e-1",
+        "-write_tracks_every", "1", "-calc_secondmoment")
+    s = sdc_b200.Solver(*CASE, n_tracers=256, tracer_sets=2, track_frames=256, track_period=1)
+    s.init_fields(5, 1e-2, 3.0)
+    for k, D in enumerate((1e-3, 1e-1)):
+        s.tracer_set_diffusivity(k, D)
+        s.tracers_init_set(k, "random", seed=5 + k)
+    m2 = [[], []]
+    for _ in range(6):
+        s.step(1)
+        for k in range(2):
+            m2[k].append(s.tracer_moments_set(k)[2])
+    fr, times = s.tracks_read()
+    for k, tag in enumerate(("1e-03", "1e-01")):
+        trk = oracle.read_trkss(tmp_path / f"particles_le{tag}_{6:08d}.trkss")
+        assert trk["tracks"] == 128
+        assert np.array_equal(trk["frames"], fr[:, :, 128 * k:128 * (k + 1)])
+        lines = open(tmp_path / f"secondmoment_{k}.dat").read().splitlines()
+        data = np.array([[float(v) for v in ln.split("\t")] for ln in lines[3:]])
+        assert np.allclose(data[:, 1], m2[k], rtol=1e-5, atol=0)
+    assert m2[1][-1] > m2[0][-1]  # the more diffusive set spreads faster
