@@ -61,3 +61,35 @@ def test_invalid_params_rejected_before_any_device_work():
     with pytest.raises(sdc_b200.RBCError) as e:
         sdc_b200.Solver(64, 64, 7, 8.0, 8.0, 2000.0, 1.0, 1e-3)
     assert e.value.status == 6
+
+
+@pytest.mark.parametrize("kw", [
+    dict(field_ops=("freeze",), penalization=(-0.5, "rectangle")),  # negative eta
+    dict(penalization=(float("inf"), "circle")),
+    dict(mean_F=float("nan")),
+    dict(n_tracers=100, tracer_sets=3),                              # sets must divide the tracers
+    dict(n_tracers=0, tracer_sets=2),
+    dict(tracer_sets=-1),
+])
+def test_invalid_optional_physics_params_rejected_before_any_device_work(kw):
+    with pytest.raises(sdc_b200.RBCError) as e:
+        sdc_b200.Solver(64, 64, 4, 8.0, 8.0, 2000.0, 1.0, 1e-3, **kw)
+    assert e.value.status == 1
+
+
+def test_params_struct_matches_header_layout():
+    """The ctypes mirror of rbc_params has the header's fields in the header's order."""
+    hdr = open(os.path.join(ROOT, "include", "rbc.h")).read()
+    body = hdr[hdr.index("typedef struct {\n    int nx;"):hdr.index("} rbc_params;")]
+    names = re.findall(r"^\s+(?:unsigned long long|double|int)\s+([\w, ]+);", body, re.M)
+    fields = [n.strip() for group in names for n in group.split(",")]
+    assert fields == [f[0] for f in sdc_b200._Params._fields_]
+
+
+def test_cli_driver_rejects_unknown_penalization_mask(tmp_path):
+    import subprocess
+    exe = os.path.join(os.path.dirname(sdc_b200.LIB_PATH), "rbc_run")
+    r = subprocess.run([exe, "-nmodes", "32", "32", "3", "-clength", "8", "8", "-ra", "3000", "-pr", "1",
+                        "-dt", "1e-3", "-t", "0.001", "-penalized", "hexagon", "-dir", str(tmp_path)],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "hexagon" in r.stderr
