@@ -37,7 +37,7 @@ def _worker(rank, world, port, out):
 def test_two_rank_timing_reduction():
     world = 2
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this (threaded) test process
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
     assert out[0] == out[1]
