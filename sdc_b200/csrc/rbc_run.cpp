@@ -30,6 +30,8 @@
 // Tracers the reference's way (main.cu:150-199, 490-532, 620-660, 719-726):
 //   -npart n -le_count k -le D1 .. Dk   k tracer sets of n tracers, set s with diffusivity
 //                        Ds; as in the reference, no tracers without -le
+//   -multitracer         without -le: the ten diffusivities of the reference's MULTITRACER
+//                        builds (1e1, 3, 1, 0.3, 0.1, 0.03, 0.01, 1e-3, 1e-4, 1e-5; main.cu:201-207)
 //   -part_center | -part_center_sigma | -part_diagonal | -part_pairs |
 //   -part_coord_sigma x y  start patterns (sigma 0.125), -part_sigma s overrides sigma
 //   -write_tracks_every p  record every p-th step; at each state dump the recorded frames
@@ -133,9 +135,14 @@ int main(int argc, char** argv)
     // tracers as main.cu configures them
     const int npart = (int)a.num("-npart", 0);
     std::vector<double> lewis;
-    if (a.has("-le")) {
-        const int le_count = std::max(1, (int)a.num("-le_count", 1));
-        for (int k = 0; k < le_count; ++k) lewis.push_back(a.num("-le", 0.0, k, true));
+    if (a.has("-le") || a.has("-multitracer")) {
+        if (a.has("-le")) {
+            const int le_count = std::max(1, (int)a.num("-le_count", 1));
+            for (int k = 0; k < le_count; ++k) lewis.push_back(a.num("-le", 0.0, k, true));
+        } else {
+            lewis = {1e1, 3e0, 1e0, 3e-1, 1e-1, 3e-2, 1e-2, 1e-3, 1e-4, 1e-5};
+        }
+        const int le_count = (int)lewis.size();
         if (npart > 0) {
             p.n_tracers = npart * le_count;
             p.tracer_sets = le_count;

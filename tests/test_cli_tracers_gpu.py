@@ -95,3 +95,14 @@ def test_several_lewis_numbers_give_one_set_each(tmp_path):
         data = np.array([[float(v) for v in ln.split("\t")] for ln in lines[3:]])
         assert np.allclose(data[:, 1], m2[k], rtol=1e-5, atol=0)
     assert m2[1][-1] > m2[0][-1]  # the more diffusive set spreads faster
+
+
+def test_multitracer_defaults_give_ten_sets(tmp_path):
+    """-multitracer without -le: the ten Lewis numbers of the reference's MULTITRACER builds."""
+    run(tmp_path, "-t", "0.003", "-npart", "64", "-multitracer", "-calc_secondmoment", "-write_tracks_every", "1")
+    les = [1e1, 3e0, 1e0, 3e-1, 1e-1, 3e-2, 1e-2, 1e-3, 1e-4, 1e-5]
+    for k, le in enumerate(les):
+        lines = open(tmp_path / f"secondmoment_{k}.dat").read().splitlines()
+        assert lines[1] == "# Le %.9f" % le and len(lines) == 3 + 3
+        trk = oracle.read_trkss(tmp_path / ("particles_le%.0e_%08d.trkss" % (le, 3)))
+        assert trk["tracks"] == 64
