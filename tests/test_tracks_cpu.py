@@ -81,3 +81,29 @@ def test_trkss_writer_round_trip(tmp_path):
 def test_trkss_writer_rejects_bad_arguments(tmp_path):
     with pytest.raises(sdc_b200.RBCError):
         sdc_b200.track_write(tmp_path / "missing_dir" / "t.trkss", np.zeros((1, 3, 2), np.float32), [0])
+
+
+def test_oracle_tracer_sets_pinned_by_uniform_runs():
+    """Sets [D, 0]: the first half moves exactly as with D for every tracer, the second half
+    exactly as without diffusion (the noise is indexed by the global tracer number, and the
+    tracers do not act on the flow)."""
+    from tests.helpers import random_state
+    case = (32, 32, 2, 8.0, 8.0, 3000.0, 1.0, 1e-3)
+    nx, ny, L = case[:3]
+    n = 256
+    st = random_state(nx, ny, L, seed=81, amp=0.05)
+    xyz = oracle.tracer_positions(6, n, case[3], case[4])
+    runs = {}
+    for name, D, sets in (("sets", 0.0, [1e-3, 0.0]), ("all", 1e-3, None), ("none", 0.0, None)):
+        o = oracle.Oracle(*case, threads=2)
+        o.set_state(*st)
+        o.set_diffusion(D, 13)
+        if sets is not None:
+            o.set_tracer_sets(sets)
+        o.tracers_set(xyz)
+        o.step(6)
+        runs[name] = o.tracers_get().reshape(3, n)
+    h = n // 2
+    assert np.array_equal(runs["sets"][:, :h], runs["all"][:, :h])
+    assert np.array_equal(runs["sets"][:, h:], runs["none"][:, h:])
+    assert not np.array_equal(runs["all"][:, h:], runs["none"][:, h:])
