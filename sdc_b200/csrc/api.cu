@@ -143,6 +143,7 @@ struct rbc_handle {
     cudaStream_t graph_chain_stream = nullptr;
     int graph_chain_launches = 0;
     bool chain_tracers = false;   // while capturing that graph
+    bool k1_dep = false;          // K1 follows the previous step's update inside such a graph
     // programmatic dependent launches off: set for ensemble members, whose steps run as
     // concurrent graph branches (CTAs waiting at griddepcontrol.wait would hold SM
     // resources the other branches can use)
@@ -454,9 +455,17 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     StageScope sc(h, ST_SYNTH);
     const size_t sm = smem_cols<R>(h, 8);
     switch (rx_y(h)) {
-    case 16: k_synth_columns_tp<R, 16><<<g1, 8 * h->W * 16, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H); break;
-    case 8: k_synth_columns_tp<R, 8><<<g1, 8 * h->W * 8, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H); break;
-    default: k_synth_columns<R><<<g1, kThreads, sm, h->stream>>>(G, h->W, h->py, h->twy, th, f, g, FG, (C*)h->H);
+    case 16:
+        if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, 16>, g1, dim3(8 * h->W * 16), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
+        else k_synth_columns_tp<R, 16><<<g1, 8 * h->W * 16, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H);
+        break;
+    case 8:
+        if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, 8>, g1, dim3(8 * h->W * 8), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
+        else k_synth_columns_tp<R, 8><<<g1, 8 * h->W * 8, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H);
+        break;
+    default:
+        if (h->k1_dep) launch_dep(h, k_synth_columns<R>, g1, dim3(kThreads), sm, G, h->W, h->py, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
+        else k_synth_columns<R><<<g1, kThreads, sm, h->stream>>>(G, h->W, h->py, h->twy, th, f, g, FG, (C*)h->H);
     }
     RBC_CUDA(cudaGetLastError());
     }
@@ -1357,12 +1366,15 @@ static void capture_chain(rbc_handle* h)
         for (int i = 0; i < kChainSteps; ++i) {
             h->have_hist = true;
             h->tracer_pending = true;
+            h->k1_dep = i > 0; // after the previous step's update, which wrote the state
             if (h->mixed) run_step<float>(h);
             else run_step<double>(h);
         }
+        h->k1_dep = false;
         join_tracer(h); // the last advance
     } catch (...) {
         h->chain_tracers = false;
+        h->k1_dep = false;
         h->join_pending = false;
         cudaStreamEndCapture(h->stream, &g);
         if (g) cudaGraphDestroy(g);

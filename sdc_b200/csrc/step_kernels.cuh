@@ -97,7 +97,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns(
     const int k = blockIdx.y;
     const int c0 = blockIdx.x * W;
     const int st = py.stride;
+    pdl_trigger();
     load_twiddles<R>(tw, twy, G.ny);
+    pdl_wait(); // the state is complete (K1 is a dependent launch inside multi-step graphs)
     const size_t base = ((size_t)k * G.ckp + c0) * G.ny;
     constexpr bool kStage = sizeof(C) == sizeof(double2);
     if constexpr (kStage) {
@@ -358,6 +360,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
     const int k = blockIdx.y;
     const int c0 = blockIdx.x * W;
     const size_t base = ((size_t)k * G.ckp + c0) * N;
+    pdl_trigger();
+    load_twiddles_async<R>(tw, twy, N);
+    pdl_wait(); // the state is complete (K1 is a dependent launch inside multi-step graphs)
     for (int e = threadIdx.x; e < W * N; e += blockDim.x) {
         const int cc = e / N, r = e - cc * N;
         if (c0 + cc < G.ckeep && row_kept(r, N)) {
@@ -366,7 +371,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
             cp_async<16>(stg + 2 * W * N + e, g + base + e);
         }
     }
-    load_twiddles<R>(tw, twy, N);
     cp_async_wait_all();
     __syncthreads();
     const int q = threadIdx.x / RX, t = threadIdx.x - q * RX;
