@@ -43,6 +43,7 @@
 #include "rbc.h"
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <initializer_list>
 #include <cstdio>
@@ -64,10 +65,16 @@ struct Args {
         return -1;
     }
     bool has(const char* name) const { return find(name) >= 0; }
+    // the k-th value after option `name`; an option name ends the values (a negative number
+    // such as -0.5 is a value)
+    static bool is_option(const char* s) { return s[0] == '-' && std::isalpha((unsigned char)s[1]); }
     const char* str(const char* name, int k = 0) const
     {
         const int i = find(name);
-        return (i >= 0 && i + 1 + k < argc) ? argv[i + 1 + k] : nullptr;
+        if (i < 0 || i + 1 + k >= argc) return nullptr;
+        for (int j = i + 1; j <= i + 1 + k; ++j)
+            if (is_option(argv[j])) return nullptr;
+        return argv[i + 1 + k];
     }
     double num(const char* name, double def, int k = 0, bool mandatory = false) const
     {

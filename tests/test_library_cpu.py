@@ -93,3 +93,14 @@ def test_cli_driver_rejects_unknown_penalization_mask(tmp_path):
                         "-dt", "1e-3", "-t", "0.001", "-penalized", "hexagon", "-dir", str(tmp_path)],
                        capture_output=True, text=True, timeout=60)
     assert r.returncode == 2 and "hexagon" in r.stderr
+
+
+def test_cli_driver_usage_and_le_count_mismatch(tmp_path):
+    import subprocess
+    exe = os.path.join(os.path.dirname(sdc_b200.LIB_PATH), "rbc_run")
+    r = subprocess.run([exe, "-h"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "usage" in r.stdout
+    r = subprocess.run([exe, "-nmodes", "32", "32", "3", "-clength", "8", "8", "-ra", "3000", "-pr", "1",
+                        "-dt", "1e-3", "-t", "0.001", "-npart", "16", "-le_count", "3", "-le", "1", "0.1",
+                        "-dir", str(tmp_path)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "-le" in r.stderr
