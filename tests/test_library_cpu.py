@@ -104,3 +104,19 @@ def test_cli_driver_usage_and_le_count_mismatch(tmp_path):
                         "-dt", "1e-3", "-t", "0.001", "-npart", "16", "-le_count", "3", "-le", "1", "0.1",
                         "-dir", str(tmp_path)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 2 and "-le" in r.stderr
+
+
+def test_header_is_plain_c99_and_links(tmp_path):
+    """include/rbc.h compiles as C99 and every declared function links against the library
+    with C linkage (the program is built, not run)."""
+    import subprocess
+    names = declared_functions()
+    src = tmp_path / "use.c"
+    src.write_text('#include "rbc.h"\ntypedef void (*fn)(void);\nint main(void) {\n    volatile fn t[] = {\n' +
+                   "".join(f"        (fn)&{n},\n" for n in names) + "    };\n    return t[0] == 0;\n}\n")
+    lib_dir = os.path.dirname(sdc_b200.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        str(src), "-L", lib_dir, "-lsdc_b200", "-o", str(tmp_path / "use")],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert len(names) == len(sdc_b200.EXPORTS)
