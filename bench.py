@@ -26,6 +26,9 @@ METRIC = "Sim-time/s per GPU: mixed/batched/surrogate vs plain FP64 at ≤1e-3 N
 WORK = dict(nx=256, ny=256, nz=8, lx=32.0, ly=32.0, ra=5000.0, pr=0.9, dt=5e-4)
 NTRACERS = 65536
 SEED = 2
+# the workload string both arms print (the same workload, so the lines are comparable)
+WORKLOAD = ("plain FP64 RBC step 256x256x8, Lx=Ly=32, Ra=5000, Pr=0.9, dt=5e-4, Nz=8 Galerkin modes, "
+            "+65536 tracers, 1000-2000-step run length sampled by the timed steps")
 
 
 def bytes_alg(nx, ny, L, ntr):
@@ -188,8 +191,7 @@ def run_reference(args, rank):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 / cb["steps_per_s"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "plain FP64 RBC step 256x256x8, Lx=Ly=32, Ra=5000, Pr=0.9, dt=5e-4, "
-                                   "+65536 tracers", "impl": "oracle port of the reference method"},
+            "config": {"workload": WORKLOAD, "form": "fp64", "impl": "oracle port of the reference method"},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "sim-time/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -661,14 +663,29 @@ def main():
         # FMA throughput measured on this device (no FP64 figure in the measured peaks)
         flops = 2.0 * contract_fmas_per_point(L) * nx * ny
         fp64_peak = sdc_b200.fp64_peak_tflops(local)
-        roof["fp64"] = {"achieved": flops / (stages[dom][0] * 1e-3) / 1e12, "peak": fp64_peak,
-                        "unit": "TFLOP/s", "frac": flops / (stages[dom][0] * 1e-3) / 1e12 / fp64_peak,
-                        "flops_per_launch": flops, "peak_source": "measured on this device (FMA loop)"}
+        hbm = {k: roof.pop(k) for k in ("achieved", "peak", "unit", "frac", "peak_source")}
+        tf = flops / (stages[dom][0] * 1e-3) / 1e12
+        roof.update({"bound": "fp64", "achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": tf / fp64_peak, "flops_per_launch": flops,
+                     "peak_source": "measured on this device (FP64 FMA loop; no FP64 figure in the measured peaks)",
+                     "hbm": hbm})
     step_b, tr_b = bytes_alg(nx, ny, L, NTRACERS)
 
-    # ---- end to end through the C ABI with host buffers
-    host_state = s.get_state()
-    host_tr = s.tracers_get()
+    # ---- end to end through the C ABI with host buffers (pinned, as a caller that streams
+    # states in and out would hold them)
+    pins = []
+
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        pins.append(t)
+        v = t.numpy().view(a.dtype).reshape(a.shape)
+        v[...] = a
+        return v
+
+    host_state = [pinned(a) for a in s.get_state()]
+    host_tr = pinned(s.tracers_get())
+    out_state = [pinned(a) for a in host_state]
+    out_tr = pinned(host_tr)
     barrier()
     t0 = time.perf_counter()
     s.set_state(*host_state)
@@ -682,14 +699,15 @@ def main():
             s.diagnostics_get(prev)  # waits for that step only; reports a non-finite state
         prev = t
     s.diagnostics_get(prev)
-    out_state = s.get_state()
-    out_tr = s.tracers_get()
+    s.get_state(out_state)
+    s.tracers_get(out_tr)
     el = max_over_ranks(time.perf_counter() - t0, world, device="cuda")
     state_bytes = sum(a.nbytes for a in host_state)
     tr_bytes = host_tr.nbytes
     e2e = {"value": world * args.steps * WORK["dt"] / el, "unit": "sim-time/s",
            "h2d_bytes_per_step": (state_bytes + tr_bytes) / args.steps,
            "d2h_bytes_per_step": 36 + (state_bytes + tr_bytes) / args.steps,
+           "host_buffers": "pinned (cudaHostAlloc through torch)",
            "includes": "set_state + tracers_set, K x (rbc_step_async(1) + rbc_diagnostics_async, then "
                        "rbc_diagnostics_get of the step before), get_state + tracers_get"}
     d = s.diagnostics()
@@ -719,8 +737,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "steps_per_s": 1000.0 * args.steps / ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64", "data": "synthetic",
-                "config": {"workload": f"plain {args.form.upper()} RBC step 256x256x8, Lx=Ly=32, Ra=5000, "
-                                       f"Pr=0.9, dt=5e-4, +65536 tracers (RK4, 128 z levels)",
+                "config": {"workload": WORKLOAD if args.form == "fp64" else WORKLOAD.replace("FP64", "MIXED"),
                            "form": args.form, "parallelism": f"replicas x{world}",
                            "launch": {"autotuned": bool(args.tune), "column_block": W, "row_pairs": NP},
                            "l2": "working set > 126 MB L2 (state, history, scratch ~300 MB); no flush",

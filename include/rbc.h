@@ -332,21 +332,26 @@ rbc_status rbc_stage_times(rbc_handle* h, int nsteps, double* ms, int* counts);
  * contraction; no reference counterpart). */
 rbc_status rbc_measure_fp64_peak(int device, double* tflops);
 /* --- nonlinear operator without device allocation ----------------------------- */
-/* No counterpart in the reference. For callers that cannot call cudaMalloc (code that
- * runs inside another framework's memory pool, or that must not change the device's
- * allocation state, e.g. while it is captured or checkpointed): the same operator as
- * rbc_nonlinear, without a handle, on DEVICE buffers in the reference layout (inputs
- * theta, f, g [nz][ny][nx/2+1] and F, G [nz] complex; the five outputs alike). It calls
- * no cudaMalloc, cudaFree or allocating library routine: all scratch lives in one
- * file-scope __device__ array of RBC_NOALLOC_SCRATCH_BYTES, which every GPU that loads
- * this library holds until the process exits. Limits: nx, ny <= 64 (2^a 3^b, even),
- * 2 <= nz <= 4; larger sizes return RBC_ERR_INVALID_ARG with the reason in errbuf (may be
- * NULL). The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call before any
- * stream capture. Every call shares the array and leaves its contents behind (each call
- * rewrites all it reads): calls that overlap on the GPU -- on different streams, or from
- * several host threads -- race and must be serialised by the caller. Work is enqueued on
- * `stream` (cudaStream_t, NULL = legacy default stream) and not waited for. */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc: a plug-in
+ * inside a host framework that has already reserved the device's memory for its own
+ * caching allocator (a new cudaMalloc there fails or fragments that pool), or a
+ * latency-critical loop that must not pay the implicit device-wide synchronisation of
+ * cudaMalloc/cudaFree. The same operator as rbc_nonlinear, without a handle, on DEVICE
+ * buffers in the reference layout (inputs theta, f, g [nz][ny][nx/2+1] and F, G [nz]
+ * complex; the five outputs alike). It calls no cudaMalloc, cudaFree or allocating
+ * library routine: all scratch and tables live in one file-scope __device__ array of
+ * RBC_NOALLOC_SCRATCH_BYTES, which every GPU that loads this library holds until the
+ * process exits. Limits: nx, ny <= 64 (2^a 3^b, even), 2 <= nz <= 4; larger sizes return
+ * RBC_ERR_INVALID_ARG with the reason in errbuf (may be NULL). Set-up happens inside the
+ * calls: the first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current), and the first call of a grid size
+ * (nx, ny, nz) on a device, or the first after a call of another size, copies that size's
+ * twiddle and coefficient tables into the array from host memory. Make the first call
+ * before any stream capture. Every call shares the array and leaves its contents behind
+ * (each call rewrites the scratch it reads): calls that overlap on the GPU -- on different
+ * streams, or from several host threads -- race and must be serialised by the caller.
+ * Work is enqueued on `stream` (cudaStream_t, NULL = legacy default stream) and not
+ * waited for; the caller's current device is restored before the call returns. */
 #define RBC_NOALLOC_MAX_NX 64
 #define RBC_NOALLOC_MAX_NY 64
 #define RBC_NOALLOC_MAX_NZ 4

@@ -358,8 +358,10 @@ class Solver:
         a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (theta, f, g, F, G)]
         self._check(lib().rbc_set_state(self.h, *[_p(x) for x in a]))
 
-    def get_state(self):
-        b = self._bufs()
+    def get_state(self, out=None):
+        """The state in the reference layout; `out` (five C-contiguous complex128 arrays of
+        the state's shapes, e.g. views of pinned host memory) is filled and returned."""
+        b = self._bufs() if out is None else out
         self._check(lib().rbc_get_state(self.h, *[_p(x) for x in b]))
         return b
 
@@ -421,8 +423,8 @@ class Solver:
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         self._check(lib().rbc_tracers_set(self.h, _p(xyz), xyz.size // 3))
 
-    def tracers_get(self):
-        out = np.zeros(3 * self.n_tracers)
+    def tracers_get(self, out=None):
+        out = np.zeros(3 * self.n_tracers) if out is None else out
         self._check(lib().rbc_tracers_get(self.h, _p(out), self.n_tracers))
         return out
 

@@ -1240,7 +1240,6 @@ static void download_field(rbc_handle* h, const double2* src, double* dst, int n
     k_cm_to_ref<<<512, 256, 0, h->stream>>>(src, h->stage, h->G, nmat);
     RBC_CUDA(cudaGetLastError());
     RBC_CUDA(cudaMemcpyAsync(dst, h->stage, n * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
-    RBC_CUDA(cudaStreamSynchronize(h->stream));
 }
 
 rbc_status rbc_set_state(rbc_handle* h, const double* th, const double* f, const double* g, const double* F, const double* G)
@@ -1357,6 +1356,7 @@ static void capture_chain(rbc_handle* h)
         cudaGraphExecDestroy(h->graph_chain);
         h->graph_chain = nullptr;
     }
+    const bool hist = h->have_hist, pend = h->tracer_pending;
     const long long launches = h->launches, hs = h->host_steps;
     cudaGraph_t g = nullptr;
     RBC_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -1387,10 +1387,23 @@ static void capture_chain(rbc_handle* h)
     cudaGraphDestroy(g);
     RBC_CUDA(e);
     h->graph_chain_stream = h->stream;
-    h->have_hist = true;
-    h->tracer_pending = true;
+    h->have_hist = hist;
+    h->tracer_pending = pend;
     h->launches = launches;
     h->host_steps = hs;
+}
+
+// Instantiates every steady-step graph a run on the current stream can replay (the
+// single step with and without a pending tracer advance, and the kChainSteps chain when
+// tracers are on) the first time any of them is needed, so that a later call replays
+// graphs only and never captures and instantiates in the middle of a run of steps.
+static void prepare_graphs(rbc_handle* h)
+{
+    if (h->ntr > 0) {
+        if (!h->graph[1] || h->graph_stream[1] != h->stream) capture_step(h, 1);
+        if (!h->graph_chain || h->graph_chain_stream != h->stream) capture_chain(h);
+    }
+    if (!h->graph[0] || h->graph_stream[0] != h->stream) capture_step(h, 0);
 }
 
 rbc_status rbc_step_async(rbc_handle* h, int nsteps)
@@ -1402,6 +1415,7 @@ rbc_status rbc_step_async(rbc_handle* h, int nsteps)
     for (int s = 0; s < nsteps; ++s) {
         // graphs need a real stream (the legacy default stream cannot be captured)
         if (h->use_graphs && h->have_hist && !h->profiling && h->stream != nullptr) {
+            prepare_graphs(h);
             if (h->tracer_pending && h->ntr > 0 && nsteps - s >= kChainSteps) {
                 if (!h->graph_chain || h->graph_chain_stream != h->stream) capture_chain(h);
                 RBC_CUDA(cudaGraphLaunch(h->graph_chain, h->stream));

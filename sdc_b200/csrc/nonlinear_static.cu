@@ -1,14 +1,15 @@
 // nonlinear_static.cu -- the nonlinear operator for callers that cannot allocate device
 // memory.
 //
-// Some callers cannot call cudaMalloc at all: code that runs inside another framework's
-// memory pool or arena, or a host program that must not change the device's allocation
-// state while it is being captured or checkpointed. rbc_nonlinear_noalloc gives them the
-// nonlinear operator without a handle and without any device allocation: the caller
-// passes device buffers for the input state and the five results, and every scratch
-// plane the kernels need lives in one file-scope __device__ array of fixed size
-// (RBC_NOALLOC_SCRATCH_BYTES), which every GPU that loads this library keeps until the
-// process exits.
+// Some callers cannot call cudaMalloc: a plug-in running inside a host framework that has
+// already reserved the device's memory for its own caching allocator (a new cudaMalloc
+// there fails or fragments that pool), or a latency-critical loop that must not pay the
+// implicit device-wide synchronisation of cudaMalloc and cudaFree. rbc_nonlinear_noalloc
+// gives them the nonlinear operator without a handle and without any device allocation:
+// the caller passes device buffers for the input state and the five results, and every
+// scratch plane and table the kernels need lives in one file-scope __device__ array of
+// fixed size (RBC_NOALLOC_SCRATCH_BYTES), which every GPU that loads this library keeps
+// until the process exits.
 //
 // The kernels are the same as those of rbc_nonlinear (step_kernels.cuh,
 // contract_kernel.cuh); only the placement of their scratch differs.
@@ -35,6 +36,17 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[RBC_NOALLOC_SCRATCH_BY
 
 std::mutex g_mu;
 void* g_addr[64] = {nullptr}; // device address of g_noalloc_scratch, per device ordinal
+
+// The size whose tables (twiddles, contraction coefficients) sit at the start of the
+// array on each device: a call of the same size finds them there and enqueues kernels
+// only; a call of another size rewrites them (its scratch planes may overlap the old
+// tables' place). The host copies are kept for the life of the process.
+struct TableKey {
+    int nx = 0, ny = 0, nz = 0;
+};
+TableKey g_tables[64];
+std::vector<double> g_coef[64];
+std::vector<double2> g_twx[64], g_twy[64];
 
 // Device address of the scratch array on `device` (which must be current). Looked up
 // once per device and cached.
@@ -114,6 +126,14 @@ __global__ void k_na_fg(const double* __restrict__ nfg, double2* __restrict__ F,
     }
 }
 
+struct DeviceRestore {
+    int dev = -1;
+    ~DeviceRestore()
+    {
+        if (dev >= 0) cudaSetDevice(dev);
+    }
+};
+
 void say(char* buf, int len, const char* msg)
 {
     if (buf && len > 0) {
@@ -152,10 +172,18 @@ extern "C" rbc_status rbc_nonlinear_noalloc(int device, int nx, int ny, int nz, 
         say(errbuf, errlen, "rbc_nonlinear_noalloc: invalid grid or parameters");
         return RBC_ERR_INVALID_ARG;
     }
-    if (cudaSetDevice(device) != cudaSuccess) {
+    if (device < 0 || device >= 64) {
+        say(errbuf, errlen, "rbc_nonlinear_noalloc: device ordinal out of range");
+        return RBC_ERR_INVALID_ARG;
+    }
+    // the caller's current device is restored on every return path
+    DeviceRestore restore;
+    if (cudaGetDevice(&restore.dev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
         say(errbuf, errlen, "rbc_nonlinear_noalloc: cudaSetDevice failed");
         return RBC_ERR_CUDA;
     }
+    // an error left pending by earlier, unrelated work is not this call's failure
+    (void)cudaGetLastError();
     void* base = nullptr;
     cudaError_t e = scratch_address(device, &base);
     if (e != cudaSuccess) {
@@ -184,26 +212,42 @@ extern "C" rbc_status rbc_nonlinear_noalloc(int device, int nx, int ny, int nz, 
         return RBC_ERR_INVALID_ARG;
     }
     unsigned char* b = static_cast<unsigned char*>(base);
-    // tables for this call (host computation; the previous call may have used another size)
-    rbchost::Tables T;
-    rbchost::build_tables(nz, T);
-    std::vector<double> coef;
-    rbchost::pack_contraction(T, coef);
-    std::vector<double2> twx(nx), twy(ny);
-    for (int t = 0; t < nx; ++t) {
-        const long double a = -2.0L * 3.14159265358979323846264338327950288L * t / nx;
-        twx[t] = make_double2((double)cosl(a), (double)sinl(a));
-    }
-    for (int t = 0; t < ny; ++t) {
-        const long double a = -2.0L * 3.14159265358979323846264338327950288L * t / ny;
-        twy[t] = make_double2((double)cosl(a), (double)sinl(a));
-    }
-    e = cudaMemcpyAsync(b + l.twx, twx.data(), sizeof(double2) * nx, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b + l.twy, twy.data(), sizeof(double2) * ny, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b + l.coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) {
-        say(errbuf, errlen, cudaGetErrorString(e));
-        return RBC_ERR_CUDA;
+    {
+        // tables: uploaded when this device's array holds another size's (host computation
+        // into process-lifetime buffers)
+        std::lock_guard<std::mutex> lock(g_mu);
+        TableKey& key = g_tables[device];
+        if (key.nx != nx || key.ny != ny || key.nz != nz) {
+            rbchost::Tables T;
+            rbchost::build_tables(nz, T);
+            std::vector<double>& coef = g_coef[device];
+            rbchost::pack_contraction(T, coef);
+            std::vector<double2>& twx = g_twx[device];
+            std::vector<double2>& twy = g_twy[device];
+            twx.resize(nx);
+            twy.resize(ny);
+            for (int t = 0; t < nx; ++t) {
+                const long double a = -2.0L * 3.14159265358979323846264338327950288L * t / nx;
+                twx[t] = make_double2((double)cosl(a), (double)sinl(a));
+            }
+            for (int t = 0; t < ny; ++t) {
+                const long double a = -2.0L * 3.14159265358979323846264338327950288L * t / ny;
+                twy[t] = make_double2((double)cosl(a), (double)sinl(a));
+            }
+            e = cudaMemcpyAsync(b + l.twx, twx.data(), sizeof(double2) * nx, cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(b + l.twy, twy.data(), sizeof(double2) * ny, cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(b + l.coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) {
+                key = TableKey{};
+                say(errbuf, errlen, cudaGetErrorString(e));
+                return RBC_ERR_CUDA;
+            }
+            key.nx = nx;
+            key.ny = ny;
+            key.nz = nz;
+        }
     }
     double2* st = reinterpret_cast<double2*>(b + l.st);
     const size_t plane = (size_t)G.ckp * ny;
@@ -212,6 +256,11 @@ extern "C" rbc_status rbc_nonlinear_noalloc(int device, int nx, int ny, int nz, 
     k_na_ref_to_cm<<<256, 256, 0, s>>>(reinterpret_cast<const double2*>(theta), st, G, nz);
     k_na_ref_to_cm<<<256, 256, 0, s>>>(reinterpret_cast<const double2*>(f), st + plane * nz, G, nz);
     k_na_ref_to_cm<<<256, 256, 0, s>>>(reinterpret_cast<const double2*>(g), st + 2 * plane * nz, G, nz);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        say(errbuf, errlen, cudaGetErrorString(e));
+        return RBC_ERR_CUDA;
+    }
     e = cudaMemcpyAsync(FG, F, sizeof(double2) * nz, cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(FG + nz, Gm, sizeof(double2) * nz, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) {

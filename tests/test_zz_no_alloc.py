@@ -23,27 +23,33 @@ def _device_copy(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128).view(np.float64).copy()).cuda()
 
 
-def call_noalloc(case, state):
+def call_noalloc(case, state, use_stream=False):
     """Runs the no-allocation operator on device copies of `state` (torch owns the
-    input and output buffers; the entry point itself allocates nothing)."""
+    input and output buffers; the entry point itself allocates nothing). With
+    use_stream the work goes to a torch side stream, which is then waited for."""
     import torch
     nx, ny, L, lx, ly, ra, pr, dt = case
     ins = [_device_copy(torch, a) for a in state]
     outs = [torch.zeros_like(t) for t in ins]
     err = ctypes.create_string_buffer(256)
     ptrs = [ctypes.c_void_p(t.data_ptr()) for t in ins + outs]
-    st = sdc_b200.lib().rbc_nonlinear_noalloc(0, nx, ny, L, lx, ly, pr, *ptrs, None, err, 256)
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream() if use_stream else None
+    handle = ctypes.c_void_p(stream.cuda_stream) if use_stream else None
+    st = sdc_b200.lib().rbc_nonlinear_noalloc(0, nx, ny, L, lx, ly, pr, *ptrs, handle, err, 256)
+    if use_stream:
+        stream.synchronize()
     torch.cuda.synchronize()
     shapes = [a.shape for a in state]
     res = [o.cpu().numpy().view(np.complex128).reshape(s) for o, s in zip(outs, shapes)]
     return st, res, err.value.decode()
 
 
-def check_against_regular(case, seed):
+def check_against_regular(case, seed, use_stream=False):
     nx, ny, L = case[:3]
     state = random_state(nx, ny, L, seed=seed, amp=1.0)
     ref = sdc_b200.Solver(*case).nonlinear(*state)
-    st, got, msg = call_noalloc(case, state)
+    st, got, msg = call_noalloc(case, state, use_stream)
     assert st == 0, msg
     for name, a, b in zip(("theta", "f", "g", "F", "G"), got, ref):
         assert rel_err(a, b) < 1e-12, (name, rel_err(a, b))
@@ -56,6 +62,13 @@ def test_noalloc_matches_regular_operator_on_consecutive_calls():
     check_against_regular(c1, seed=4)   # same size again: no stale scratch is used
     check_against_regular(c2, seed=5)   # another size and L over the same scratch
     check_against_regular(c1, seed=6)
+
+
+def test_noalloc_two_modes_and_a_side_stream():
+    c = (48, 32, 2, 12.0, 8.0, 2000.0, 1.3, 1e-3)
+    check_against_regular(c, seed=7, use_stream=True)
+    check_against_regular(c, seed=8, use_stream=True)   # tables of this size already in place
+    check_against_regular((64, 64, 4, 8.0, 8.0, 2000.0, 1.0, 1e-3), seed=9, use_stream=True)
 
 
 def test_noalloc_rejects_sizes_beyond_the_static_limit():
