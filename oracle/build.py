@@ -1,7 +1,8 @@
 """Builds the CPU oracle (test infrastructure) into oracle/_build/liboracle.so.
 
-Also builds oracle/_ref/libref_coeff.so from the reference's own coeff.cu when the
-reference sources are present (see build_ref.sh). Neither library is product code.
+Also builds, when the reference sources are present, oracle/_ref/libref_coeff.so from the
+reference's own coeff.cu (build_ref.sh) and oracle/_ref/ref_step, the reference's own FP64
+step (build_ref_step.sh). None of these is product code.
 """
 import os
 import subprocess
@@ -20,11 +21,22 @@ def build(force=False, verbose=False):
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)
-    ref_script = os.path.join(HERE, "build_ref.sh")
-    ref_out = os.path.join(HERE, "_ref", "libref_coeff.so")
-    if os.path.exists(ref_script) and (force or not os.path.exists(ref_out)):
-        subprocess.call(["sh", ref_script])
+    root = reference_root()
+    if root:
+        for script, out in (("build_ref.sh", "libref_coeff.so"), ("build_ref_step.sh", "ref_step")):
+            if force or not os.path.exists(os.path.join(HERE, "_ref", out)):
+                subprocess.call(["sh", os.path.join(HERE, script), root])
     return OUT
+
+
+def reference_root():
+    """The reference project's root for the checker builds in oracle/_ref: SDC_REFERENCE,
+    else the reference's usual read-only mount when present (None where there is no copy
+    of the reference: the prebuilt files are used there)."""
+    for r in (os.environ.get("SDC_REFERENCE"), "/root/reference"):
+        if r and os.path.isdir(os.path.join(r, "gpu_flow", "code")):
+            return r
+    return None
 
 
 if __name__ == "__main__":

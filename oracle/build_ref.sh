@@ -4,9 +4,11 @@
 # Test infrastructure only: used to pin the oracle's and the library's tables.
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${SDC_REFERENCE:-/root/reference}/gpu_flow/code/util
-if [ ! -f "$REF/coeff.cu" ]; then
-    echo "reference sources not present; skipping oracle/_ref" >&2
+# usage: sh oracle/build_ref.sh <reference root>   (or SDC_REFERENCE=<root>)
+ROOT=${1:-$SDC_REFERENCE}
+REF="$ROOT/gpu_flow/code/util"
+if [ -z "$ROOT" ] || [ ! -f "$REF/coeff.cu" ]; then
+    echo "reference sources not given or not present; skipping oracle/_ref" >&2
     exit 0
 fi
 mkdir -p "$HERE/_ref"

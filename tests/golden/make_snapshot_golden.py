@@ -1,8 +1,8 @@
 """Generates tests/golden/snapshot_00030000.npz from the reference's own FP32 state
 snapshots (gpu_flow/data/{theta,f,g,F,G}_00030000.bin, written by
 matrix_folder_writer::write_binary_file, gpu_flow/code/output/matrix_folder_writer.cu:3-101).
-Run in a container where the reference exists:
-    python tests/golden/make_snapshot_golden.py [reference root]
+Run where the reference exists:
+    python tests/golden/make_snapshot_golden.py <reference root>
 The fixture keeps, per file, the header words, the file size and its SHA-256, and for
 theta the complete kx = 0 column of both vertical planes (raw FP32 pairs), which is
 enough to rebuild a file of the same header and size and to check the Hermitian
@@ -19,7 +19,9 @@ NAMES = ["theta", "f", "g", "F", "G"]
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_snapshot_golden.py <reference root>")
+    root = sys.argv[1]
     data = os.path.join(root, "gpu_flow", "data")
     out = {}
     for n in NAMES:
