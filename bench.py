@@ -236,6 +236,55 @@ def mixed_form(s64, stream, args, local, world):
             "fp64_nu_wall": d64["nu_wall"], "nu_err_le_1e-3": bool(err["nu_wall"] <= 1e-3)}
 
 
+SDC = dict(nx=512, ny=512, nz=12, lx=64.0, ly=64.0, ra=6000.0, pr=1.0, dt=2.5e-4)
+# the surrogate's spectrum judge: relative L2 error of the z = 0 theta spectrum over 32
+# shells, against the plain step's, above which the plain step takes over
+SPEC_TOL = 0.05
+
+
+def mixed_sdc_form(stream, local, steps=4000):
+    """The mixed-precision configuration: 512 x 512 grid, Lx = Ly = 64, Nz = 12, Ra = 6000,
+    Pr = 1, dt = 2.5e-4, 4000 steps from the seeded perturbation (seed 3, |k| <= 8). The
+    mixed form (FP32 synthesis, products and transforms; FP64 implicit solve, mean flow and
+    reductions) and the FP64 form run the same steps from the same state; reported: both
+    forms' sim-time/s (CUDA events) and the error of Nu (wall and volume), kinetic energy
+    and the radial spectrum of theta at z = 0 against the FP64 run."""
+    import numpy as np
+    import torch
+    import sdc_b200
+    res = {}
+    diag = {}
+    for form in ("fp64", "mixed"):
+        s = sdc_b200.Solver(**SDC, form=form, device=local, tune=True)
+        s.set_stream(stream.cuda_stream)
+        s.init_fields(3, 1e-3, 8.0)
+        s.step(3)
+        s.init_fields(3, 1e-3, 8.0)  # warm-up steps discarded: both forms start from the seed
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step_async(steps)
+        e1.record(stream)
+        s.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[form] = {"sim_time_per_s": steps * SDC["dt"] / (ms * 1e-3), "ms_per_step": ms / steps}
+        d = s.diagnostics()
+        diag[form] = (d, s.spectrum(64, 0.0))
+        s.close()
+    (d64, sp64), (dm, spm) = diag["fp64"], diag["mixed"]
+    err = {k: abs(dm[k] - d64[k]) / abs(d64[k]) for k in ("nu_wall", "nu_vol", "ke")}
+    err["spectrum_rel_l2"] = float(np.linalg.norm(spm - sp64) / np.linalg.norm(sp64))
+    return {"config": "512x512x12, Lx=Ly=64, Ra=6000, Pr=1, dt=2.5e-4, %d steps, seed 3 |k|<=8" % steps,
+            "value": res["mixed"]["sim_time_per_s"], "unit": "sim-time/s",
+            "fp64_value": res["fp64"]["sim_time_per_s"],
+            "speedup_vs_fp64": res["mixed"]["sim_time_per_s"] / res["fp64"]["sim_time_per_s"],
+            "ms_per_step": res["mixed"]["ms_per_step"], "fp64_ms_per_step": res["fp64"]["ms_per_step"],
+            "rel_err_vs_fp64": err, "fp64_nu_wall": d64["nu_wall"], "fp64_ke": d64["ke"],
+            "nu_err_le_1e-3": bool(err["nu_wall"] <= 1e-3),
+            "dtype": "f32 synthesis/products/FFTs + f64 implicit solve, mean flow, diagnostics"}
+
+
 def optional_physics_forms(s64, stream, local, steps=2000):
     """The reference's optional physics on the same workload and state: the penalized
     operator (PENALIZED build, circle mask, eta = 0.01) as plain steps, and the iteration
@@ -401,7 +450,7 @@ def surrogate_form(local, epochs=80, ntraj=50, nsnap=41, n_intervals=200, judge_
         s.set_stream(stream.cuda_stream)
         s.set_state(*st0)
         rep = model.run(s, intervals=n_intervals, judge_every=judge_every,
-                        nu_tol=1e-3, spec_tol=0.0, spec_bins=32, fallback_intervals=judge_every, trace=True)
+                        nu_tol=1e-3, spec_tol=SPEC_TOL, spec_bins=32, fallback_intervals=judge_every, trace=True)
         s.close()
         tr = rep.pop("nu_trace")
         rep["nu_wall"] = float(tr[-1])
@@ -718,7 +767,8 @@ def main():
     # over the same 2000 steps from that state
     forms = None
     if args.form == "fp64" and not args.no_forms and world == 1:
-        forms = {"mixed": mixed_form(s, stream, args, local, world)}
+        forms = {"mixed": mixed_form(s, stream, args, local, world),
+                 "mixed_512x512x12": mixed_sdc_form(stream, local)}
         forms.update(optional_physics_forms(s, stream, local))
         if not args.no_batched:
             forms["batched"] = batched_form(local)

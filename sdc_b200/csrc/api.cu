@@ -317,12 +317,11 @@ __global__ void k_structure_function(const double2* __restrict__ th, const doubl
 // Launch of a step kernel that follows another kernel of the step on the same stream: with
 // programmatic stream serialization, so that its CTAs start and load their constant tables
 // while the predecessor drains (the kernel fences with pdl_wait before it touches step data).
-// A kernel launched this way reads step data written by its immediate predecessor only:
-// pdl_wait makes the predecessor's writes visible, and the chain of waits orders the
-// kernels, but a kernel that also read data written two launches back (the penalization
-// kernels, reading the synthesis) saw stale values when both links were programmatic.
-// Those kernels are launched plainly, which also covers the kernel after them. Plain
-// launches too while stage timing brackets every kernel with events.
+// Every CTA of every kernel launched this way executes pdl_wait before it can exit, so the
+// waits chain: a kernel's wait returns after all earlier kernels of the step completed.
+// Step data is read through L2 only (ld_cg / copy_cg, common.cuh): with L1-cached reads the
+// penalized operator read stale group values after its read-modify-write kernel. Plain
+// launches while stage timing brackets every kernel with events.
 template <typename... KArgs, typename... Args>
 static void launch_dep(rbc_handle* h, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args)
 {
@@ -558,10 +557,22 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
 // ------------------------------------------------------------------ tracers
 // 128 z levels of particle_tracer.cu:151-154 and the basis values of
 // calculate_velocity_operator.cu:458-488 (get_z_coeff_at), host FP64.
+template <typename R, int L> static void tracer_attributes(rbc_handle*)
+{
+    if constexpr (NodeRecLen<L>::value * sizeof(R) % 16 == 0)
+        RBC_CUDA(cudaFuncSetAttribute(k_tracers_bulk<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)tracer_bulk_smem<R, L>(kTracerBulkThreads)));
+}
+
 static void tracer_setup(rbc_handle* h)
 {
     h->ntr = h->prm.n_tracers;
     if (h->ntr == 0) return;
+    if (h->mixed) {
+        RBC_DISPATCH_L(tracer_attributes, float, h->G.L, h);
+    } else {
+        RBC_DISPATCH_L(tracer_attributes, double, h->G.L, h);
+    }
     const int L = h->G.L;
     const double zmax = 0.5f - 1e-3;
     std::vector<double> zb((size_t)kZNum * 3 * L);
@@ -657,6 +668,11 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.ly = h->G.ly;
     A.dt = h->G.dt;
     A.zmax = 0.5f - 1e-3;
+    A.sx = h->G.nx / h->G.lx;
+    A.sy = h->G.ny / h->G.ly;
+    A.sz = (kZNum - 1) / (2 * A.zmax);
+    A.inx = 1.0 / h->G.nx;
+    A.iny = 1.0 / h->G.ny;
     A.set_sigma = h->set_sig;
     A.per_set = h->tr_per_set;
     A.noise_seed = h->prm.noise_seed;
@@ -664,8 +680,15 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.track = h->trk;
     A.track_cap = h->trk_cap;
     A.track_period = h->trk_period;
+    A.err = h->err;
     StageScope sc(h, ST_TRACER);
-    k_tracers<R, L><<<(4 * h->ntr + 127) / 128, 128, 0, h->stream>>>(A); // 4 lanes per tracer
+    // 4 lanes per tracer; whole records by bulk copy where their size allows it
+    if constexpr (NodeRecLen<L>::value * sizeof(R) % 16 == 0) {
+        constexpr int T = kTracerBulkThreads;
+        k_tracers_bulk<R, L><<<(4 * h->ntr + T - 1) / T, T, tracer_bulk_smem<R, L>(T), h->stream>>>(A);
+    } else {
+        k_tracers<R, L><<<(4 * h->ntr + 127) / 128, 128, 0, h->stream>>>(A);
+    }
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -884,19 +907,17 @@ static void penalization_setup(rbc_handle* h)
 template <typename R, int L> static void launch_penalize(rbc_handle* h)
 {
     const rbc_params& p = h->prm;
-    // a plain launch: this kernel reads the synthesis, written two launches back
-    k_penalize<R, L><<<h->pen_blocks, kPenThreads, 0, h->stream>>>((const R*)h->phys, (R*)h->grp, h->pen_mask,
-                                                                    h->pen_cf, h->G.P, p.pr / p.penalization_eta,
-                                                                    0.5 / p.penalization_eta, h->pen_partial);
+    launch_dep(h, k_penalize<R, L>, dim3(h->pen_blocks), dim3(kPenThreads), 0, (const R*)h->phys, (R*)h->grp,
+               (const double*)h->pen_mask, (const double*)h->pen_cf, h->G.P, p.pr / p.penalization_eta,
+               0.5 / p.penalization_eta, h->pen_partial);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
 
 template <typename R, int L> static void launch_penalize_fg(rbc_handle* h)
 {
-    // a plain launch: this kernel reads k_penalize's partial sums, three launches back
-    k_penalize_fg<L><<<1, kPenFgThreads, 0, h->stream>>>(h->pen_partial, h->pen_blocks, h->pen_ia2,
-                                                         1.0 / (h->prm.penalization_eta * h->G.P), h->NFG);
+    launch_dep(h, k_penalize_fg<L>, dim3(1), dim3(kPenFgThreads), 0, (const double*)h->pen_partial, h->pen_blocks,
+               (const double*)h->pen_ia2, 1.0 / (h->prm.penalization_eta * h->G.P), h->NFG);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }

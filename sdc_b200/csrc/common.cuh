@@ -41,6 +41,31 @@ template <int BYTES> RBC_D void cp_async(void* smem_dst, const void* gmem_src)
 }
 RBC_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Reads of step data: data that an earlier kernel of the step wrote. The step's kernels
+// are launched with programmatic stream serialization (below), so a kernel can be resident
+// on an SM while its predecessor still runs there. Measured on B200: when the predecessor
+// also READ the data it then rewrote (the penalization kernel's read-modify-write of the
+// contracted groups), the dependent's non-coherent loads issued after griddepcontrol.wait
+// returned the pre-write values for a few rows; no such failure was seen with loads that
+// skip the L1. So step data is read with ld.global.cg / cp.async.cg, which go to L2, the
+// point of coherence; the data is streamed once per kernel, so nothing is lost.
+template <typename T> RBC_D T ld_cg(const T* p) { return __ldcg(p); }
+// Global -> shared copy of step data of 4, 8 or 16 bytes through L2: cp.async.cg for 16
+// bytes (asynchronous, completes at cp_async_wait_all), a register copy for 4 and 8
+// (cp.async has no L2-only form for them). Either is published by the __syncthreads that
+// follows cp_async_wait_all.
+template <int BYTES> RBC_D void copy_cg(void* smem_dst, const void* gmem_src)
+{
+    static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "copies of 4, 8 or 16 bytes");
+    if constexpr (BYTES == 16) {
+        cp_async<16>(smem_dst, gmem_src);
+    } else if constexpr (BYTES == 8) {
+        *static_cast<uint2*>(smem_dst) = __ldcg(static_cast<const uint2*>(gmem_src));
+    } else {
+        *static_cast<unsigned*>(smem_dst) = __ldcg(static_cast<const unsigned*>(gmem_src));
+    }
+}
+
 // Programmatic dependent launch (sm_90+). A kernel launched with the programmatic
 // stream-serialization attribute may start once every CTA of its predecessor in the stream
 // has called pdl_trigger (or exited), i.e. while the predecessor drains. Before pdl_wait
@@ -49,3 +74,51 @@ RBC_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory
 // completed and its writes are visible. Both are no-ops for an ordinary launch.
 RBC_D void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 RBC_D void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+// ---------------------------------------------------------------------------------
+// Bulk asynchronous copies (sm_90+): one instruction moves a contiguous block of global
+// memory into shared memory through the copy engine, completing on an mbarrier by bytes.
+// Both addresses 16-byte aligned, size a multiple of 16. Every wait on an mbarrier is
+// bounded: after kMbarSpins failed polls it gives up and reports false.
+RBC_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+RBC_D void mbar_init(unsigned long long* mbar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+// Makes initialised mbarriers visible to the copy engine (before the CTA barrier that
+// publishes them).
+RBC_D void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// Orders this thread's earlier generic accesses of shared memory before later bulk copies
+// into it.
+RBC_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+RBC_D void mbar_arrive(unsigned long long* mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(mbar)) : "memory");
+}
+RBC_D void mbar_arrive_expect_tx(unsigned long long* mbar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mbar)), "r"(bytes)
+                 : "memory");
+}
+RBC_D void bulk_g2s(void* smem_dst, const void* gmem_src, unsigned bytes, unsigned long long* mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(smem_dst)),
+                 "l"(gmem_src), "r"(bytes), "r"(smem_u32(mbar))
+                 : "memory");
+}
+constexpr unsigned kMbarSpins = 1u << 22;
+// Waits until the phase with the given parity has completed; false after kMbarSpins polls.
+RBC_D bool mbar_wait_parity(unsigned long long* mbar, unsigned parity)
+{
+    const unsigned a = smem_u32(mbar);
+    for (unsigned i = 0; i < kMbarSpins; ++i) {
+        unsigned ok;
+        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(ok)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+    }
+    return false;
+}

@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(128) k_contract(const R* __restrict__ phys, R*
 #pragma unroll
         for (int f = 0; f < rbcprog::NFIELD; ++f)
 #pragma unroll
-            for (int i = 0; i < L; ++i) in[f][i] = phys[((size_t)f * L + i) * P + x];
+            for (int i = 0; i < L; ++i) in[f][i] = ld_cg(phys + ((size_t)f * L + i) * P + x);
         if (nv) {
             constexpr int NR = NodeRec<L>::value;
             typedef typename cplx_t<R>::type R2;

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(kPenThreads) k_penalize(const R* __restrict__ 
 #pragma unroll
     for (int f = 0; f < 4; ++f)
 #pragma unroll
-        for (int j = 0; j < L; ++j) v[f][j] = m != 0.0 ? (double)phys[((size_t)fidx[f] * L + j) * sP + p] : 0.0;
+        for (int j = 0; j < L; ++j) v[f][j] = m != 0.0 ? (double)ld_cg(phys + ((size_t)fidx[f] * L + j) * sP + p) : 0.0;
     if (m != 0.0) {
         // modes in pairs: every load of a pair is issued before its stores
         constexpr int KB = L < 2 ? L : 2;
@@ -58,10 +58,10 @@ __global__ void __launch_bounds__(kPenThreads) k_penalize(const R* __restrict__ 
             for (int kk = 0; kk < KB; ++kk) {
                 const int k = k0 + kk;
                 if (k < L) {
-                    u31[kk] = (double)phys[((size_t)2 * L + k) * sP + p];
-                    th[kk] = (double)phys[((size_t)5 * L + k) * sP + p];
+                    u31[kk] = (double)ld_cg(phys + ((size_t)2 * L + k) * sP + p);
+                    th[kk] = (double)ld_cg(phys + ((size_t)5 * L + k) * sP + p);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) g[q][kk] = (double)grp[((size_t)gid[q] * L + k) * sP + p];
+                    for (int q = 0; q < 4; ++q) g[q][kk] = (double)ld_cg(grp + ((size_t)gid[q] * L + k) * sP + p);
                 }
             }
 #pragma unroll
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kPenFgThreads) k_penalize_fg(const double* __r
     for (int t = warp; t < 4 * L; t += nwarp) {
         double s = 0.0;
 #pragma unroll 8
-        for (int b = lane; b < nblocks; b += 32) s += partial[(size_t)b * 4 * L + t];
+        for (int b = lane; b < nblocks; b += 32) s += ld_cg(partial + (size_t)b * 4 * L + t);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) S[t] = s;
@@ -133,8 +133,8 @@ __global__ void __launch_bounds__(kPenFgThreads) k_penalize_fg(const double* __r
             f += ia2[j + k * L] * S[0 * L + j];
             g += ia2[j + k * L] * S[1 * L + j];
         }
-        NFG[k] += f * inv;
-        NFG[L + k] += g * inv;
+        NFG[k] = ld_cg(NFG + k) + f * inv;
+        NFG[L + k] = ld_cg(NFG + L + k) + g * inv;
     }
 }
 

@@ -108,9 +108,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns(
         for (int e = threadIdx.x; e < W * G.ny; e += blockDim.x) {
             const int cc = e / G.ny, r = e - cc * G.ny, c = c0 + cc;
             if (c < G.ckeep && row_kept(r, G.ny)) {
-                cp_async<16>(buf + (5 * W + cc) * st + rbcfft::pad(r), th + base + e);
-                cp_async<16>(buf + (0 * W + cc) * st + rbcfft::pad(r), f + base + e);
-                cp_async<16>(buf + (3 * W + cc) * st + rbcfft::pad(r), g + base + e);
+                copy_cg<16>(buf + (5 * W + cc) * st + rbcfft::pad(r), th + base + e);
+                copy_cg<16>(buf + (0 * W + cc) * st + rbcfft::pad(r), f + base + e);
+                copy_cg<16>(buf + (3 * W + cc) * st + rbcfft::pad(r), g + base + e);
             }
         }
         cp_async_wait_all();
@@ -126,9 +126,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns(
                 vf = make_double2(b.x, b.y);
                 vg = make_double2(d.x, d.y);
             } else {
-                vt = th[base + e];
-                vf = f[base + e];
-                vg = g[base + e];
+                vt = ld_cg(th + base + e);
+                vf = ld_cg(f + base + e);
+                vg = ld_cg(g + base + e);
             }
         }
         const Mult m(c, r, G);
@@ -180,8 +180,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r(
     for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
         const int n = e / NP, pp = e - n * NP;
         C* row = buf + pp * st;
-        cp_async<sizeof(C)>(row + rbcfft::pad(n), src + (size_t)n * G.ny + 2 * pp);
-        cp_async<sizeof(C)>(row + (n ? rbcfft::pad(nx - n) : st - 1), src + (size_t)n * G.ny + 2 * pp + 1);
+        copy_cg<sizeof(C)>(row + rbcfft::pad(n), src + (size_t)n * G.ny + 2 * pp);
+        copy_cg<sizeof(C)>(row + (n ? rbcfft::pad(nx - n) : st - 1), src + (size_t)n * G.ny + 2 * pp + 1);
     }
     for (int e = threadIdx.x; e < NP * nx; e += blockDim.x) {
         const int pp = e / nx, n = e - pp * nx;
@@ -236,8 +236,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c(
     for (int e = threadIdx.x; e < NP * nx; e += blockDim.x) {
         const int pp = e / nx, x = e - pp * nx;
         R* d = reinterpret_cast<R*>(buf + pp * st + rbcfft::pad(x));
-        cp_async<sizeof(R)>(d, src + (size_t)(2 * pp) * nx + x);
-        cp_async<sizeof(R)>(d + 1, src + (size_t)(2 * pp + 1) * nx + x);
+        copy_cg<sizeof(R)>(d, src + (size_t)(2 * pp) * nx + x);
+        copy_cg<sizeof(R)>(d + 1, src + (size_t)(2 * pp + 1) * nx + x);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
     const C* src = gh + ((size_t)k * G.ckp + c) * ny;
     for (int e = threadIdx.x; e < 13 * ny; e += blockDim.x) {
         const int grpi = e / ny, r = e - grpi * ny;
-        cp_async<sizeof(C)>(buf + grpi * py.stride + rbcfft::pad(r), src + grpi * cstride + r);
+        copy_cg<sizeof(C)>(buf + grpi * py.stride + rbcfft::pad(r), src + grpi * cstride + r);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -366,9 +366,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
     for (int e = threadIdx.x; e < W * N; e += blockDim.x) {
         const int cc = e / N, r = e - cc * N;
         if (c0 + cc < G.ckeep && row_kept(r, N)) {
-            cp_async<16>(stg + e, th + base + e);
-            cp_async<16>(stg + W * N + e, f + base + e);
-            cp_async<16>(stg + 2 * W * N + e, g + base + e);
+            copy_cg<16>(stg + e, th + base + e);
+            copy_cg<16>(stg + W * N + e, f + base + e);
+            copy_cg<16>(stg + 2 * W * N + e, g + base + e);
         }
     }
     cp_async_wait_all();
@@ -431,8 +431,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
     for (int e = threadIdx.x; e < NP * G.ckeep; e += blockDim.x) {
         const int n = e / NP, pp = e - n * NP;
         C* row = buf + pp * st;
-        cp_async<sizeof(C)>(row + rbcfft::pad(n), src + (size_t)n * G.ny + 2 * pp);
-        cp_async<sizeof(C)>(row + (n ? rbcfft::pad(N - n) : st - 1), src + (size_t)n * G.ny + 2 * pp + 1);
+        copy_cg<sizeof(C)>(row + rbcfft::pad(n), src + (size_t)n * G.ny + 2 * pp);
+        copy_cg<sizeof(C)>(row + (n ? rbcfft::pad(N - n) : st - 1), src + (size_t)n * G.ny + 2 * pp + 1);
     }
     for (int e = threadIdx.x; e < NP * N; e += blockDim.x) {
         const int pp = e / N, n = e - pp * N;
@@ -491,8 +491,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     C v[RX];
 #pragma unroll
     for (int a = 0; a < RX; ++a) {
-        v[a].x = src[t + RX * a];
-        v[a].y = src[N + t + RX * a];
+        v[a].x = ld_cg(src + t + RX * a);
+        v[a].y = ld_cg(src + N + t + RX * a);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     pdl_wait();
     C v[RX];
 #pragma unroll
-    for (int a = 0; a < RX; ++a) v[a] = src[t + RX * a];
+    for (int a = 0; a < RX; ++a) v[a] = ld_cg(src + t + RX * a);
     cp_async_wait_all();
     __syncthreads();
     C* S = buf + gq * st;

@@ -25,12 +25,16 @@ struct TracerArgs {
     double* pos;          // [3][n] x, y, z
     int n, nx, ny, L;
     double lx, ly, dt, zmax;
+    // grid-coordinate scales, precomputed on the host: nx / lx, ny / ly,
+    // (128 - 1) / (2 zmax), 1 / nx, 1 / ny (one multiply each where the reference divides)
+    double sx, sy, sz, inx, iny;
     const double* set_sigma;          // [sets] sqrt(2 D dt) of each tracer set (0: no diffusion)
     int per_set;                      // tracers per set (consecutive ranges)
     unsigned long long noise_seed;
     const long long* step_counter;    // completed fluid steps = step m of the new positions
     float* track;                     // [track_cap][3][n] FP32 frames, or null
     int track_cap, track_period;
+    int* err;                         // device error word (RBC_DEVERR_TIMEOUT from a wait that gave up)
 };
 
 template <int L> struct NodeRecLen { static constexpr int value = (5 * L + 1) & ~1; };
@@ -52,8 +56,7 @@ RBC_D void load_record(const R* __restrict__ nv, size_t xy, R (&rec)[NodeRecLen<
 
 // Velocity (u, v, w) of a node on the levels z0 and z1 from its record.
 template <typename R, int L>
-RBC_D void node_velocity(const R (&rec)[NodeRecLen<L>::value], const double* zb0, const double* zb1,
-                         double (&u0)[3], double (&u1)[3])
+RBC_D void node_velocity(const R* rec, const double* zb0, const double* zb1, double (&u0)[3], double (&u1)[3])
 {
     double a0 = 0, b0 = 0, c0 = 0, a1 = 0, b1 = 0, c1 = 0;
 #pragma unroll
@@ -72,22 +75,23 @@ RBC_D void node_velocity(const R (&rec)[NodeRecLen<L>::value], const double* zb0
     u1[0] = a1; u1[1] = b1; u1[2] = c1;
 }
 
-// Velocity at (x, y, z) by trilinear interpolation of the node velocities (the
-// reference's vel_interpolate). A team of 4 consecutive lanes handles one particle: lane
-// q takes the xy corner (q & 1, q >> 1), evaluates its node at the two bracketing levels,
-// weights it, and the team adds the 4 contributions with two shuffle rounds; every lane
-// of the team returns the sum.
-template <typename R, int L>
-RBC_D void vel_interp_team(const TracerArgs& A, const double* zb, int q, double x, double y, double z,
-                           double& rx, double& ry, double& rz, R (&rec)[NodeRecLen<L>::value], int& cached)
+// Cell of (x, y, z) as the reference's vel_interpolate finds it, for corner lane q of a team
+// of 4 (lane q takes the xy corner (q & 1, q >> 1)): the corner's node, the two bracketing
+// levels and the lane's trilinear weights.
+struct Corner {
+    int node, iz0, iz1;
+    double w, wz0, wz1;
+};
+RBC_D Corner find_corner(const TracerArgs& A, int q, double x, double y, double z)
 {
-    const R* nv = reinterpret_cast<const R*>(A.nv);
     const int xs = A.nx, ys = A.ny;
-    double xg = x * xs / A.lx;
-    double yg = y * ys / A.ly;
-    double zg = (A.zmax + z) / (2 * A.zmax) * (kZNum - 1);
-    xg -= floor(xg / xs) * xs;
-    yg -= floor(yg / ys) * ys;
+    // the reference's x Nx / Lx, (zmax + z) / (2 zmax) (Nz - 1) and periodic wrap, with the
+    // divisions replaced by multiplies with host-computed factors (equal to rounding)
+    double xg = x * A.sx;
+    double yg = y * A.sy;
+    double zg = (A.zmax + z) * A.sz;
+    xg -= floor(xg * A.inx) * xs;
+    yg -= floor(yg * A.iny) * ys;
     // __float2int_rd of the double: round to float, then down
     int ix0 = __float2int_rd((float)xg), iy0 = __float2int_rd((float)yg), iz0 = __float2int_rd((float)zg);
     if (ix0 < 0 || ix0 >= xs) ix0 = 0;
@@ -96,24 +100,31 @@ RBC_D void vel_interp_team(const TracerArgs& A, const double* zb, int q, double 
     else if (iz0 >= kZNum) iz0 = kZNum - 1;
     const int ix1 = (ix0 + 1 >= xs) ? 0 : ix0 + 1;
     const int iy1 = (iy0 + 1 >= ys) ? 0 : iy0 + 1;
-    const int iz1 = (iz0 + 1 >= kZNum) ? iz0 : iz0 + 1;
+    Corner c;
+    c.iz0 = iz0;
+    c.iz1 = (iz0 + 1 >= kZNum) ? iz0 : iz0 + 1;
     const double wx1 = xg - (double)ix0, wx0 = 1 - wx1;
     const double wy1 = yg - (double)iy0, wy0 = 1 - wy1;
-    const double wz1 = zg - (double)iz0, wz0 = 1 - wz1;
+    c.wz1 = zg - (double)iz0;
+    c.wz0 = 1 - c.wz1;
     const int ix = (q & 1) ? ix1 : ix0, iy = (q >> 1) ? iy1 : iy0;
-    const double w = ((q & 1) ? wx1 : wx0) * ((q >> 1) ? wy1 : wy0);
-    // RK stages rarely leave the cell: reload this corner's record only when it changed
-    const int node = iy * xs + ix;
-    if (node != cached) {
-        load_record<R, L>(nv, (size_t)node, rec);
-        cached = node;
-    }
+    c.w = ((q & 1) ? wx1 : wx0) * ((q >> 1) ? wy1 : wy0);
+    c.node = iy * xs + ix;
+    return c;
+}
+
+// The team's interpolated velocity from this lane's corner record: the node evaluated at
+// the two levels, weighted, and the 4 contributions added with two shuffle rounds; every
+// lane of the team returns the sum.
+template <typename R, int L>
+RBC_D void team_velocity(const Corner& c, const R* rec, const double* zb, double& rx, double& ry, double& rz)
+{
     double u0[3], u1[3];
-    node_velocity<R, L>(rec, zb + (size_t)iz0 * 3 * L, zb + (size_t)iz1 * 3 * L, u0, u1);
+    node_velocity<R, L>(rec, zb + (size_t)c.iz0 * 3 * L, zb + (size_t)c.iz1 * 3 * L, u0, u1);
     double v[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        v[d] = w * (wz0 * u0[d] + wz1 * u1[d]);
+        v[d] = c.w * (c.wz0 * u0[d] + c.wz1 * u1[d]);
         v[d] += __shfl_xor_sync(0xffffffffu, v[d], 1, 4);
         v[d] += __shfl_xor_sync(0xffffffffu, v[d], 2, 4);
     }
@@ -122,33 +133,46 @@ RBC_D void vel_interp_team(const TracerArgs& A, const double* zb, int q, double 
     rz = v[2];
 }
 
+// Velocity at (x, y, z) by trilinear interpolation of the node velocities (the
+// reference's vel_interpolate), a team of 4 consecutive lanes per particle, the corner
+// record held in registers.
 template <typename R, int L>
-__global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
+RBC_D void vel_interp_team(const TracerArgs& A, const double* zb, int q, double x, double y, double z,
+                           double& rx, double& ry, double& rz, R (&rec)[NodeRecLen<L>::value], int& cached)
 {
-    __shared__ double zb[kZNum * 3 * L];
-    for (int e = threadIdx.x; e < kZNum * 3 * L; e += blockDim.x) zb[e] = A.zbasis[e];
-    __syncthreads();
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = gt >> 2, q = gt & 3;               // particle, corner lane
-    const bool live = t < A.n;                       // whole teams are live or not
-    const int tt = live ? t : 0;
-    double x = A.pos[tt], y = A.pos[A.n + tt], z = A.pos[2 * A.n + tt];
-    const double dt = A.dt;
+    const Corner c = find_corner(A, q, x, y, z);
+    // RK stages rarely leave the cell: reload this corner's record only when it changed
+    if (c.node != cached) {
+        load_record<R, L>(reinterpret_cast<const R*>(A.nv), (size_t)c.node, rec);
+        cached = c.node;
+    }
+    team_velocity<R, L>(c, rec, zb, rx, ry, rz);
+}
+
+// RK4 on the frozen field (step_particle_on_GPU, particle_tracer.cu:610-687): vel(x, y, z,
+// vx, vy, vz) returns the team's interpolated velocity.
+template <typename V>
+RBC_D void rk4_team(double& x, double& y, double& z, double dt, V&& vel)
+{
     double vx, vy, vz;
-    R rec[NodeRecLen<L>::value];
-    int cached = -1;
-    vel_interp_team<R, L>(A, zb, q, x, y, z, vx, vy, vz, rec, cached);
+    vel(x, y, z, vx, vy, vz);
     const double dx1 = dt * vx, dy1 = dt * vy, dz1 = dt * vz;
-    vel_interp_team<R, L>(A, zb, q, x + 0.5 * dx1, y + 0.5 * dy1, z + 0.5 * dz1, vx, vy, vz, rec, cached);
+    vel(x + 0.5 * dx1, y + 0.5 * dy1, z + 0.5 * dz1, vx, vy, vz);
     const double dx2 = dt * vx, dy2 = dt * vy, dz2 = dt * vz;
-    vel_interp_team<R, L>(A, zb, q, x + 0.5 * dx2, y + 0.5 * dy2, z + 0.5 * dz2, vx, vy, vz, rec, cached);
+    vel(x + 0.5 * dx2, y + 0.5 * dy2, z + 0.5 * dz2, vx, vy, vz);
     const double dx3 = dt * vx, dy3 = dt * vy, dz3 = dt * vz;
-    vel_interp_team<R, L>(A, zb, q, x + dx3, y + dy3, z + dz3, vx, vy, vz, rec, cached);
+    vel(x + dx3, y + dy3, z + dz3, vx, vy, vz);
     const double dx4 = dt * vx, dy4 = dt * vy, dz4 = dt * vz;
-    x += (dx1 + 2 * (dx2 + dx3) + dx4) / 6.;
-    y += (dy1 + 2 * (dy2 + dy3) + dy4) / 6.;
-    z += (dz1 + 2 * (dz2 + dz3) + dz4) / 6.;
-    if (!(live && q == 0)) return;
+    constexpr double sixth = 1.0 / 6.0;
+    x += (dx1 + 2 * (dx2 + dx3) + dx4) * sixth;
+    y += (dy1 + 2 * (dy2 + dy3) + dy4) * sixth;
+    z += (dz1 + 2 * (dz2 + dz3) + dz4) * sixth;
+}
+
+// Diffusion step, lid reflection and store (with the track frame) of particle t's new
+// position; called by one lane per particle.
+RBC_D void finish_tracer(const TracerArgs& A, int t, double x, double y, double z)
+{
     const long long m = *A.step_counter;
     const double sg = A.set_sigma[t / A.per_set];
     if (sg > 0.0) {
@@ -169,6 +193,91 @@ __global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
         fr[A.n + t] = (float)y;
         fr[2 * A.n + t] = (float)z;
     }
+}
+
+// Corner records gathered by the lanes' own loads into registers (any record size).
+template <typename R, int L>
+__global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
+{
+    __shared__ double zb[kZNum * 3 * L];
+    for (int e = threadIdx.x; e < kZNum * 3 * L; e += blockDim.x) zb[e] = A.zbasis[e];
+    __syncthreads();
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = gt >> 2, q = gt & 3;               // particle, corner lane
+    const bool live = t < A.n;                       // whole teams are live or not
+    const int tt = live ? t : 0;
+    double x = A.pos[tt], y = A.pos[A.n + tt], z = A.pos[2 * A.n + tt];
+    R rec[NodeRecLen<L>::value];
+    int cached = -1;
+    rk4_team(x, y, z, A.dt, [&](double px, double py, double pz, double& vx, double& vy, double& vz) {
+        vel_interp_team<R, L>(A, zb, q, px, py, pz, vx, vy, vz, rec, cached);
+    });
+    if (live && q == 0) finish_tracer(A, t, x, y, z);
+}
+
+// Bytes of dynamic shared memory of k_tracers_bulk: the z basis, then one record slot per
+// thread.
+template <typename R, int L> RBC_HD constexpr size_t tracer_bulk_smem(int threads)
+{
+    return ((size_t)kZNum * 3 * L * sizeof(double) + 15) / 16 * 16 + (size_t)threads * NodeRecLen<L>::value * sizeof(R);
+}
+constexpr int kTracerBulkThreads = 256;
+
+// The same advance with each corner record brought into the lane's own shared-memory slot
+// by one bulk copy (the copy engine moves the whole record, where register loads issue one
+// 16-byte request per lane per chunk and fill the load queue). Record size a multiple of 16
+// bytes. Per RK stage every lane of a warp arrives once on the warp's mbarrier, with the
+// record's bytes when it copies (its corner changed); the warp then waits for the phase.
+// A wait that gives up sets RBC_DEVERR_TIMEOUT in the error word.
+template <typename R, int L>
+__global__ void __launch_bounds__(kTracerBulkThreads) k_tracers_bulk(TracerArgs A)
+{
+    constexpr int NR = NodeRecLen<L>::value;
+    constexpr unsigned RB = NR * sizeof(R);
+    static_assert(RB % 16 == 0, "bulk copies move multiples of 16 bytes");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned long long mbar[kTracerBulkThreads / 32];
+    double* zb = reinterpret_cast<double*>(smem_raw);
+    R* slot = reinterpret_cast<R*>(smem_raw + ((size_t)kZNum * 3 * L * sizeof(double) + 15) / 16 * 16) +
+              (size_t)threadIdx.x * NR;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        mbar_init(&mbar[wid], 32);
+        mbar_fence_init();
+    }
+    for (int e = threadIdx.x; e < kZNum * 3 * L; e += blockDim.x) zb[e] = A.zbasis[e];
+    __syncthreads();
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = gt >> 2, q = gt & 3;
+    const bool live = t < A.n;
+    const int tt = live ? t : 0;
+    double x = A.pos[tt], y = A.pos[A.n + tt], z = A.pos[2 * A.n + tt];
+    const R* nv = reinterpret_cast<const R*>(A.nv);
+    int cached = -1;
+    unsigned phase = 0;
+    bool ok = true;
+    rk4_team(x, y, z, A.dt, [&](double px, double py, double pz, double& vx, double& vy, double& vz) {
+        const Corner c = find_corner(A, q, px, py, pz);
+        if (c.node != cached) {
+            fence_proxy_async_smem(); // this lane's reads of its slot come before the copy
+            mbar_arrive_expect_tx(&mbar[wid], RB);
+            bulk_g2s(slot, nv + (size_t)c.node * NR, RB, &mbar[wid]);
+            cached = c.node;
+        } else {
+            mbar_arrive(&mbar[wid]);
+        }
+        if (!mbar_wait_parity(&mbar[wid], phase)) ok = false;
+        phase ^= 1;
+        team_velocity<R, L>(c, slot, zb, vx, vy, vz);
+    });
+    if (!ok) {
+        // a copy this warp waited for did not land: flag it, give any copy still in flight
+        // into this CTA's shared memory one more bounded wait, and leave the position as is
+        atomicOr(A.err, RBC_DEVERR_TIMEOUT);
+        mbar_wait_parity(&mbar[wid], phase ^ 1);
+        return;
+    }
+    if (live && q == 0) finish_tracer(A, t, x, y, z);
 }
 
 // Copies positions into one FP32 track frame (the frame of freshly set positions).

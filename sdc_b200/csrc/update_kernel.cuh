@@ -86,18 +86,19 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
         const bool mirror = (c == 0 && r > 0 && r < ny / 2);
         double2 nt = make_double2(0, 0), nf = nt, ng = nt, ut = nt, uf = nt, ug = nt, ht = nt, hf = nt, hg = nt;
         if (geo) {
-            const C t0 = Nc[(0 * L + k) * plane + o], t1 = Nc[(1 * L + k) * plane + o], t2 = Nc[(2 * L + k) * plane + o];
+            const C t0 = ld_cg(Nc + (0 * L + k) * plane + o), t1 = ld_cg(Nc + (1 * L + k) * plane + o),
+                    t2 = ld_cg(Nc + (2 * L + k) * plane + o);
             nt = make_double2(t0.x, t0.y);
             nf = make_double2(t1.x, t1.y);
             ng = make_double2(t2.x, t2.y);
             if (!mirror) {
-                ut = A.th[k * plane + o];
-                uf = A.f[k * plane + o];
-                ug = A.g[k * plane + o];
+                ut = ld_cg(A.th + k * plane + o);
+                uf = ld_cg(A.f + k * plane + o);
+                ug = ld_cg(A.g + k * plane + o);
                 if (!A.first) {
-                    ht = A.hist[(0 * L + k) * plane + o];
-                    hf = A.hist[(1 * L + k) * plane + o];
-                    hg = A.hist[(2 * L + k) * plane + o];
+                    ht = ld_cg(A.hist + (0 * L + k) * plane + o);
+                    hf = ld_cg(A.hist + (1 * L + k) * plane + o);
+                    hg = ld_cg(A.hist + (2 * L + k) * plane + o);
                 }
             }
         }
@@ -215,10 +216,10 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
                 const double fac = 1.0 / (1.0 + dt * pr * mpi * mpi);
 #pragma unroll
                 for (int s = 0; s < 2; ++s) {
-                    const double b = 2.0 * pr * A.NFG[s * L + k];
-                    double2 u = A.FG[s * L + k];
+                    const double b = 2.0 * pr * ld_cg(A.NFG + s * L + k);
+                    double2 u = ld_cg(A.FG + s * L + k);
                     u.x = fma(b, a1, u.x);
-                    if (!A.first) u.x = fma(A.hFG[s * L + k].x, a2, u.x);
+                    if (!A.first) u.x = fma(ld_cg(A.hFG + s * L + k).x, a2, u.x);
                     A.hFG[s * L + k] = make_double2(b, 0.0);
                     u = make_double2(fac * u.x, 0.0);
                     A.FG[s * L + k] = u;
