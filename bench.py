@@ -562,6 +562,24 @@ def profile_field_ops(local, iters=5):
                       "n_theta_00": abs(n[0][0, 0, 0])}))
 
 
+def profile_diagnostics(local, iters=3):
+    """Small workload for kernel profiling of the diagnostics and loop extras on the plain
+    step's 256 x 256 x 8 grid without tracers: `iters` radial spectra of theta at z = 0 (64
+    shells), structure functions of theta and u_1 along x (32 displacements each), and steps
+    with the mean-flow forcing (-mean_F 0.01, one forcing kernel per step)."""
+    import sdc_b200
+    s = sdc_b200.Solver(**WORK, device=local, mean_F=0.01)
+    s.init_fields(SEED, 1e-3, 8.0)
+    s.step(5)
+    for _ in range(iters):
+        sp = s.spectrum(64, 0.0)
+        s.structure_function("theta", "x", 0.1, 8.0, 32)
+        s.structure_function("u1", "x", 0.1, 8.0, 32)
+        s.step(1)
+    print(json.dumps({"profile_diagnostics": "done", "spectrum_0": float(sp[0]),
+                      "nu_wall": s.diagnostics()["nu_wall"]}))
+
+
 def ensemble_configs(n=64, seed=4):
     """The uneven ensemble: per member a grid from {64, 128, 192, 256}^2, Nz from {4, 6, 8},
     Ra ~ U[2000, 8000], Pr from {0.7, 1, 7}, Lx = Ly = grid / 8, dt = 5e-4 (drawn by seed)."""
@@ -635,6 +653,8 @@ def main():
                     help="run only a small surrogate workload (for kernel profiling) and exit")
     ap.add_argument("--profile-field-ops", action="store_true",
                     help="run only a small freeze/heating/penalization workload (for kernel profiling) and exit")
+    ap.add_argument("--profile-diagnostics", action="store_true",
+                    help="run only a small spectrum/structure-function/mean-forcing workload (for kernel profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_surrogate:
@@ -642,6 +662,9 @@ def main():
         return
     if args.profile_field_ops:
         profile_field_ops(int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.profile_diagnostics:
+        profile_diagnostics(int(os.environ.get("LOCAL_RANK", "0")))
         return
 
     world, rank, local = dist_env()

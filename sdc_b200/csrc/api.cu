@@ -92,6 +92,7 @@ struct rbc_handle {
     int* err = nullptr;
     int ring_cap = 4096;
     int upd_blocks = 0;
+    int upd_nlow = 0, upd_nkr = 0;  // kept rows r < upd_nlow or r >= upd_nlow + (Ny - upd_nkr)
     long long host_steps = 0;
     // staging for layout conversion
     double2* stage = nullptr;
@@ -394,6 +395,8 @@ template <typename R, int L> static void launch_update(rbc_handle* h)
     A.ring_cap = h->ring_cap;
     A.step_counter = h->step_counter;
     A.err = h->err;
+    A.nlow = h->upd_nlow;
+    A.nkr = h->upd_nkr;
     StageScope sc(h, ST_UPDATE);
     launch_dep(h, k_update<R, L>, dim3(h->upd_blocks), dim3(kThreads), 0, A);
     RBC_CUDA(cudaGetLastError());
@@ -557,22 +560,10 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
 // ------------------------------------------------------------------ tracers
 // 128 z levels of particle_tracer.cu:151-154 and the basis values of
 // calculate_velocity_operator.cu:458-488 (get_z_coeff_at), host FP64.
-template <typename R, int L> static void tracer_attributes(rbc_handle*)
-{
-    if constexpr (NodeRecLen<L>::value * sizeof(R) % 16 == 0)
-        RBC_CUDA(cudaFuncSetAttribute(k_tracers_bulk<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)tracer_bulk_smem<R, L>(kTracerBulkThreads)));
-}
-
 static void tracer_setup(rbc_handle* h)
 {
     h->ntr = h->prm.n_tracers;
     if (h->ntr == 0) return;
-    if (h->mixed) {
-        RBC_DISPATCH_L(tracer_attributes, float, h->G.L, h);
-    } else {
-        RBC_DISPATCH_L(tracer_attributes, double, h->G.L, h);
-    }
     const int L = h->G.L;
     const double zmax = 0.5f - 1e-3;
     std::vector<double> zb((size_t)kZNum * 3 * L);
@@ -680,15 +671,8 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.track = h->trk;
     A.track_cap = h->trk_cap;
     A.track_period = h->trk_period;
-    A.err = h->err;
     StageScope sc(h, ST_TRACER);
-    // 4 lanes per tracer; whole records by bulk copy where their size allows it
-    if constexpr (NodeRecLen<L>::value * sizeof(R) % 16 == 0) {
-        constexpr int T = kTracerBulkThreads;
-        k_tracers_bulk<R, L><<<(4 * h->ntr + T - 1) / T, T, tracer_bulk_smem<R, L>(T), h->stream>>>(A);
-    } else {
-        k_tracers<R, L><<<(4 * h->ntr + 127) / 128, 128, 0, h->stream>>>(A);
-    }
+    k_tracers<R, L><<<(4 * h->ntr + 127) / 128, 128, 0, h->stream>>>(A); // 4 lanes per tracer
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -1168,14 +1152,24 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         h->gh = dalloc<unsigned char>(13 * plane * L * csz, h->owned);
         h->N = dalloc<unsigned char>(3 * plane * L * csz, h->owned);
         h->NFG = dalloc<double>(2 * L, h->owned);
+        // the 2/3 rule keeps a prefix and a suffix of the rows
+        h->upd_nlow = 0;
+        while (h->upd_nlow < G.ny && row_kept(h->upd_nlow, G.ny)) ++h->upd_nlow;
+        h->upd_nkr = 0;
+        for (int r = 0; r < G.ny; ++r)
+            if (row_kept(r, G.ny)) ++h->upd_nkr;
+        for (int r = 0; r < G.ny; ++r) {
+            const bool want = r < h->upd_nlow || r >= h->upd_nlow + (G.ny - h->upd_nkr);
+            if (want != row_kept(r, G.ny)) throw ArgError{"kept rows are not a prefix and a suffix"};
+        }
         switch (L) {
-        case 2: h->upd_blocks = update_blocks<2>(G.ckeep, G.ny); break;
-        case 3: h->upd_blocks = update_blocks<3>(G.ckeep, G.ny); break;
-        case 4: h->upd_blocks = update_blocks<4>(G.ckeep, G.ny); break;
-        case 5: h->upd_blocks = update_blocks<5>(G.ckeep, G.ny); break;
-        case 6: h->upd_blocks = update_blocks<6>(G.ckeep, G.ny); break;
-        case 8: h->upd_blocks = update_blocks<8>(G.ckeep, G.ny); break;
-        default: h->upd_blocks = update_blocks<12>(G.ckeep, G.ny); break;
+        case 2: h->upd_blocks = update_blocks<2>(G.ckeep, h->upd_nkr); break;
+        case 3: h->upd_blocks = update_blocks<3>(G.ckeep, h->upd_nkr); break;
+        case 4: h->upd_blocks = update_blocks<4>(G.ckeep, h->upd_nkr); break;
+        case 5: h->upd_blocks = update_blocks<5>(G.ckeep, h->upd_nkr); break;
+        case 6: h->upd_blocks = update_blocks<6>(G.ckeep, h->upd_nkr); break;
+        case 8: h->upd_blocks = update_blocks<8>(G.ckeep, h->upd_nkr); break;
+        default: h->upd_blocks = update_blocks<12>(G.ckeep, h->upd_nkr); break;
         }
         h->partial = dalloc<double>(2 * (size_t)h->upd_blocks, h->owned);
         h->th00 = dalloc<double>(L, h->owned);

@@ -34,7 +34,6 @@ struct TracerArgs {
     const long long* step_counter;    // completed fluid steps = step m of the new positions
     float* track;                     // [track_cap][3][n] FP32 frames, or null
     int track_cap, track_period;
-    int* err;                         // device error word (RBC_DEVERR_TIMEOUT from a wait that gave up)
 };
 
 template <int L> struct NodeRecLen { static constexpr int value = (5 * L + 1) & ~1; };
@@ -212,71 +211,6 @@ __global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
     rk4_team(x, y, z, A.dt, [&](double px, double py, double pz, double& vx, double& vy, double& vz) {
         vel_interp_team<R, L>(A, zb, q, px, py, pz, vx, vy, vz, rec, cached);
     });
-    if (live && q == 0) finish_tracer(A, t, x, y, z);
-}
-
-// Bytes of dynamic shared memory of k_tracers_bulk: the z basis, then one record slot per
-// thread.
-template <typename R, int L> RBC_HD constexpr size_t tracer_bulk_smem(int threads)
-{
-    return ((size_t)kZNum * 3 * L * sizeof(double) + 15) / 16 * 16 + (size_t)threads * NodeRecLen<L>::value * sizeof(R);
-}
-constexpr int kTracerBulkThreads = 256;
-
-// The same advance with each corner record brought into the lane's own shared-memory slot
-// by one bulk copy (the copy engine moves the whole record, where register loads issue one
-// 16-byte request per lane per chunk and fill the load queue). Record size a multiple of 16
-// bytes. Per RK stage every lane of a warp arrives once on the warp's mbarrier, with the
-// record's bytes when it copies (its corner changed); the warp then waits for the phase.
-// A wait that gives up sets RBC_DEVERR_TIMEOUT in the error word.
-template <typename R, int L>
-__global__ void __launch_bounds__(kTracerBulkThreads) k_tracers_bulk(TracerArgs A)
-{
-    constexpr int NR = NodeRecLen<L>::value;
-    constexpr unsigned RB = NR * sizeof(R);
-    static_assert(RB % 16 == 0, "bulk copies move multiples of 16 bytes");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ unsigned long long mbar[kTracerBulkThreads / 32];
-    double* zb = reinterpret_cast<double*>(smem_raw);
-    R* slot = reinterpret_cast<R*>(smem_raw + ((size_t)kZNum * 3 * L * sizeof(double) + 15) / 16 * 16) +
-              (size_t)threadIdx.x * NR;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) {
-        mbar_init(&mbar[wid], 32);
-        mbar_fence_init();
-    }
-    for (int e = threadIdx.x; e < kZNum * 3 * L; e += blockDim.x) zb[e] = A.zbasis[e];
-    __syncthreads();
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = gt >> 2, q = gt & 3;
-    const bool live = t < A.n;
-    const int tt = live ? t : 0;
-    double x = A.pos[tt], y = A.pos[A.n + tt], z = A.pos[2 * A.n + tt];
-    const R* nv = reinterpret_cast<const R*>(A.nv);
-    int cached = -1;
-    unsigned phase = 0;
-    bool ok = true;
-    rk4_team(x, y, z, A.dt, [&](double px, double py, double pz, double& vx, double& vy, double& vz) {
-        const Corner c = find_corner(A, q, px, py, pz);
-        if (c.node != cached) {
-            fence_proxy_async_smem(); // this lane's reads of its slot come before the copy
-            mbar_arrive_expect_tx(&mbar[wid], RB);
-            bulk_g2s(slot, nv + (size_t)c.node * NR, RB, &mbar[wid]);
-            cached = c.node;
-        } else {
-            mbar_arrive(&mbar[wid]);
-        }
-        if (!mbar_wait_parity(&mbar[wid], phase)) ok = false;
-        phase ^= 1;
-        team_velocity<R, L>(c, slot, zb, vx, vy, vz);
-    });
-    if (!ok) {
-        // a copy this warp waited for did not land: flag it, give any copy still in flight
-        // into this CTA's shared memory one more bounded wait, and leave the position as is
-        atomicOr(A.err, RBC_DEVERR_TIMEOUT);
-        mbar_wait_parity(&mbar[wid], phase ^ 1);
-        return;
-    }
     if (live && q == 0) finish_tracer(A, t, x, y, z);
 }
 

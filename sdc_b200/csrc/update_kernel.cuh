@@ -39,6 +39,8 @@ struct UpdateArgs {
     int ring_cap;
     long long* step_counter;
     int* err;
+    // kept rows (2/3 rule): r < nlow or r >= nlow + (ny - nkr); teams cover only these
+    int nlow, nkr;
 };
 
 template <int L> struct TeamSize { static constexpr int value = L <= 2 ? 2 : L <= 4 ? 4 : L <= 8 ? 8 : 16; };
@@ -49,7 +51,7 @@ RBC_D double2 shfl2(double2 v, int src, int width)
 }
 
 template <typename R, int L>
-__global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
+__global__ void __launch_bounds__(kThreads, L <= 8 ? 2 : 1) k_update(UpdateArgs A)
 {
     typedef typename cplx_t<R>::type C;
     constexpr int T = TeamSize<L>::value;
@@ -68,18 +70,21 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
     const double a1 = A.first ? dt : 1.5 * dt, a2 = -0.5 * dt;
     const double mpi = (k + 1) * kPi;
     double esum = 0.0, wsum = 0.0;
-    const long long nwave = (long long)G.ckeep * ny;
+    const long long nwave = (long long)G.ckeep * A.nkr; // kept wavenumbers
     pdl_trigger();
     {
-        const long long e = (long long)blockIdx.x * (blockDim.x / T) + threadIdx.x / T; // wavenumber c * ny + r
-        const int c = (int)(e / ny), r = (int)(e - (long long)c * ny);
+        // kept wavenumber e = c * nkr + j, j the kept-row index (the removed rows stay zero
+        // and get no team)
+        const long long e = (long long)blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
+        const int c = (int)(e / A.nkr), j = (int)(e - (long long)c * A.nkr);
+        const int r = j < A.nlow ? j : j + (ny - A.nkr);
+        const size_t o = (size_t)c * ny + r;           // CM offset in a plane
         // the class index is constant and is fetched before the wait; after it the
         // vectors and the class's table rows are fetched together (the vector loads are
         // predicated on the kept band by its formula, always in bounds)
-        const int cl = (e < nwave) ? __ldg(A.cls + e) : -1;   // uniform over the team
+        const int cl = (e < nwave) ? __ldg(A.cls + o) : -1;   // uniform over the team
         pdl_wait(); // N and the mean-flow terms come from the column pass
         const bool geo = e < nwave && k < L && c < G.ckeep && row_kept(r, ny);
-        const size_t o = (size_t)e;
         const int ry = wrap_row(r, ny);
         const double mx = (kPi + kPi) * (c / G.lx), my = (kPi + kPi) * (ry / G.ly);
         const double q2d = mx * mx + my * my;       // device formula of the reference kernels
@@ -283,10 +288,10 @@ __global__ void __launch_bounds__(kThreads) k_update(UpdateArgs A)
     }
 }
 
-// One team per kept-column wavenumber.
-template <int L> inline int update_blocks(int ckeep, int ny)
+// One team per kept wavenumber (ckeep columns x nkr kept rows).
+template <int L> inline int update_blocks(int ckeep, int nkr)
 {
-    const long long threads = (long long)ckeep * ny * TeamSize<L>::value;
+    const long long threads = (long long)ckeep * nkr * TeamSize<L>::value;
     return (int)((threads + kThreads - 1) / kThreads);
 }
 
