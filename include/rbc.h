@@ -445,8 +445,18 @@ typedef struct {
                                 step's own q = 0 recursion over interval_steps steps, forced by
                                 the solver's nonlinear operator at the interval start (linear
                                 in time with the previous interval's); 0: from the network */
+    int gemm_path;           /* 0: products with K-contiguous rows, N <= 256 and >= 128 rows on
+                                the 5th-generation tensor cores (tcgen05, TMEM accumulator),
+                                the rest on mma.sync tiles; 1: mma.sync tiles for all */
 } rbc_fno_params;
 rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out);
+/* BF16 GEMM of the surrogate's kernels on device buffers (no reference counterpart; the
+ * numerics check of its tensor-core paths): C[M][N] (FP32, row-major) = A[M][K] B[K][N]
+ * (BF16, row-major, FP32 accumulation). path 0: tcgen05 when eligible (M >= 128, N <= 256,
+ * K a multiple of 8), 1: mma.sync tiles. Work on `stream` (NULL: legacy default stream),
+ * waited for before the call returns; RBC_ERR_CUDA if a tensor-core wait gave up. */
+rbc_status rbc_gemm_bf16(int device, const void* A, const void* B, float* C, int M, int N, int K, int path,
+                         void* stream);
 void rbc_fno_destroy(rbc_fno* m);
 const char* rbc_fno_last_error(const rbc_fno* m);
 long long rbc_fno_num_params(const rbc_fno* m);

@@ -45,7 +45,8 @@ class _FnoParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nq", ctypes.c_int),
                 ("width", ctypes.c_int), ("modes", ctypes.c_int), ("layers", ctypes.c_int),
                 ("hidden", ctypes.c_int), ("max_batch", ctypes.c_int), ("device", ctypes.c_int),
-                ("seed", ctypes.c_ulonglong), ("interval_steps", ctypes.c_int), ("physics_mean", ctypes.c_int)]
+                ("seed", ctypes.c_ulonglong), ("interval_steps", ctypes.c_int), ("physics_mean", ctypes.c_int),
+                ("gemm_path", ctypes.c_int)]
 
 
 class _SurrogateParams(ctypes.Structure):
@@ -74,7 +75,7 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_save_state", "rbc_load_state", "rbc_save_history", "rbc_load_history", "rbc_ensemble_create",
            "rbc_ensemble_destroy", "rbc_ensemble_member", "rbc_ensemble_step", "rbc_ensemble_last_error", "rbc_launch_config",
            "rbc_kernel_launches", "rbc_tracers_init", "rbc_tracer_moments", "rbc_tracks_read", "rbc_track_write",
-           "rbc_init_pattern", "rbc_fno_create", "rbc_fno_destroy", "rbc_fno_last_error", "rbc_fno_num_params",
+           "rbc_init_pattern", "rbc_fno_create", "rbc_gemm_bf16", "rbc_fno_destroy", "rbc_fno_last_error", "rbc_fno_num_params",
            "rbc_fno_get_params", "rbc_fno_set_params", "rbc_fno_get_norm", "rbc_fno_set_norm", "rbc_fno_forward",
            "rbc_fno_loss_grad", "rbc_fno_colloc_get", "rbc_fno_colloc_add", "rbc_fno_dataset_reserve",
            "rbc_fno_dataset_capture", "rbc_fno_train", "rbc_fno_advance", "rbc_surrogate_run",
@@ -86,6 +87,7 @@ FIELD_OPS = {"freeze": 1, "heat": 2, "scale": 4}
 MASK_SHAPES = {"circle": 0, "rectangle": 1}
 PEN_MASKS = {"rectangle": 0, "circle": 1, "disk_array": 2, "everywhere": 3}
 INIT_PATTERNS = {"isr": 1, "dislocation": 2, "rectangle": 3, "sv": 4, "cr": 5, "giantspiral": 6, "test": 7}
+GEMM_PATHS = {"tcgen05": 0, "mma_sync": 1}
 TRACER_PATTERNS = {"random": 0, "center": 1, "center_sigma": 2, "diagonal": 3, "pairs": 4, "coord_sigma": 5}
 
 
@@ -168,6 +170,7 @@ def lib():
     L.rbc_tracer_moments_set.argtypes = [vp, ctypes.c_int, _dp]
     L.rbc_diagnostics_get.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(_Diag)]
     L.rbc_fno_create.argtypes = [ctypes.POINTER(_FnoParams), ctypes.POINTER(vp)]
+    L.rbc_gemm_bf16.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
     L.rbc_fno_destroy.argtypes = [vp]
     L.rbc_fno_destroy.restype = None
     L.rbc_fno_last_error.argtypes = [vp]
@@ -555,12 +558,12 @@ class FNO:
     [batch][ny][nx][C]."""
 
     def __init__(self, nx, ny, nz, nq, width=32, modes=16, layers=4, hidden=128, max_batch=8, device=0, seed=0,
-                 interval_steps=40, physics_mean=True):
+                 interval_steps=40, physics_mean=True, gemm_path="tcgen05"):
         self.nx, self.ny, self.nz, self.nq = nx, ny, nz, nq
         self.C = 4 * nq
         self.interval_steps = interval_steps
         p = _FnoParams(nx, ny, nz, nq, width, modes, layers, hidden, max_batch, device, seed, interval_steps,
-                       int(physics_mean))
+                       int(physics_mean), GEMM_PATHS[gemm_path])
         m = ctypes.c_void_p()
         st = lib().rbc_fno_create(ctypes.byref(p), ctypes.byref(m))
         if st != RBC_OK:

@@ -19,6 +19,7 @@
 // R_l [2m][m][2][W][W] (ky index, kx, re/im, in, out); Q1 [H][W], q1 [H]; Q2 [C][H], q2 [C].
 #include "rbc.h"
 #include "fno_kernels.cuh"
+#include "gemm_tc.cuh"
 #include "galerkin.h"
 #include "solver_internal.h"
 #include "splitmix.h"
@@ -91,6 +92,7 @@ struct rbc_fno {
     int dloss_n = 0;
     float* skbuf = nullptr;   // split-K slices of one-batch GEMMs
     size_t skcap = 0;
+    int* tc_err = nullptr;    // error word of the tensor-core GEMMs (null: mma.sync tiles only)
     // solver coupling
     double *basis = nullptr, *proj = nullptr;
     void* dec = nullptr;
@@ -140,6 +142,19 @@ rbc_status ffail(rbc_fno* f, rbc_status s, const std::string& m)
     return s;
 }
 
+// Reads (and clears) the error word of the tensor-core GEMMs after the caller's stream
+// has been synchronised: a bounded wait inside one of them gave up.
+rbc_status tc_check(rbc_fno* f)
+{
+    if (!f->tc_err) return RBC_OK;
+    int e = 0;
+    if (cudaMemcpy(&e, f->tc_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return ffail(f, RBC_ERR_CUDA, "reading the tensor-core GEMM error word failed");
+    if (!e) return RBC_OK;
+    cudaMemset(f->tc_err, 0, sizeof(int));
+    return ffail(f, RBC_ERR_CUDA, "a tensor-core GEMM wait gave up (accumulator not committed)");
+}
+
 #define FNO_GUARD(f)                                                                     \
     if (!f) return RBC_ERR_INVALID_ARG;                                                  \
     try {                                                                                \
@@ -163,8 +178,48 @@ int load_mode(const bf16* base, long long rs, long long cs, long long bs, int ro
 }
 
 constexpr int kSMs = 148;
-void launch_gemm(cudaStream_t s, const GemmOp& op, int BM, int BN)
+
+// The tensor-core (tcgen05) GEMM serves products whose A rows are K-contiguous (load mode
+// 2), with N <= 256 and at least one full 128-row tile; tc_err null selects the mma.sync
+// tiles for every product.
+bool tc_eligible(const GemmOp& op, const int* tc_err)
 {
+    return tc_err && op.amode == 2 && op.N <= kTcNmax && op.M >= kTcM;
+}
+
+int tc_cols(int N)
+{
+    const int n16 = (N + 15) & ~15;
+    return n16 <= 32 ? 32 : n16 <= 64 ? 64 : n16 <= 128 ? 128 : 256;
+}
+
+void set_tc_attributes()
+{
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(32)));
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(64)));
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(128)));
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(256)));
+}
+
+void launch_gemm_tc(cudaStream_t s, const GemmOp& op, int* tc_err)
+{
+    dim3 grid((op.M + kTcM - 1) / kTcM, 1, op.batch);
+    const size_t sm = gemm_tc_smem((op.N + 15) & ~15);
+    switch (tc_cols(op.N)) {
+    case 32: k_gemm_tc<32><<<grid, 128, sm, s>>>(op, tc_err); break;
+    case 64: k_gemm_tc<64><<<grid, 128, sm, s>>>(op, tc_err); break;
+    case 128: k_gemm_tc<128><<<grid, 128, sm, s>>>(op, tc_err); break;
+    default: k_gemm_tc<256><<<grid, 128, sm, s>>>(op, tc_err); break;
+    }
+    FNO_CUDA(cudaGetLastError());
+}
+
+void launch_gemm(cudaStream_t s, const GemmOp& op, int BM, int BN, int* tc_err = nullptr)
+{
+    if (tc_eligible(op, tc_err)) {
+        launch_gemm_tc(s, op, tc_err);
+        return;
+    }
     dim3 grid((op.M + BM - 1) / BM, (op.N + BN - 1) / BN, op.batch);
     if (grid.y > 65535) throw ArgErr{"gemm N too large"};
     if (BM == 32 && BN == 32) k_gemm<32, 32><<<grid, 128, 0, s>>>(op);
@@ -179,7 +234,7 @@ void launch_gemm(cudaStream_t s, const GemmOp& op, int BM, int BN)
 // the one with the most CTAs. A one-batch product with too few CTAs and a plain store
 // epilogue is split along K into FP32 slices (scratch splitk, cap floats) summed in order
 // by k_splitk_finish.
-void gemm_on(cudaStream_t s, GemmOp op, float* splitk, size_t cap)
+void gemm_on(cudaStream_t s, GemmOp op, float* splitk, size_t cap, int* tc_err = nullptr)
 {
     if (op.batch < 1 || op.batch > 65535 || op.M < 1 || op.N < 1 || op.K < 1) throw ArgErr{"gemm shape"};
     // split-K chunks start at multiples of K: 16-byte loads along k need K and ktot % 8 == 0
@@ -231,7 +286,7 @@ void gemm_on(cudaStream_t s, GemmOp op, float* splitk, size_t cap)
             const long long kc8 = (Kc % 8 == 0 && op.K % 8 == 0) ? 8 : 1;
             p.amode = load_mode(p.A, p.a_rs, p.a_cs, p.a_bs, p.M, kc8);
             p.bmode = load_mode(p.B, p.b_cs, p.b_rs, p.b_bs, p.N, kc8);
-            launch_gemm(s, p, BM, BN);
+            launch_gemm(s, p, BM, BN, tc_err);
             const long long mn = (long long)op.M * op.N;
             k_splitk_finish<<<(int)std::min<long long>((mn + 255) / 256, 4 * kSMs), 256, 0, s>>>(
                 splitk, S, op.M, op.N, op.c_rs, op.c_cs, op.outf, op.outb);
@@ -239,10 +294,10 @@ void gemm_on(cudaStream_t s, GemmOp op, float* splitk, size_t cap)
             return;
         }
     }
-    launch_gemm(s, op, BM, BN);
+    launch_gemm(s, op, BM, BN, tc_err);
 }
 
-void gemm(rbc_fno* f, cudaStream_t s, const GemmOp& op) { gemm_on(s, op, f->skbuf, f->skcap); }
+void gemm(rbc_fno* f, cudaStream_t s, const GemmOp& op) { gemm_on(s, op, f->skbuf, f->skcap, f->tc_err); }
 
 int grid_1d(long long n, int threads = 256, int cap = 148 * 8)
 {
@@ -610,7 +665,7 @@ rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out)
     if (p->nx < 8 || p->ny < 8 || p->nq < 1 || p->nz < 1 || p->nq < p->nz || p->width < 8 || p->width > 64 ||
         p->width % 8 || p->modes < 1 || 2 * p->modes > p->nx - 2 || 2 * p->modes > p->ny || p->layers < 1 ||
         p->hidden < 8 || p->hidden > 256 || p->max_batch < 1 || 4 * p->nq > 256 || p->interval_steps < 1 ||
-        3 * p->nz > 64)
+        3 * p->nz > 64 || p->gemm_path < 0 || p->gemm_path > 1)
         return RBC_ERR_INVALID_ARG;
     rbc_fno* f = new rbc_fno;
     f->p = *p;
@@ -695,6 +750,11 @@ rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out)
         f->lpart = falloc<float>(f, f->nloss_blocks);
         f->skcap = (size_t)1 << 20;
         f->skbuf = falloc<float>(f, f->skcap);
+        if (p->gemm_path == 0) {
+            set_tc_attributes();
+            f->tc_err = falloc<int>(f, 1);
+            FNO_CUDA(cudaMemset(f->tc_err, 0, sizeof(int)));
+        }
         f->dloss_n = 1 << 16;
         f->dloss = falloc<double>(f, f->dloss_n);
         // solver coupling (grids with nz vertical modes)
@@ -833,7 +893,7 @@ rbc_status rbc_fno_forward(rbc_fno* f, const float* x, int batch, float* y)
     forward(f, batch, f->stream);
     FNO_CUDA(cudaMemcpyAsync(y, f->out, n * sizeof(float), cudaMemcpyDeviceToHost, f->stream));
     FNO_CUDA(cudaStreamSynchronize(f->stream));
-    return RBC_OK;
+    return tc_check(f);
     FNO_GUARD_END(f)
 }
 
@@ -852,7 +912,7 @@ rbc_status rbc_fno_loss_grad(rbc_fno* f, const float* x, const float* target, in
     FNO_CUDA(cudaMemcpyAsync(loss, f->dloss, sizeof(double), cudaMemcpyDeviceToHost, f->stream));
     FNO_CUDA(cudaMemcpyAsync(grad, f->grad, f->nparam * sizeof(float), cudaMemcpyDeviceToHost, f->stream));
     FNO_CUDA(cudaStreamSynchronize(f->stream));
-    return RBC_OK;
+    return tc_check(f);
     FNO_GUARD_END(f)
 }
 
@@ -1050,7 +1110,7 @@ rbc_status rbc_fno_train(rbc_fno* f, const int* src, const int* dst, int npairs,
         epoch_loss[e] = m / iters;
     }
     FNO_CUDA(cudaStreamSynchronize(s));
-    return RBC_OK;
+    return tc_check(f);
     FNO_GUARD_END(f)
 }
 
@@ -1074,7 +1134,7 @@ rbc_status rbc_fno_advance(rbc_fno* f, rbc_handle* h, int n)
     f->have_prev = false;
     for (int i = 0; i < n; ++i) advance_once(f, h);
     FNO_CUDA(cudaStreamSynchronize(rbcint::stream(h)));
-    return RBC_OK;
+    return tc_check(f);
     FNO_GUARD_END(f)
 }
 
@@ -1149,8 +1209,53 @@ rbc_status rbc_surrogate_run(rbc_fno* f, rbc_handle* h, const rbc_surrogate_para
     check_status(rbc_synchronize(h), h);
     if (nu_trace && sp->intervals > 0)
         FNO_CUDA(cudaMemcpy(nu_trace, f->trace, sp->intervals * sizeof(double), cudaMemcpyDeviceToHost));
-    return RBC_OK;
+    return tc_check(f);
     FNO_GUARD_END(f)
+}
+
+rbc_status rbc_gemm_bf16(int device, const void* A, const void* B, float* C, int M, int N, int K, int path,
+                         void* stream)
+{
+    if (!A || !B || !C || M < 1 || N < 1 || K < 1 || path < 0 || path > 1) return RBC_ERR_INVALID_ARG;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return RBC_ERR_CUDA;
+    rbc_status st = RBC_OK;
+    int* err = nullptr;
+    try {
+        cudaStream_t s = (cudaStream_t)stream;
+        GemmOp op;
+        op.A = static_cast<const bf16*>(A);
+        op.a_rs = K;
+        op.a_cs = 1;
+        op.B = static_cast<const bf16*>(B);
+        op.b_rs = N;
+        op.b_cs = 1;
+        op.M = M;
+        op.N = N;
+        op.K = K;
+        op.c_rs = N;
+        op.c_cs = 1;
+        op.outf = C;
+        if (path == 0) {
+            set_tc_attributes();
+            FNO_CUDA(cudaMalloc(&err, sizeof(int)));
+            FNO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+        }
+        gemm_on(s, op, nullptr, 0, err);
+        FNO_CUDA(cudaStreamSynchronize(s));
+        if (err) {
+            int e = 0;
+            FNO_CUDA(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
+            if (e) st = RBC_ERR_CUDA;
+        }
+    } catch (const CudaErr&) {
+        st = RBC_ERR_CUDA;
+    } catch (const ArgErr&) {
+        st = RBC_ERR_INVALID_ARG;
+    }
+    if (err) cudaFree(err);
+    cudaSetDevice(prev);
+    return st;
 }
 
 } // extern "C"
