@@ -180,11 +180,13 @@ int load_mode(const bf16* base, long long rs, long long cs, long long bs, int ro
 constexpr int kSMs = 148;
 
 // The tensor-core (tcgen05) GEMM serves products whose A rows are K-contiguous (load mode
-// 2), with N <= 256 and at least one full 128-row tile; tc_err null selects the mma.sync
-// tiles for every product.
+// 2), with N <= 256 and at least two waves of 128-row tiles (a CTA runs its staging, MMAs and
+// epilogue in turn; smaller products keep more CTAs in flight on the mma.sync tiles); tc_err
+// null selects the mma.sync tiles for every product.
 bool tc_eligible(const GemmOp& op, const int* tc_err)
 {
-    return tc_err && op.amode == 2 && op.N <= kTcNmax && op.M >= kTcM;
+    const long long tiles = (long long)((op.M + kTcM - 1) / kTcM) * op.batch;
+    return tc_err && op.amode == 2 && op.N <= kTcNmax && op.M >= kTcM && tiles >= 2 * kSMs;
 }
 
 int tc_cols(int N)
@@ -1220,6 +1222,7 @@ rbc_status rbc_gemm_bf16(int device, const void* A, const void* B, float* C, int
     int prev = -1;
     if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return RBC_ERR_CUDA;
     rbc_status st = RBC_OK;
+    static int* err_words[64] = {nullptr}; // one error word per device, kept for the process
     int* err = nullptr;
     try {
         cudaStream_t s = (cudaStream_t)stream;
@@ -1237,11 +1240,18 @@ rbc_status rbc_gemm_bf16(int device, const void* A, const void* B, float* C, int
         op.c_cs = 1;
         op.outf = C;
         if (path == 0) {
+            // the tensor-core kernel for every size it can take (partial tiles included)
+            op.amode = load_mode(op.A, op.a_rs, op.a_cs, op.a_bs, op.M, op.K);
+            if (op.amode != 2 || op.N > kTcNmax) throw ArgErr{"shape not supported by the tensor-core GEMM"};
+            if (device < 0 || device >= 64) throw ArgErr{"device ordinal"};
             set_tc_attributes();
-            FNO_CUDA(cudaMalloc(&err, sizeof(int)));
+            if (!err_words[device]) FNO_CUDA(cudaMalloc(&err_words[device], sizeof(int)));
+            err = err_words[device];
             FNO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+            launch_gemm_tc(s, op, err);
+        } else {
+            gemm_on(s, op, nullptr, 0, nullptr);
         }
-        gemm_on(s, op, nullptr, 0, err);
         FNO_CUDA(cudaStreamSynchronize(s));
         if (err) {
             int e = 0;
@@ -1253,7 +1263,6 @@ rbc_status rbc_gemm_bf16(int device, const void* A, const void* B, float* C, int
     } catch (const ArgErr&) {
         st = RBC_ERR_INVALID_ARG;
     }
-    if (err) cudaFree(err);
     cudaSetDevice(prev);
     return st;
 }

@@ -11,8 +11,10 @@
 //   - one elected thread issues 4 tcgen05.mma kind::f16 (M = 128, N, K = 16; BF16 inputs,
 //     FP32 accumulate) into a TMEM accumulator of 128 lanes x N columns and commits them to
 //     an mbarrier, which the CTA waits on before the chunk's shared memory is reused;
-//   - the epilogue warps read their 32 rows of the accumulator with tcgen05.ld (warp w owns
-//     TMEM lanes 32 w .. 32 w + 31) and apply the epilogue of GemmOp.
+//   - per 32 output columns, each warp reads its 32 rows of the accumulator with tcgen05.ld
+//     (warp w owns TMEM lanes 32 w .. 32 w + 31) into a shared [128][33] tile, and the CTA
+//     applies the epilogue of GemmOp walking the tile row by row, so that consecutive threads
+//     read and write consecutive outputs.
 // Every wait is bounded (kMbarSpins polls); a wait that gives up sets *err and the kernel
 // still frees its TMEM. TMEM is allocated by warp 0 (power-of-two columns >= 32) and freed
 // by warp 0 on every path.
@@ -105,9 +107,11 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmOp op, int* err)
     unsigned phase = 0;
     bool ok = true;
     for (int k0 = 0; k0 < K; k0 += kTcKC) {
+        // K = 16 steps of this chunk that carry data (the rest of the chunk is not read)
+        const int nk = min(kTcKC / 16, (K - k0 + 15) / 16), kw = 16 * nk;
         // A tile: row-major K-contiguous rows, 16-byte loads of 8 elements
-        for (int i = threadIdx.x; i < kTcM * (kTcKC / 8); i += blockDim.x) {
-            const int r = i / (kTcKC / 8), kc = (i - r * (kTcKC / 8)) * 8;
+        for (int i = threadIdx.x; i < kTcM * (kw / 8); i += blockDim.x) {
+            const int r = i / (kw / 8), kc = (i - r * (kw / 8)) * 8;
             const int gr = m0 + r, gk = k0 + kc;
             uint4 v = make_uint4(0, 0, 0, 0);
             if (gr < op.M && gk < K) {
@@ -120,9 +124,10 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmOp op, int* err)
             }
             *reinterpret_cast<uint4*>(As + tc_off(r, kc)) = v;
         }
-        // B^T tile: element (n, k) = B[k b_rs + n b_cs]
-        for (int i = threadIdx.x; i < N16 * kTcKC; i += blockDim.x) {
-            const int n = i / kTcKC, k = i - n * kTcKC;
+        // B^T tile: element (n, k) = B[k b_rs + n b_cs]; consecutive threads take
+        // consecutive n (the weights' rows are n-contiguous)
+        for (int i = threadIdx.x; i < N16 * kw; i += blockDim.x) {
+            const int k = i / N16, n = i - k * N16;
             const int gk = k0 + k;
             Bs[tc_off(n, k)] = (n < op.N && gk < K) ? B[gk * op.b_rs + n * op.b_cs] : zero;
         }
@@ -132,8 +137,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmOp op, int* err)
         tc_fence_after();
         if (threadIdx.x == 0) {
             const unsigned a0 = smem_u32(As), b0 = smem_u32(Bs);
-#pragma unroll
-            for (int kk = 0; kk < kTcKC / 16; ++kk) {
+            for (int kk = 0; kk < nk; ++kk) {
                 // K = 16 covers two core matrices along K (128 bytes apart): +256 bytes per step
                 const uint64_t ad = umma_desc(a0 + kk * 256, 128, (kTcKC / 8) * 128);
                 const uint64_t bd = umma_desc(b0 + kk * 256, 128, (kTcKC / 8) * 128);
@@ -161,42 +165,39 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmOp op, int* err)
         if (threadIdx.x == 0) atomicOr(err, RBC_DEVERR_TIMEOUT);
         mbar_wait_parity(mbar, phase ^ 1);
     }
-    // epilogue: this thread's row m of the accumulator, 16 columns per tcgen05.ld
-    const int m = m0 + threadIdx.x;
+    // epilogue, 32 columns at a time: each warp moves its 32 accumulator rows from TMEM into
+    // a shared [128][33] tile (the A/B staging area, free now), then the CTA walks the tile in
+    // row-major order so that consecutive threads touch consecutive outputs (and addends)
+    float* T = reinterpret_cast<float*>(base);
     const long long cz = (long long)z * op.c_bs;
     const unsigned lane_base = (unsigned)(warp * 32) << 16;
-    if (ok && K > 0) {
-        for (int c0 = 0; c0 < N16; c0 += 16) {
-            uint32_t r[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                : "r"(tmem + lane_base + (unsigned)c0)
-                : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-            if (m < op.M) {
+    for (int c0 = 0; c0 < N16; c0 += 32) {
+        const int cw = min(32, N16 - c0);
+        if (ok && K > 0) {
+            for (int h = 0; h < cw; h += 16) {
+                uint32_t r[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];\n"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15])
+                    : "r"(tmem + lane_base + (unsigned)(c0 + h))
+                    : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int n = c0 + j;
-                    if (n >= op.N) break;
-                    const long long o = cz + m * op.c_rs + n * op.c_cs;
-                    float v = __uint_as_float(r[j]) * op.alpha;
-                    if (op.bias) v += op.bias[n];
-                    if (op.add) v += op.add[o];
-                    if (op.pre) op.pre[o] = v;
-                    if (op.act == ACT_GELU) v = gelu(v);
-                    else if (op.act == ACT_GELU_BWD) v *= gelu_grad(op.aux[o]);
-                    if (op.outf) op.outf[o] = v;
-                    if (op.outb) op.outb[o] = __float2bfloat16_rn(v);
-                }
+                for (int j = 0; j < 16; ++j) T[threadIdx.x * 33 + h + j] = __uint_as_float(r[j]);
             }
+        } else {
+            for (int j = 0; j < cw; ++j) T[threadIdx.x * 33 + j] = 0.0f; // an empty split-K slice
         }
-    } else if (K <= 0 && m < op.M) {
-        // an empty split-K slice: the product is zero
-        for (int n = 0; n < op.N; ++n) {
-            const long long o = cz + m * op.c_rs + n * op.c_cs;
-            float v = 0.0f;
+        __syncthreads();
+        for (int e = threadIdx.x; e < kTcM * cw; e += blockDim.x) {
+            const int rr = e / cw, j = e - rr * cw;
+            const int mm = m0 + rr, n = c0 + j;
+            if (mm >= op.M || n >= op.N) continue;
+            const long long o = cz + mm * op.c_rs + n * op.c_cs;
+            float v = T[rr * 33 + j] * op.alpha;
             if (op.bias) v += op.bias[n];
             if (op.add) v += op.add[o];
             if (op.pre) op.pre[o] = v;
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmOp op, int* err)
             if (op.outf) op.outf[o] = v;
             if (op.outb) op.outb[o] = __float2bfloat16_rn(v);
         }
+        __syncthreads();
     }
     tc_fence_before();
     __syncthreads();

@@ -256,3 +256,36 @@ def test_pushforward_and_augmented_training_run():
     assert np.all(np.isfinite(losses)) and losses[-5:].mean() < 0.7 * losses[:5].mean(), losses
     with pytest.raises(sdc_b200.RBCError):
         f.set_train_options(augment=3)
+
+
+NET_BIG = dict(nx=128, ny=128, nz=2, nq=2, width=16, modes=8, layers=2, hidden=32)
+
+
+def test_fno_tensor_core_path_matches_oracle():
+    """At 128^2 with batch 3 (49,152 rows, 384 row tiles) the channel-map products run on the
+    tcgen05 kernel: forward and gradient against the oracle with the bars above, and the two
+    GEMM paths agree with each other to BF16 resolution."""
+    b = 3
+    f = sdc_b200.FNO(NET_BIG["nx"], NET_BIG["ny"], NET_BIG["nz"], NET_BIG["nq"], width=NET_BIG["width"],
+                     modes=NET_BIG["modes"], layers=NET_BIG["layers"], hidden=NET_BIG["hidden"], max_batch=b, seed=5)
+    g = sdc_b200.FNO(NET_BIG["nx"], NET_BIG["ny"], NET_BIG["nz"], NET_BIG["nq"], width=NET_BIG["width"],
+                     modes=NET_BIG["modes"], layers=NET_BIG["layers"], hidden=NET_BIG["hidden"], max_batch=b, seed=5,
+                     gemm_path="mma_sync")
+    o = FNOOracle(NET_BIG["nx"], NET_BIG["ny"], 4 * NET_BIG["nq"], NET_BIG["width"], NET_BIG["modes"],
+                  NET_BIG["layers"], NET_BIG["hidden"], bf16=True)
+    v = f.get_params()
+    g.set_params(v)
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal((b, NET_BIG["ny"], NET_BIG["nx"], 4 * NET_BIG["nq"])).astype(np.float32)
+    t = rng.standard_normal(x.shape).astype(np.float32)
+    got, alt = f.forward(x), g.forward(x)
+    ref = o.forward(v.astype(np.float64), x)[0]
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-3
+    assert np.linalg.norm(got - alt) / np.linalg.norm(alt) < 2e-3
+    loss, gr = f.loss_grad(x, t)
+    lref, gref = o.loss_grad(v.astype(np.float64), x, t)
+    assert abs(loss - lref) <= 1e-4 * lref
+    gp, gq = o.unpack(gr), o.unpack(gref)
+    for name, _ in o.shapes:
+        e = np.linalg.norm(gp[name] - gq[name]) / max(np.linalg.norm(gq[name]), 1e-30)
+        assert e < 1e-2, (name, e)

@@ -55,3 +55,9 @@ def test_gemm_tc_consecutive_calls_and_bad_arguments():
     bad = sdc_b200.lib().rbc_gemm_bf16(0, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(B.data_ptr()),
                                        ctypes.c_void_p(C.data_ptr()), 384, 64, 64, 2, None)
     assert bad == 1
+    # N above the tensor-core limit
+    B2 = torch.randn((64, 272)).to(torch.bfloat16).cuda()
+    C2 = torch.zeros((384, 272), dtype=torch.float32, device="cuda")
+    bad2 = sdc_b200.lib().rbc_gemm_bf16(0, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(B2.data_ptr()),
+                                        ctypes.c_void_p(C2.data_ptr()), 384, 272, 64, 0, None)
+    assert bad2 == 1
