@@ -452,10 +452,10 @@ typedef struct {
 rbc_status rbc_fno_create(const rbc_fno_params* p, rbc_fno** out);
 /* BF16 GEMM of the surrogate's kernels on device buffers (no reference counterpart; the
  * numerics check of its tensor-core paths): C[M][N] (FP32, row-major) = A[M][K] B[K][N]
- * (BF16, row-major, FP32 accumulation). path 0: the tcgen05 kernel (N <= 256, K a multiple
- * of 8 and A 16-byte aligned, else RBC_ERR_INVALID_ARG), 1: mma.sync tiles. Work on `stream`
- * (NULL: legacy default stream), waited for before the call returns; RBC_ERR_CUDA if a
- * tensor-core wait gave up. */
+ * (BF16, row-major, FP32 accumulation). path 0: the tcgen05 kernel (TMA-staged A, TMEM
+ * accumulator; N <= 256, K <= 256 and a multiple of 8, A 16-byte aligned, B^T within 64 KB,
+ * else RBC_ERR_INVALID_ARG), 1: mma.sync tiles. Work on `stream` (NULL: legacy default
+ * stream), waited for before the call returns; RBC_ERR_CUDA if a tensor-core wait gave up. */
 rbc_status rbc_gemm_bf16(int device, const void* A, const void* B, float* C, int M, int N, int K, int path,
                          void* stream);
 void rbc_fno_destroy(rbc_fno* m);

@@ -20,6 +20,8 @@
 #include "rbc.h"
 #include "fno_kernels.cuh"
 #include "gemm_tc.cuh"
+
+#include <cudaTypedefs.h>
 #include "galerkin.h"
 #include "solver_internal.h"
 #include "splitmix.h"
@@ -180,13 +182,22 @@ int load_mode(const bf16* base, long long rs, long long cs, long long bs, int ro
 constexpr int kSMs = 148;
 
 // The tensor-core (tcgen05) GEMM serves products whose A rows are K-contiguous (load mode
-// 2), with N <= 256 and at least two waves of 128-row tiles (a CTA runs its staging, MMAs and
-// epilogue in turn; smaller products keep more CTAs in flight on the mma.sync tiles); tc_err
-// null selects the mma.sync tiles for every product.
+// 2), with one B for all batches, N <= 256, K <= 256 (B^T held in shared memory: at most
+// 64 KB), no split-K, and at least two waves of 128-row tiles (smaller products keep more
+// CTAs in flight on the mma.sync tiles); tc_err null selects the mma.sync tiles for every
+// product.
+bool tc_shape_ok(const GemmOp& op)
+{
+    const int n16 = (op.N + 15) & ~15, nchunk = (op.K + kTcKC - 1) / kTcKC;
+    return op.amode == 2 && op.N <= kTcNmax && op.K <= kTcKmax && op.ktot == 0 &&
+           (op.batch == 1 || op.b_bs == 0) && (size_t)nchunk * n16 * 128 <= 65536;
+}
 bool tc_eligible(const GemmOp& op, const int* tc_err)
 {
+    // products with N < 16 or K < 32 stay on the mma.sync tiles: measured faster there (their
+    // cost is the epilogue's stores, which the many CTAs of the tiles spread wider)
     const long long tiles = (long long)((op.M + kTcM - 1) / kTcM) * op.batch;
-    return tc_err && op.amode == 2 && op.N <= kTcNmax && op.M >= kTcM && tiles >= 2 * kSMs;
+    return tc_err && tc_shape_ok(op) && tiles >= 2 * kSMs && op.N >= 16 && op.K >= 32;
 }
 
 int tc_cols(int N)
@@ -195,33 +206,77 @@ int tc_cols(int N)
     return n16 <= 32 ? 32 : n16 <= 64 ? 64 : n16 <= 128 ? 128 : 256;
 }
 
+// One CTA per SM where two would not fit the TMEM (2 x 2 x 256 columns): the dynamic
+// shared memory asked for is then at least this much.
+constexpr size_t kTcSmemFloor = 116 * 1024;
+
 void set_tc_attributes()
 {
-    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(32)));
-    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(64)));
-    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(128)));
-    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_tc_smem(256)));
+    const int mx = (int)std::max<size_t>(kTcSmemFloor, gemm_tc_smem(kTcKmax / kTcKC, 128));
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FNO_CUDA(cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
 }
 
-void launch_gemm_tc(cudaStream_t s, const GemmOp& op, int* tc_err)
+// cuTensorMapEncodeTiled, from the driver through the runtime's entry-point query (no link
+// against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
-    dim3 grid((op.M + kTcM - 1) / kTcM, 1, op.batch);
-    const size_t sm = gemm_tc_smem((op.N + 15) & ~15);
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// Launches the tensor-core GEMM; false (nothing launched) when the tensor map of A cannot be
+// encoded, and the caller uses the mma.sync tiles.
+bool launch_gemm_tc(cudaStream_t s, const GemmOp& op, int* tc_err)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    CUtensorMap map;
+    const long long bs = op.batch > 1 ? op.a_bs : (long long)op.M * op.a_rs;
+    const cuuint64_t dims[3] = {(cuuint64_t)op.K, (cuuint64_t)op.M, (cuuint64_t)op.batch};
+    const cuuint64_t strides[2] = {(cuuint64_t)op.a_rs * sizeof(bf16), (cuuint64_t)bs * sizeof(bf16)};
+    const cuuint32_t box[3] = {(cuuint32_t)kTcKC, (cuuint32_t)kTcM, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(op.A), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    TcArgs a;
+    a.op = op;
+    a.err = tc_err;
+    a.mtiles = (op.M + kTcM - 1) / kTcM;
+    a.ntiles = a.mtiles * op.batch;
+    a.nchunk = (op.K + kTcKC - 1) / kTcKC;
+    a.n16 = (op.N + 15) & ~15;
+    auto al = [](const void* p, int b) { return p == nullptr || (uintptr_t)p % b == 0; };
+    a.vec4 = (op.c_cs == 1 && op.c_rs % 4 == 0 && op.c_bs % 4 == 0 && al(op.outf, 16) && al(op.pre, 16) &&
+              al(op.add, 16) && al(op.aux, 16) && al(op.bias, 16) && al(op.outb, 8)) ? 1 : 0;
+    // two CTAs per SM when their accumulators fit the TMEM together and their shared memory too
+    const bool two = tc_cols(op.N) <= 128 && gemm_tc_smem(a.nchunk, a.n16) <= 113 * 1024;
+    const size_t sm = two ? gemm_tc_smem(a.nchunk, a.n16) : std::max(kTcSmemFloor, gemm_tc_smem(a.nchunk, a.n16));
+    const int grid = std::min(a.ntiles, (two ? 2 : 1) * kSMs);
     switch (tc_cols(op.N)) {
-    case 32: k_gemm_tc<32><<<grid, 128, sm, s>>>(op, tc_err); break;
-    case 64: k_gemm_tc<64><<<grid, 128, sm, s>>>(op, tc_err); break;
-    case 128: k_gemm_tc<128><<<grid, 128, sm, s>>>(op, tc_err); break;
-    default: k_gemm_tc<256><<<grid, 128, sm, s>>>(op, tc_err); break;
+    case 32: k_gemm_tc<32><<<grid, kTcThreads, sm, s>>>(map, a); break;
+    case 64: k_gemm_tc<64><<<grid, kTcThreads, sm, s>>>(map, a); break;
+    case 128: k_gemm_tc<128><<<grid, kTcThreads, sm, s>>>(map, a); break;
+    default: k_gemm_tc<256><<<grid, kTcThreads, sm, s>>>(map, a); break;
     }
     FNO_CUDA(cudaGetLastError());
+    return true;
 }
 
 void launch_gemm(cudaStream_t s, const GemmOp& op, int BM, int BN, int* tc_err = nullptr)
 {
-    if (tc_eligible(op, tc_err)) {
-        launch_gemm_tc(s, op, tc_err);
-        return;
-    }
+    if (tc_eligible(op, tc_err) && launch_gemm_tc(s, op, tc_err)) return;
     dim3 grid((op.M + BM - 1) / BM, (op.N + BN - 1) / BN, op.batch);
     if (grid.y > 65535) throw ArgErr{"gemm N too large"};
     if (BM == 32 && BN == 32) k_gemm<32, 32><<<grid, 128, 0, s>>>(op);
@@ -1242,13 +1297,13 @@ rbc_status rbc_gemm_bf16(int device, const void* A, const void* B, float* C, int
         if (path == 0) {
             // the tensor-core kernel for every size it can take (partial tiles included)
             op.amode = load_mode(op.A, op.a_rs, op.a_cs, op.a_bs, op.M, op.K);
-            if (op.amode != 2 || op.N > kTcNmax) throw ArgErr{"shape not supported by the tensor-core GEMM"};
+            if (!tc_shape_ok(op)) throw ArgErr{"shape not supported by the tensor-core GEMM"};
             if (device < 0 || device >= 64) throw ArgErr{"device ordinal"};
             set_tc_attributes();
             if (!err_words[device]) FNO_CUDA(cudaMalloc(&err_words[device], sizeof(int)));
             err = err_words[device];
             FNO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-            launch_gemm_tc(s, op, err);
+            if (!launch_gemm_tc(s, op, err)) throw ArgErr{"the tensor map of A could not be encoded"};
         } else {
             gemm_on(s, op, nullptr, 0, nullptr);
         }
