@@ -76,10 +76,9 @@ RBC_D void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::
 RBC_D void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------------
-// Bulk asynchronous copies (sm_90+): one instruction moves a contiguous block of global
-// memory into shared memory through the copy engine, completing on an mbarrier by bytes.
-// Both addresses 16-byte aligned, size a multiple of 16. Every wait on an mbarrier is
-// bounded: after kMbarSpins failed polls it gives up and reports false.
+// mbarriers (sm_90+) for the asynchronous copy engine and the tensor cores: initialisation,
+// arrivals (with an expected transaction byte count), and the poll budget of every bounded
+// wait on one (kMbarSpins).
 RBC_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 RBC_D void mbar_init(unsigned long long* mbar, unsigned count)
 {
@@ -88,8 +87,8 @@ RBC_D void mbar_init(unsigned long long* mbar, unsigned count)
 // Makes initialised mbarriers visible to the copy engine (before the CTA barrier that
 // publishes them).
 RBC_D void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-// Orders this thread's earlier generic accesses of shared memory before later bulk copies
-// into it.
+// Orders this thread's earlier generic accesses of shared memory before later accesses by
+// the async proxy (copies into it, tensor-core reads of it).
 RBC_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 RBC_D void mbar_arrive(unsigned long long* mbar)
 {
@@ -100,25 +99,4 @@ RBC_D void mbar_arrive_expect_tx(unsigned long long* mbar, unsigned bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mbar)), "r"(bytes)
                  : "memory");
 }
-RBC_D void bulk_g2s(void* smem_dst, const void* gmem_src, unsigned bytes, unsigned long long* mbar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(smem_dst)),
-                 "l"(gmem_src), "r"(bytes), "r"(smem_u32(mbar))
-                 : "memory");
-}
 constexpr unsigned kMbarSpins = 1u << 22;
-// Waits until the phase with the given parity has completed; false after kMbarSpins polls.
-RBC_D bool mbar_wait_parity(unsigned long long* mbar, unsigned parity)
-{
-    const unsigned a = smem_u32(mbar);
-    for (unsigned i = 0; i < kMbarSpins; ++i) {
-        unsigned ok;
-        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(ok)
-                     : "r"(a), "r"(parity)
-                     : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
