@@ -762,26 +762,35 @@ def main():
     t0 = time.perf_counter()
     s.set_state(*host_state)
     s.tracers_set(host_tr)
-    # each step's diagnostics are read back while the next step is already queued
+    # steps are enqueued in chunks of 8 (the library's multi-step graph), the newest
+    # diagnostics of each chunk read back while the next chunk is already queued, and at
+    # the end every step's Nu_wall, Nu_vol and KE from the diagnostics ring
     prev = None
-    for _ in range(args.steps):
-        s.step_async(1)
+    done = nchunks = 0
+    while done < args.steps:
+        n = 8 if args.steps - done >= 8 else 1
+        s.step_async(n)
+        done += n
+        nchunks += 1
         t = s.diagnostics_async()
         if prev is not None:
-            s.diagnostics_get(prev)  # waits for that step only; reports a non-finite state
+            s.diagnostics_get(prev)  # waits for that chunk only; reports a non-finite state
         prev = t
     s.diagnostics_get(prev)
+    hist = s.diag_history(args.steps)
     s.get_state(out_state)
     s.tracers_get(out_tr)
     el = max_over_ranks(time.perf_counter() - t0, world, device="cuda")
+    assert hist.shape[0] == args.steps and np.all(np.isfinite(hist))
     state_bytes = sum(a.nbytes for a in host_state)
     tr_bytes = host_tr.nbytes
     e2e = {"value": world * args.steps * WORK["dt"] / el, "unit": "sim-time/s",
            "h2d_bytes_per_step": (state_bytes + tr_bytes) / args.steps,
-           "d2h_bytes_per_step": 36 + (state_bytes + tr_bytes) / args.steps,
+           "d2h_bytes_per_step": (state_bytes + tr_bytes + 36 * nchunks + 32 * args.steps) / args.steps,
            "host_buffers": "pinned (cudaHostAlloc through torch)",
-           "includes": "set_state + tracers_set, K x (rbc_step_async(1) + rbc_diagnostics_async, then "
-                       "rbc_diagnostics_get of the step before), get_state + tracers_get"}
+           "includes": "set_state + tracers_set, rbc_step_async in chunks of 8 steps (1 for the rest) each "
+                       "followed by rbc_diagnostics_async and rbc_diagnostics_get of the chunk before, "
+                       "rbc_diag_history of every step, get_state + tracers_get"}
     d = s.diagnostics()
     assert np.isfinite(d["ke"]) and np.all(np.isfinite(out_tr)) and all(np.all(np.isfinite(a)) for a in out_state)
 
