@@ -593,7 +593,7 @@ static void tracer_setup(rbc_handle* h)
     RBC_CUDA(cudaMemcpy(h->zbasis, zb.data(), zb.size() * sizeof(double), cudaMemcpyHostToDevice));
     h->trpos = dalloc<double>(3 * (size_t)h->ntr, h->owned);
     const size_t rsz = h->mixed ? sizeof(float) : sizeof(double);
-    h->nv = dalloc<unsigned char>((size_t)h->G.P * ((5 * L + 1) & ~1) * rsz, h->owned);
+    h->nv = dalloc<unsigned char>((size_t)h->G.P * node_rec_len(L) * rsz, h->owned);
     RBC_CUDA(cudaMemset(h->trpos, 0, 3 * (size_t)h->ntr * sizeof(double)));
     h->trsums = dalloc<double>(4, h->owned);
     h->tr_step = dalloc<long long>(1, h->owned);
@@ -672,7 +672,9 @@ template <typename R, int L> static void launch_tracer_L(rbc_handle* h)
     A.track_cap = h->trk_cap;
     A.track_period = h->trk_period;
     StageScope sc(h, ST_TRACER);
-    k_tracers<R, L><<<(4 * h->ntr + 127) / 128, 128, 0, h->stream>>>(A); // 4 lanes per tracer
+    // 8 lanes per tracer; each team's 4 corner records in shared memory
+    k_tracers<R, L><<<(8 * h->ntr + kTracerThreads - 1) / kTracerThreads, kTracerThreads, tracer_smem<R, L>(),
+                      h->stream>>>(A);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -739,6 +741,12 @@ static void flush_tracers(rbc_handle* h, bool overlap = false)
     else flush_tracers_t<double>(h, overlap);
 }
 
+template <typename R, int L> static void set_tracer_attribute(rbc_handle*)
+{
+    RBC_CUDA(cudaFuncSetAttribute(k_tracers<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tracer_smem<R, L>()));
+}
+
 // The dynamic shared-memory limit is an attribute of the kernel, shared by every handle
 // in the process; it is set to the device's opt-in maximum (a cap only: occupancy follows
 // the size each launch asks for), so handles of different shapes can run side by side.
@@ -761,6 +769,7 @@ template <typename R> static void set_attributes(rbc_handle* h)
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    if (h->prm.n_tracers > 0) RBC_DISPATCH_L(set_tracer_attribute, R, h->G.L, h);
 }
 
 // ------------------------------------------------------------------ autotuner

@@ -23,6 +23,18 @@ template <typename C> RBC_HD C cconj(C a) { a.y = -a.y; return a; }
 // multiply by i*s
 template <typename C, typename R> RBC_HD C cmul_is(C a, R s) { C r; r.x = -s * a.y; r.y = s * a.x; return r; }
 
+// One node record of the tracer velocity array: the 5 L velocity-field values u11, u21,
+// u31, u12, u22 of a grid point in two halves, modes i < LH and i >= LH (LH = ceil(L/2)).
+// Each half lists its modes' five values mode by mode and is padded to an even count, so
+// that in FP64 every half starts on a 16-byte boundary: one tracer lane reads one half.
+template <int L> struct NodeRec {
+    static constexpr int LH = (L + 1) / 2;
+    static constexpr int HALF = (5 * LH + 1) & ~1;
+    static constexpr int value = 2 * HALF;
+    static RBC_HD constexpr int at(int f, int i) { return (i / LH) * HALF + (i % LH) * 5 + f; }
+};
+RBC_HD constexpr int node_rec_len(int L) { return 2 * ((5 * ((L + 1) / 2) + 1) & ~1); }
+
 // Error word written by kernels that detect a violated precondition (never traps).
 enum rbc_dev_error { RBC_DEVERR_NONE = 0, RBC_DEVERR_BOUNDS = 1, RBC_DEVERR_NAN = 2, RBC_DEVERR_TIMEOUT = 4 };
 

@@ -61,32 +61,41 @@ RBC_D void contract_mode(const R (&in)[rbcprog::NFIELD][L], const R* __restrict_
     for (int gi = 0; gi < rbcprog::NGROUP; ++gi) grp[((size_t)gi * L + k) * P + x] = acc[gi];
 }
 
-// Length of one node record of the tracer velocity array: the 5 L velocity-field values
-// u11, u21, u31, u12, u22 of a grid point, padded to an even count (16-byte records).
-template <int L> struct NodeRec { static constexpr int value = (5 * L + 1) & ~1; };
+// Writes point x's node record (fields 0..4 of `in`, pads zero) with 8- or 16-byte stores.
+template <typename R, int L, typename In>
+RBC_D void store_node_record(const In& in, R* __restrict__ nv, size_t x)
+{
+    constexpr int NR = NodeRec<L>::value;
+    typedef typename cplx_t<R>::type R2;
+    R rec[NR];
+#pragma unroll
+    for (int e = 0; e < NR; ++e) rec[e] = 0;
+#pragma unroll
+    for (int f = 0; f < 5; ++f)
+#pragma unroll
+        for (int i = 0; i < L; ++i) rec[NodeRec<L>::at(f, i)] = in[f][i];
+    R2* dst = reinterpret_cast<R2*>(nv + x * NR);
+#pragma unroll
+    for (int q = 0; q < NR / 2; ++q) {
+        R2 v;
+        v.x = rec[2 * q];
+        v.y = rec[2 * q + 1];
+        dst[q] = v;
+    }
+}
 
 // The node records alone (no contraction): the tracer advance that runs on a state no
 // step will start from (a state about to be changed between steps) needs only these.
 template <typename R, int L>
 __global__ void __launch_bounds__(256) k_node_records(const R* __restrict__ phys, int P, R* __restrict__ nv)
 {
-    constexpr int NR = NodeRec<L>::value;
-    typedef typename cplx_t<R>::type R2;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < P; x += gridDim.x * blockDim.x) {
-        R rec[NR];
+        R in[5][L];
 #pragma unroll
         for (int f = 0; f < 5; ++f)
 #pragma unroll
-            for (int i = 0; i < L; ++i) rec[f * L + i] = phys[((size_t)f * L + i) * P + x];
-        if (NR > 5 * L) rec[NR - 1] = 0;
-        R2* dst = reinterpret_cast<R2*>(nv + (size_t)x * NR);
-#pragma unroll
-        for (int q = 0; q < NR / 2; ++q) {
-            R2 v;
-            v.x = rec[2 * q];
-            v.y = rec[2 * q + 1];
-            dst[q] = v;
-        }
+            for (int i = 0; i < L; ++i) in[f][i] = phys[((size_t)f * L + i) * P + x];
+        store_node_record<R, L>(in, nv, (size_t)x);
     }
 }
 
@@ -110,24 +119,7 @@ __global__ void __launch_bounds__(128) k_contract(const R* __restrict__ phys, R*
         for (int f = 0; f < rbcprog::NFIELD; ++f)
 #pragma unroll
             for (int i = 0; i < L; ++i) in[f][i] = ld_cg(phys + ((size_t)f * L + i) * P + x);
-        if (nv) {
-            constexpr int NR = NodeRec<L>::value;
-            typedef typename cplx_t<R>::type R2;
-            R rec[NR];
-#pragma unroll
-            for (int f = 0; f < 5; ++f)
-#pragma unroll
-                for (int i = 0; i < L; ++i) rec[f * L + i] = in[f][i];
-            if (NR > 5 * L) rec[NR - 1] = 0;
-            R2* dst = reinterpret_cast<R2*>(nv + (size_t)x * NR);
-#pragma unroll
-            for (int q = 0; q < NR / 2; ++q) {
-                R2 v;
-                v.x = rec[2 * q];
-                v.y = rec[2 * q + 1];
-                dst[q] = v;
-            }
-        }
+        if (nv) store_node_record<R, L>(in, nv, (size_t)x);
         for (int k = 0; k < L; k += 2) {
             contract_mode<R, L, 0>(in, coef, k, grp, P, x);
             if (k + 1 < L) contract_mode<R, L, 1>(in, coef, k + 1, grp, P, x);

@@ -36,47 +36,54 @@ struct TracerArgs {
     int track_cap, track_period;
 };
 
-template <int L> struct NodeRecLen { static constexpr int value = (5 * L + 1) & ~1; };
-
-// Loads the node record of grid point xy into registers.
+// Loads half `hf` of the node record of grid point xy into registers (NodeRec layout:
+// modes i in [hf LH, hf LH + LH), five values per mode). Records are written by the
+// contraction of the same step, which has completed before the tracer kernel starts.
 template <typename R, int L>
-RBC_D void load_record(const R* __restrict__ nv, size_t xy, R (&rec)[NodeRecLen<L>::value])
+RBC_D void load_half_record(const R* __restrict__ nv, size_t xy, int hf, R (&rec)[NodeRec<L>::HALF])
 {
-    constexpr int NR = NodeRecLen<L>::value;
+    constexpr int HALF = NodeRec<L>::HALF;
     typedef typename cplx_t<R>::type R2;
-    const R2* src = reinterpret_cast<const R2*>(nv + xy * NR);
+    const R2* src = reinterpret_cast<const R2*>(nv + xy * NodeRec<L>::value + (size_t)hf * HALF);
 #pragma unroll
-    for (int q = 0; q < NR / 2; ++q) {
+    for (int q = 0; q < HALF / 2; ++q) {
         const R2 v = __ldg(src + q);
         rec[2 * q] = v.x;
         rec[2 * q + 1] = v.y;
     }
 }
 
-// Velocity (u, v, w) of a node on the levels z0 and z1 from its record.
+// This half's share of the velocity (u, v, w) of a node on the levels zb0 and zb1 (rows of
+// the [128][3][L] basis table: C_i, S_i, C'_i) from its half record.
 template <typename R, int L>
-RBC_D void node_velocity(const R* rec, const double* zb0, const double* zb1, double (&u0)[3], double (&u1)[3])
+RBC_D void half_node_velocity(const R (&rec)[NodeRec<L>::HALF], int hf, const double* __restrict__ zb0,
+                              const double* __restrict__ zb1, double (&u0)[3], double (&u1)[3])
 {
+    constexpr int LH = NodeRec<L>::LH;
     double a0 = 0, b0 = 0, c0 = 0, a1 = 0, b1 = 0, c1 = 0;
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-        const double v11 = rec[i], v21 = rec[L + i], v31 = rec[2 * L + i], v12 = rec[3 * L + i], v22 = rec[4 * L + i];
-        const double C0 = zb0[i], S0 = zb0[L + i], D0 = zb0[2 * L + i];
-        const double C1 = zb1[i], S1 = zb1[L + i], D1 = zb1[2 * L + i];
-        a0 += D0 * v11 + S0 * v12;
-        b0 += D0 * v21 + S0 * v22;
-        c0 += C0 * v31;
-        a1 += D1 * v11 + S1 * v12;
-        b1 += D1 * v21 + S1 * v22;
-        c1 += C1 * v31;
+    for (int ii = 0; ii < LH; ++ii) {
+        const int i = hf * LH + ii;
+        if (i < L) { // the second half of an odd L has one mode less
+            const double v11 = rec[5 * ii], v21 = rec[5 * ii + 1], v31 = rec[5 * ii + 2];
+            const double v12 = rec[5 * ii + 3], v22 = rec[5 * ii + 4];
+            const double C0 = __ldg(zb0 + i), S0 = __ldg(zb0 + L + i), D0 = __ldg(zb0 + 2 * L + i);
+            const double C1 = __ldg(zb1 + i), S1 = __ldg(zb1 + L + i), D1 = __ldg(zb1 + 2 * L + i);
+            a0 += D0 * v11 + S0 * v12;
+            b0 += D0 * v21 + S0 * v22;
+            c0 += C0 * v31;
+            a1 += D1 * v11 + S1 * v12;
+            b1 += D1 * v21 + S1 * v22;
+            c1 += C1 * v31;
+        }
     }
     u0[0] = a0; u0[1] = b0; u0[2] = c0;
     u1[0] = a1; u1[1] = b1; u1[2] = c1;
 }
 
-// Cell of (x, y, z) as the reference's vel_interpolate finds it, for corner lane q of a team
-// of 4 (lane q takes the xy corner (q & 1, q >> 1)): the corner's node, the two bracketing
-// levels and the lane's trilinear weights.
+// Cell of (x, y, z) as the reference's vel_interpolate finds it, for the xy corner
+// (q & 1, q >> 1): the corner's node, the two bracketing levels and the corner's trilinear
+// weights.
 struct Corner {
     int node, iz0, iz1;
     double w, wz0, wz1;
@@ -110,42 +117,6 @@ RBC_D Corner find_corner(const TracerArgs& A, int q, double x, double y, double 
     c.w = ((q & 1) ? wx1 : wx0) * ((q >> 1) ? wy1 : wy0);
     c.node = iy * xs + ix;
     return c;
-}
-
-// The team's interpolated velocity from this lane's corner record: the node evaluated at
-// the two levels, weighted, and the 4 contributions added with two shuffle rounds; every
-// lane of the team returns the sum.
-template <typename R, int L>
-RBC_D void team_velocity(const Corner& c, const R* rec, const double* zb, double& rx, double& ry, double& rz)
-{
-    double u0[3], u1[3];
-    node_velocity<R, L>(rec, zb + (size_t)c.iz0 * 3 * L, zb + (size_t)c.iz1 * 3 * L, u0, u1);
-    double v[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        v[d] = c.w * (c.wz0 * u0[d] + c.wz1 * u1[d]);
-        v[d] += __shfl_xor_sync(0xffffffffu, v[d], 1, 4);
-        v[d] += __shfl_xor_sync(0xffffffffu, v[d], 2, 4);
-    }
-    rx = v[0];
-    ry = v[1];
-    rz = v[2];
-}
-
-// Velocity at (x, y, z) by trilinear interpolation of the node velocities (the
-// reference's vel_interpolate), a team of 4 consecutive lanes per particle, the corner
-// record held in registers.
-template <typename R, int L>
-RBC_D void vel_interp_team(const TracerArgs& A, const double* zb, int q, double x, double y, double z,
-                           double& rx, double& ry, double& rz, R (&rec)[NodeRecLen<L>::value], int& cached)
-{
-    const Corner c = find_corner(A, q, x, y, z);
-    // RK stages rarely leave the cell: reload this corner's record only when it changed
-    if (c.node != cached) {
-        load_record<R, L>(reinterpret_cast<const R*>(A.nv), (size_t)c.node, rec);
-        cached = c.node;
-    }
-    team_velocity<R, L>(c, rec, zb, rx, ry, rz);
 }
 
 // RK4 on the frozen field (step_particle_on_GPU, particle_tracer.cu:610-687): vel(x, y, z,
@@ -194,24 +165,82 @@ RBC_D void finish_tracer(const TracerArgs& A, int t, double x, double y, double 
     }
 }
 
-// Corner records gathered by the lanes' own loads into registers (any record size).
-template <typename R, int L>
-__global__ void __launch_bounds__(128) k_tracers(TracerArgs A)
+// One team of 8 consecutive lanes per particle. The team's four corner records (the xy
+// corners of the particle's cell) are copied into the team's slot of shared memory by all
+// eight lanes together, 16 contiguous bytes per lane and copy (the two x-neighbours are
+// adjacent records), so each copy instruction of a warp touches a few lines instead of one
+// sector per lane. Lane (q, hf), q = lane & 3 the corner (q & 1, q >> 1) and hf = (lane >> 2)
+// & 1 the record half, then evaluates its half of corner q's node velocity on the cell's
+// two levels and keeps that share in registers: an RK stage that stays in the cell (the
+// common case) only reweights the shares, and one that stays in the column re-evaluates
+// them from shared memory. The 8 shares are summed with three shuffle rounds.
+constexpr int kTracerThreads = 256;
+template <typename R, int L> constexpr size_t tracer_smem()
 {
-    __shared__ double zb[kZNum * 3 * L];
-    for (int e = threadIdx.x; e < kZNum * 3 * L; e += blockDim.x) zb[e] = A.zbasis[e];
-    __syncthreads();
+    return (size_t)(kTracerThreads / 8) * 4 * NodeRec<L>::value * sizeof(R);
+}
+
+template <typename R, int L>
+__global__ void __launch_bounds__(kTracerThreads) k_tracers(TracerArgs A)
+{
+    constexpr int NR = NodeRec<L>::value, HALF = NodeRec<L>::HALF;
+    constexpr int CH = NR * (int)sizeof(R) / 16; // 16-byte chunks per record
+    extern __shared__ __align__(16) unsigned char tr_smem[];
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = gt >> 2, q = gt & 3;               // particle, corner lane
-    const bool live = t < A.n;                       // whole teams are live or not
+    const int t = gt >> 3, l8 = gt & 7, q = gt & 3, hf = (gt >> 2) & 1; // particle, team lane, corner, half
+    R* slot = reinterpret_cast<R*>(tr_smem) + (size_t)(threadIdx.x >> 3) * 4 * NR; // the team's 4 records
+    const bool live = t < A.n;                              // whole teams are live or not
     const int tt = live ? t : 0;
     double x = A.pos[tt], y = A.pos[A.n + tt], z = A.pos[2 * A.n + tt];
-    R rec[NodeRecLen<L>::value];
-    int cached = -1;
+    int cell = -1, ev_iz = -1;
+    double u0[3] = {0, 0, 0}, u1[3] = {0, 0, 0};
+    const R* nv = reinterpret_cast<const R*>(A.nv);
     rk4_team(x, y, z, A.dt, [&](double px, double py, double pz, double& vx, double& vy, double& vz) {
-        vel_interp_team<R, L>(A, zb, q, px, py, pz, vx, vy, vz, rec, cached);
+        const Corner c = find_corner(A, q, px, py, pz);
+        // the four corner nodes, gathered by the whole warp (the shuffles are outside the
+        // branch below, which teams of one warp take differently); corner 0's node
+        // identifies the cell (uniform over the team)
+        const int n0 = __shfl_sync(0xffffffffu, c.node, 0, 4), n1 = __shfl_sync(0xffffffffu, c.node, 1, 4),
+                  n2 = __shfl_sync(0xffffffffu, c.node, 2, 4), n3 = __shfl_sync(0xffffffffu, c.node, 3, 4);
+        const bool load = n0 != cell;
+        if (load) {
+#pragma unroll
+            for (int m = 0; m < (4 * CH + 7) / 8; ++m) {
+                const int g = l8 + 8 * m;       // chunk g of the four records
+                if (g < 4 * CH) {
+                    const int cq = g / CH, part = g - cq * CH;
+                    const int node = cq == 0 ? n0 : cq == 1 ? n1 : cq == 2 ? n2 : n3;
+                    cp_async<16>(slot + cq * NR + part * (16 / (int)sizeof(R)),
+                                 nv + (size_t)node * NR + part * (16 / (int)sizeof(R)));
+                }
+            }
+            cell = n0;
+        }
+        cp_async_wait_all();
+        __syncwarp();
+        if (load || c.iz0 != ev_iz) {
+            R rec[HALF];
+            const R* src = slot + q * NR + hf * HALF;
+#pragma unroll
+            for (int e = 0; e < HALF; ++e) rec[e] = src[e];
+            half_node_velocity<R, L>(rec, hf, A.zbasis + (size_t)c.iz0 * 3 * L, A.zbasis + (size_t)c.iz1 * 3 * L,
+                                     u0, u1);
+            ev_iz = c.iz0;
+        }
+        __syncwarp(); // the slot is rewritten by the next stage's copies only after every lane read it
+        double v[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v[d] = c.w * (c.wz0 * u0[d] + c.wz1 * u1[d]);
+            v[d] += __shfl_xor_sync(0xffffffffu, v[d], 1, 8);
+            v[d] += __shfl_xor_sync(0xffffffffu, v[d], 2, 8);
+            v[d] += __shfl_xor_sync(0xffffffffu, v[d], 4, 8);
+        }
+        vx = v[0];
+        vy = v[1];
+        vz = v[2];
     });
-    if (live && q == 0) finish_tracer(A, t, x, y, z);
+    if (live && l8 == 0) finish_tracer(A, t, x, y, z);
 }
 
 // Copies positions into one FP32 track frame (the frame of freshly set positions).
