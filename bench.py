@@ -198,16 +198,18 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def mixed_form(s64, stream, args, local, world):
-    """Mixed form (FP32 synthesis, products and FFTs; FP64 implicit solve and reductions)
-    on the same workload: sim-time/s over the same timed step count from the given state,
-    and the relative error of Nu_wall, Nu_vol and KE against the FP64 form after 2000
-    steps from that state (equal sim time)."""
+def mixed_form(s64, stream, args, local, world, form="mixed"):
+    """Mixed form (FP32 synthesis, products and FFTs; FP64 implicit solve and reductions),
+    or the collocation form (form="colloc": the same, with the nonlinear products on 2 Nz
+    Gauss-Legendre levels and the mode -> level products on the tensor cores), on the same
+    workload: sim-time/s over the same timed step count from the given state, and the
+    relative error of Nu_wall, Nu_vol and KE against the FP64 form after 2000 steps from that
+    state (equal sim time)."""
     import torch
     import sdc_b200
     state = s64.get_state()
     tr = s64.tracers_get()
-    m = sdc_b200.Solver(**WORK, form="mixed", n_tracers=NTRACERS, device=local, tune=bool(args.tune))
+    m = sdc_b200.Solver(**WORK, form=form, n_tracers=NTRACERS, device=local, tune=bool(args.tune))
     m.set_stream(stream.cuda_stream)
     m.set_state(*state)
     m.tracers_set(tr)
@@ -230,8 +232,10 @@ def mixed_form(s64, stream, args, local, world):
     d64, dm = s64.diagnostics(), m.diagnostics()
     err = {k: abs(dm[k] - d64[k]) / abs(d64[k]) for k in ("nu_wall", "nu_vol", "ke")}
     m.close()
-    return {"value": value, "unit": "sim-time/s", "ms_per_step": ms / args.steps,
-            "dtype": "f32 synthesis/products/FFTs + f64 implicit solve, mean flow, diagnostics",
+    dtype = ("f32 synthesis/products/FFTs + f64 implicit solve, mean flow, diagnostics" if form == "mixed" else
+             "f32 FFTs; mode -> level products tcgen05 kind::tf32 with split operands (3xTF32), level products and "
+             "level -> mode sums f32 on 2 Nz Gauss-Legendre levels; f64 implicit solve, mean flow, diagnostics")
+    return {"value": value, "unit": "sim-time/s", "ms_per_step": ms / args.steps, "dtype": dtype,
             "rel_err_vs_fp64": err, "compared_after_steps": n_cmp,
             "fp64_nu_wall": d64["nu_wall"], "nu_err_le_1e-3": bool(err["nu_wall"] <= 1e-3)}
 
@@ -254,7 +258,7 @@ def mixed_sdc_form(stream, local, steps=4000):
     import sdc_b200
     res = {}
     diag = {}
-    for form in ("fp64", "mixed"):
+    for form in ("fp64", "mixed", "colloc"):
         s = sdc_b200.Solver(**SDC, form=form, device=local, tune=True)
         s.set_stream(stream.cuda_stream)
         s.init_fields(3, 1e-3, 8.0)
@@ -272,9 +276,16 @@ def mixed_sdc_form(stream, local, steps=4000):
         d = s.diagnostics()
         diag[form] = (d, s.spectrum(64, 0.0))
         s.close()
-    (d64, sp64), (dm, spm) = diag["fp64"], diag["mixed"]
-    err = {k: abs(dm[k] - d64[k]) / abs(d64[k]) for k in ("nu_wall", "nu_vol", "ke")}
-    err["spectrum_rel_l2"] = float(np.linalg.norm(spm - sp64) / np.linalg.norm(sp64))
+    d64, sp64 = diag["fp64"]
+
+    def errors(form):
+        dm, spm = diag[form]
+        err = {k: abs(dm[k] - d64[k]) / abs(d64[k]) for k in ("nu_wall", "nu_vol", "ke")}
+        err["spectrum_rel_l2"] = float(np.linalg.norm(spm - sp64) / np.linalg.norm(sp64))
+        return err
+
+    err = errors("mixed")
+    cerr = errors("colloc")
     return {"config": "512x512x12, Lx=Ly=64, Ra=6000, Pr=1, dt=2.5e-4, %d steps, seed 3 |k|<=8" % steps,
             "value": res["mixed"]["sim_time_per_s"], "unit": "sim-time/s",
             "fp64_value": res["fp64"]["sim_time_per_s"],
@@ -282,7 +293,12 @@ def mixed_sdc_form(stream, local, steps=4000):
             "ms_per_step": res["mixed"]["ms_per_step"], "fp64_ms_per_step": res["fp64"]["ms_per_step"],
             "rel_err_vs_fp64": err, "fp64_nu_wall": d64["nu_wall"], "fp64_ke": d64["ke"],
             "nu_err_le_1e-3": bool(err["nu_wall"] <= 1e-3),
-            "dtype": "f32 synthesis/products/FFTs + f64 implicit solve, mean flow, diagnostics"}
+            "dtype": "f32 synthesis/products/FFTs + f64 implicit solve, mean flow, diagnostics",
+            "colloc": {"value": res["colloc"]["sim_time_per_s"], "ms_per_step": res["colloc"]["ms_per_step"],
+                       "speedup_vs_fp64": res["colloc"]["sim_time_per_s"] / res["fp64"]["sim_time_per_s"],
+                       "levels": 24, "rel_err_vs_fp64": cerr, "nu_err_le_1e-3": bool(cerr["nu_wall"] <= 1e-3),
+                       "dtype": "mode -> level products on tcgen05 (kind::tf32, split operands), FP32 level "
+                                "products and sums, FP64 implicit solve"}}
 
 
 def optional_physics_forms(s64, stream, local, steps=2000):
@@ -800,6 +816,7 @@ def main():
     forms = None
     if args.form == "fp64" and not args.no_forms and world == 1:
         forms = {"mixed": mixed_form(s, stream, args, local, world),
+                 "colloc": mixed_form(s, stream, args, local, world, form="colloc"),
                  "mixed_512x512x12": mixed_sdc_form(stream, local)}
         forms.update(optional_physics_forms(s, stream, local))
         if not args.no_batched:

@@ -38,8 +38,14 @@ typedef enum {
 
 typedef enum {
     RBC_FORM_FP64 = 0,        /* plain step: everything in FP64 */
-    RBC_FORM_MIXED = 1        /* FP32 synthesis, products, contraction and FFTs;
+    RBC_FORM_MIXED = 1,       /* FP32 synthesis, products, contraction and FFTs;
                                  FP64 implicit solve, mean flow and diagnostics */
+    RBC_FORM_COLLOC = 2       /* as MIXED, with the nonlinear products formed on colloc_nq
+                                 Gauss-Legendre levels in z: the vertical mode -> level
+                                 synthesis and the level -> mode projection are tensor-core
+                                 products (tcgen05, TF32 operands split in two, FP32
+                                 accumulation) on TMA-staged tiles; FP64 implicit solve,
+                                 mean flow and diagnostics */
 } rbc_form;
 
 /* Construction parameters. Replaces main.cu's -nmodes M N L, -clength Lx Ly, -ra,
@@ -80,6 +86,11 @@ typedef struct {
     double mean_F;     /* nonzero: before every step F of the lowest vertical mode is set to
                           (mean_F, 0), the reference's -mean_F (force_mean, util.cu:74-81,
                           main.cu:139-140, 566-568); 0: no forcing */
+    int colloc_nq;     /* RBC_FORM_COLLOC: Gauss-Legendre collocation levels in z, a multiple
+                          of 8 from nz to 32 (0: 2 nz rounded up to a multiple of 8); the
+                          level rule aliases the triple products of the top modes (4 nz
+                          levels would reproduce the exact Galerkin integrals to ~1e-9 of their
+                          scale); other forms: ignored */
 } rbc_params;
 
 /* Masks of the penalized operator (nonlinear_operator_rayleigh_noslip.cu:1653-1738; 1 in

@@ -58,6 +58,8 @@ def lib():
         L.oracle_operator_table.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.oracle_operator_table.restype = None
         L.oracle_fft.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
+        L.oracle_set_colloc.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_set_colloc.restype = None
         L.oracle_fft.restype = None
         L.oracle_rfft2.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.oracle_rfft2.restype = None
@@ -236,6 +238,11 @@ class Oracle:
 
     def set_threads(self, n):
         lib().oracle_set_threads(self.h, n)
+
+    def set_colloc(self, nq):
+        """Nonlinear term of the library's collocation form on nq Gauss-Legendre levels (the
+        3-index tensors become nq-point sums; not a reference method); 0: exact integrals."""
+        lib().oracle_set_colloc(self.h, nq)
 
     def _bufs(self):
         shp = (self.L, self.ny, self.mox)

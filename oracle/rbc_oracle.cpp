@@ -142,7 +142,10 @@ static double fn_eval(char f, int m, double z)
     }
 }
 
-static void build_tables(int L, Tables& T)
+// colloc_nq > 0: the 3-index tensors are the colloc_nq-point Gauss-Legendre sums instead of
+// the integrals -- the definition of the library's collocation form (products formed on
+// colloc_nq levels and projected back with the same rule); not a reference method.
+static void build_tables(int L, Tables& T, int colloc_nq = 0)
 {
     T.L = L;
     const int nq = 96 + 16 * L;
@@ -167,6 +170,16 @@ static void build_tables(int L, Tables& T)
                 out[i + j * L] = (double)acc;
             }
     };
+    // the rule of the 3-index tensors
+    const int nq3 = colloc_nq > 0 ? colloc_nq : nq;
+    std::vector<double> zq3 = zq, wq3 = wq, val3 = val;
+    if (colloc_nq > 0) {
+        gauss_legendre(nq3, zq3, wq3);
+        val3.assign((size_t)5 * L * nq3, 0.0);
+        for (int f = 0; f < 5; ++f)
+            for (int m = 0; m < L; ++m)
+                for (int q = 0; q < nq3; ++q) val3[((size_t)f * L + m) * nq3 + q] = fn_eval(fns[f], m, zq3[q]);
+    }
     auto three = [&](const char* s, std::vector<double>& out) {
         out.assign(L * L * L, 0.0);
         for (int k = 0; k < L; ++k)
@@ -174,11 +187,11 @@ static void build_tables(int L, Tables& T)
                 for (int i = 0; i < L; ++i) {
                     int par = odd_fn(s[0], i) + odd_fn(s[1], j) + odd_fn(s[2], k);
                     if (par % 2) continue;
-                    const double* a = &val[(idx(s[0]) * L + i) * nq];
-                    const double* b = &val[(idx(s[1]) * L + j) * nq];
-                    const double* c = &val[(idx(s[2]) * L + k) * nq];
+                    const double* a = &val3[((size_t)idx(s[0]) * L + i) * nq3];
+                    const double* b = &val3[((size_t)idx(s[1]) * L + j) * nq3];
+                    const double* c = &val3[((size_t)idx(s[2]) * L + k) * nq3];
                     long double acc = 0;
-                    for (int q = 0; q < nq; ++q) acc += (long double)wq[q] * a[q] * b[q] * c[q];
+                    for (int q = 0; q < nq3; ++q) acc += (long double)wq3[q] * a[q] * b[q] * c[q];
                     out[i + j * L + k * L * L] = (double)acc;
                 }
     };
@@ -1327,6 +1340,10 @@ oracle_handle* oracle_create(int nx, int ny, int L, double lx, double ly, double
     return h;
 }
 void oracle_destroy(oracle_handle* h) { delete h; }
+
+// Switches the handle's nonlinear term to the library's collocation form on nq
+// Gauss-Legendre levels (nq > 0), or back to the exact integrals (nq = 0).
+void oracle_set_colloc(oracle_handle* h, int nq) { build_tables(h->s.p.L, h->s.T, nq); }
 
 // Penalization masks of the PENALIZED builds (nonlinear_operator_rayleigh_noslip.cu:1653-1738)
 // on [Ny][Nx], col = index % Nx, 1 inside the penalized region:

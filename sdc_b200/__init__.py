@@ -16,7 +16,7 @@ _LIB = None
 RBC_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite value", 4: "timeout",
           5: "I/O error", 6: "unsupported", 7: "out of device memory"}
-FORMS = {"fp64": 0, "mixed": 1}
+FORMS = {"fp64": 0, "mixed": 1, "colloc": 2}
 
 
 class RBCError(RuntimeError):
@@ -33,7 +33,7 @@ class _Params(ctypes.Structure):
                 ("tune", ctypes.c_int), ("tracer_diffusivity", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong),
                 ("track_frames", ctypes.c_int), ("track_period", ctypes.c_int), ("field_ops", ctypes.c_int),
                 ("penalization_eta", ctypes.c_double), ("penalization_mask", ctypes.c_int),
-                ("tracer_sets", ctypes.c_int), ("mean_F", ctypes.c_double)]
+                ("tracer_sets", ctypes.c_int), ("mean_F", ctypes.c_double), ("colloc_nq", ctypes.c_int)]
 
 
 class _Diag(ctypes.Structure):
@@ -242,14 +242,15 @@ def dump_write(path, arr, real_bytes=8):
 
 def make_params(nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0, tune=False,
                 tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
-                penalization=None, mean_F=0.0, tracer_sets=1):
+                penalization=None, mean_F=0.0, tracer_sets=1, colloc_nq=0):
     """penalization: None, or (eta, mask) with mask one of PEN_MASKS."""
     ops = 0
     for name in field_ops:
         ops |= FIELD_OPS[name]
     eta, kind = penalization if penalization else (0.0, "rectangle")
     return _Params(nx, ny, nz, lx, ly, ra, pr, dt, FORMS[form], n_tracers, device, diag_capacity, int(bool(tune)),
-                   tracer_diffusivity, noise_seed, track_frames, track_period, ops, eta, PEN_MASKS[kind], tracer_sets, mean_F)
+                   tracer_diffusivity, noise_seed, track_frames, track_period, ops, eta, PEN_MASKS[kind], tracer_sets, mean_F,
+                   colloc_nq)
 
 
 def track_write(path, frames, times, description=""):
@@ -304,7 +305,7 @@ class Solver:
 
     def __init__(self, nx, ny, nz, lx, ly, ra, pr, dt, form="fp64", n_tracers=0, device=0, diag_capacity=0,
                  tune=False, tracer_diffusivity=0.0, noise_seed=0, track_frames=0, track_period=1, field_ops=(),
-                 penalization=None, mean_F=0.0, tracer_sets=1, _handle=None):
+                 penalization=None, mean_F=0.0, tracer_sets=1, colloc_nq=0, _handle=None):
         self.nx, self.ny, self.L = nx, ny, nz
         self.mox = nx // 2 + 1
         self.n_tracers = n_tracers
@@ -315,7 +316,8 @@ class Solver:
             self.h = _handle
             return
         p = make_params(nx, ny, nz, lx, ly, ra, pr, dt, form, n_tracers, device, diag_capacity, tune,
-                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops, penalization, mean_F, tracer_sets)
+                        tracer_diffusivity, noise_seed, track_frames, track_period, field_ops, penalization, mean_F, tracer_sets,
+                        colloc_nq)
         h = ctypes.c_void_p()
         st = lib().rbc_create(ctypes.byref(p), ctypes.byref(h))
         if st != RBC_OK:

@@ -9,6 +9,7 @@
 #include "tracer_kernel.cuh"
 #include "update_kernel.cuh"
 #include "colloc_kernels.cuh"
+#include "colloc_tc.cuh"
 #include "mask_kernels.cuh"
 #include "pen_kernels.cuh"
 #include "solver_internal.h"
@@ -20,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using namespace rbck;
@@ -41,6 +43,9 @@ struct CudaError {
 struct ArgError {
     std::string msg;
 };
+
+// Most collocation levels of RBC_FORM_COLLOC (the TMEM columns of the level products).
+constexpr int kMaxCollocLevels = 32;
 
 template <typename T> T* dalloc(size_t n, std::vector<void*>& owned)
 {
@@ -70,6 +75,11 @@ struct rbc_handle {
     Geom G{};
     int W = 4, NP = 8;
     bool mixed = false;
+    int colloc_nq = 0;            // collocation form: levels of its nonlinear products (0: other forms)
+    float* col_bimg = nullptr;    // its basis operands (shared-memory image, hi then lo)
+    float* col_proj = nullptr;    // its level -> mode table [NKIND][Q][Lp]
+    int col_grid = 0;
+    size_t col_smem = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     std::vector<void*> owned;
     // state (FP64, CM) and AB2 history
@@ -353,9 +363,79 @@ template <typename R, int L> static void setup_contract(rbc_handle* h)
     h->contract_smem = smem;
 }
 
+// The collocation form's contraction (colloc_tc.cuh): the basis operands in the tensor
+// cores' shared-memory image (hi and lo TF32 parts), the weighted level -> mode table, the
+// launch shape.
+template <typename R, int L> static void setup_colloc(rbc_handle* h)
+{
+    const int Q = h->colloc_nq;
+    const CollocGeom cg = colloc_geom(L, Q);
+    int dev = 0, optin = 0, nsm = 148, per = 0;
+    RBC_CUDA(cudaGetDevice(&dev));
+    RBC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    RBC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    h->col_smem = (size_t)cg.smem + 1024;
+    if (cg.tcols > 512 || h->col_smem > (size_t)optin) throw ArgError{"collocation levels exceed the tensor-core tile"};
+    rbchost::CollocContract t;
+    rbchost::colloc_contract_tables(L, Q, t);
+    std::vector<float> img(cg.b_bytes / sizeof(float), 0.0f);
+    for (int f = 0; f < 8; ++f) {
+        const int p0 = rbccol::field_first_pair(f), np = rbccol::field_pairs(f);
+        for (int j = 0; j < np; ++j) {
+            const int kind = rbccol::spair_at(p0 + j).kind;
+            for (int q = 0; q < Q; ++q)
+                for (int i = 0; i < L; ++i) {
+                    const double v = t.basis[((size_t)kind * L + i) * Q + q];
+                    uint32_t bits;
+                    const float vf = (float)v;
+                    std::memcpy(&bits, &vf, 4);
+                    bits &= 0xFFFFE000u; // TF32 part
+                    float hi;
+                    std::memcpy(&hi, &bits, 4);
+                    const float lo = (float)(v - (double)hi);
+                    const unsigned o = cg.b_off[f] + colloc_kmajor_off(j * Q + q, i, cg.Kp);
+                    img[o / 4] = hi;
+                    img[(cg.b_half + o) / 4] = lo;
+                }
+        }
+    }
+    std::vector<float> proj((size_t)rbccol::NKIND * Q * cg.Lp, 0.0f);
+    for (int c = 0; c < rbccol::NKIND; ++c)
+        for (int q = 0; q < Q; ++q)
+            for (int k = 0; k < L; ++k) proj[((size_t)c * Q + q) * cg.Lp + k] = (float)t.proj[((size_t)c * Q + q) * L + k];
+    h->col_bimg = dalloc<float>(img.size(), h->owned);
+    h->col_proj = dalloc<float>(proj.size(), h->owned);
+    RBC_CUDA(cudaMemcpy(h->col_bimg, img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
+    RBC_CUDA(cudaMemcpy(h->col_proj, proj.data(), proj.size() * sizeof(float), cudaMemcpyHostToDevice));
+    RBC_CUDA(cudaFuncSetAttribute(k_colloc_contract<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->col_smem));
+    RBC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_colloc_contract<L>, kColThreads, h->col_smem));
+    if (per < 1) throw ArgError{"collocation contraction does not fit an SM"};
+    // one CTA per SM at most holds the TMEM columns without waiting for another CTA's
+    if (cg.tcols * per > 512) per = 512 / cg.tcols;
+    const int ntiles = (h->G.P + kColM - 1) / kColM;
+    h->col_grid = std::min(ntiles, nsm * per);
+}
+
 template <typename R, int L> static void launch_contract(rbc_handle* h)
 {
     StageScope sc(h, ST_CONTRACT);
+    if constexpr (std::is_same<R, float>::value) {
+        if (h->colloc_nq > 0) {
+            CollocArgs A;
+            A.phys = (const float*)h->phys;
+            A.grp = (float*)h->grp;
+            A.nv = h->tracer_pending ? (float*)h->nv : nullptr;
+            A.bimg = h->col_bimg;
+            A.proj = h->col_proj;
+            A.P = h->G.P;
+            A.ntiles = (h->G.P + kColM - 1) / kColM;
+            A.err = h->err;
+            launch_dep(h, k_colloc_contract<L>, dim3(h->col_grid), dim3(kColThreads), h->col_smem, A, h->colloc_nq);
+            RBC_CUDA(cudaGetLastError());
+            ++h->launches;
+            return;
+        }
+    }
     R* nv = h->tracer_pending ? (R*)h->nv : nullptr; // node records for the tracer advance
     launch_dep(h, k_contract<R, L>, dim3(h->contract_grid), dim3(128), (size_t)h->contract_smem, (const R*)h->phys,
                (R*)h->grp, (const R*)h->coef, h->G.P, nv);
@@ -1064,25 +1144,32 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
     if (!(p->tracer_diffusivity >= 0 && std::isfinite(p->tracer_diffusivity)) || p->track_frames < 0 ||
         p->track_period < 0 || (p->track_frames > 0 && p->n_tracers == 0))
         return RBC_ERR_INVALID_ARG;
-    if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED) return RBC_ERR_INVALID_ARG;
+    if (p->form != RBC_FORM_FP64 && p->form != RBC_FORM_MIXED && p->form != RBC_FORM_COLLOC)
+        return RBC_ERR_INVALID_ARG;
+    if (p->form == RBC_FORM_COLLOC && (p->colloc_nq < 0 || p->colloc_nq % 8 ||
+                                       (p->colloc_nq > 0 && p->colloc_nq < p->nz) || p->colloc_nq > kMaxCollocLevels))
+        return RBC_ERR_INVALID_ARG;
     if (p->field_ops & ~(RBC_FIELD_FREEZE | RBC_FIELD_HEAT | RBC_FIELD_SCALE)) return RBC_ERR_INVALID_ARG;
     if (!std::isfinite(p->mean_F)) return RBC_ERR_INVALID_ARG;
     if (!(p->penalization_eta >= 0 && std::isfinite(p->penalization_eta)) || p->penalization_mask < 0 ||
         p->penalization_mask > RBC_PEN_EVERYWHERE)
         return RBC_ERR_INVALID_ARG;
-    if (!L_supported(p->nz, p->form == RBC_FORM_MIXED)) return RBC_ERR_UNSUPPORTED;
+    if (!L_supported(p->nz, p->form != RBC_FORM_FP64)) return RBC_ERR_UNSUPPORTED;
     rbc_handle* h = new rbc_handle;
     h->prm = *p;
     {
         static std::atomic<unsigned long long> next_uid{1};
         h->uid = next_uid++;
     }
-    h->mixed = p->form == RBC_FORM_MIXED;
+    h->mixed = p->form != RBC_FORM_FP64;
+    // default: 2 nz levels, rounded up to the tensor-core K granularity of 8
+    h->colloc_nq = p->form == RBC_FORM_COLLOC ? (p->colloc_nq > 0 ? p->colloc_nq : std::max(8, (2 * p->nz + 7) / 8 * 8)) : 0;
     if (p->diag_capacity > 0) h->ring_cap = p->diag_capacity;
     try {
         RBC_CUDA(cudaSetDevice(p->device));
         rbchost::grid_info(p->nx, p->ny, p->nz, p->lx, p->ly, p->ra, p->pr, p->dt, h->gi);
-        rbchost::build_tables(p->nz, h->tab);
+        // the collocation form's nonlinear tensors are its level rule's sums
+        rbchost::build_tables(p->nz, h->tab, h->colloc_nq);
         const size_t csz = h->mixed ? sizeof(float2) : sizeof(double2);
         h->px = rbcfft::make_plan(p->nx);
         h->py = rbcfft::make_plan(p->ny);
@@ -1203,6 +1290,7 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         if (h->mixed) {
             set_attributes<float>(h);
             RBC_DISPATCH_L(setup_contract, float, G.L, h);
+            if (h->colloc_nq > 0) RBC_DISPATCH_L(setup_colloc, float, G.L, h);
         } else {
             set_attributes<double>(h);
             RBC_DISPATCH_L(setup_contract, double, G.L, h);

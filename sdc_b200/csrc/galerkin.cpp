@@ -88,7 +88,7 @@ static void composite_gl(int panels, int n, std::vector<double>& z, std::vector<
     }
 }
 
-void build_tables(int L, Tables& T)
+void build_tables(int L, Tables& T, int colloc_nq)
 {
     T.L = L;
     T.lambda.resize(L);
@@ -112,16 +112,27 @@ void build_tables(int L, Tables& T)
                 out[i + j * L] = (double)s;
             }
     };
+    // the rule of the 3-index tensors: the exact one, or the collocation levels' rule
+    std::vector<double> z3 = z, w3 = w, v3 = v;
+    if (colloc_nq > 0) {
+        composite_gl(1, colloc_nq, z3, w3);
+        v3.assign((size_t)5 * L * colloc_nq, 0.0);
+        for (int kind = 0; kind < 5; ++kind)
+            for (int m = 0; m < L; ++m)
+                for (int q = 0; q < colloc_nq; ++q) v3[((size_t)kind * L + m) * colloc_nq + q] = basis(kind, m, z3[q]);
+    }
+    const int nq3 = (int)z3.size();
     auto int3 = [&](int ka, int kb, int kc, std::vector<double>& out) {
         out.assign(L * L * L, 0.0);
         double mx = 0;
+        auto col3 = [&](int kind, int m) { return &v3[((size_t)kind * L + m) * nq3]; };
         for (int k = 0; k < L; ++k)
             for (int j = 0; j < L; ++j)
                 for (int i = 0; i < L; ++i) {
                     if ((basis_odd(ka, i) + basis_odd(kb, j) + basis_odd(kc, k)) & 1) continue;
-                    const double *a = col(ka, i), *b = col(kb, j), *c = col(kc, k);
+                    const double *a = col3(ka, i), *b = col3(kb, j), *c = col3(kc, k);
                     long double s = 0;
-                    for (int q = 0; q < nq; ++q) s += (long double)w[q] * a[q] * b[q] * c[q];
+                    for (int q = 0; q < nq3; ++q) s += (long double)w3[q] * a[q] * b[q] * c[q];
                     out[i + j * L + k * L * L] = (double)s;
                     mx = std::max(mx, std::fabs((double)s));
                 }
@@ -201,6 +212,22 @@ static bool ls_inverse(int nq, int L, const std::vector<double>& B, std::vector<
             P[m * nq + q] = (double)s;
         }
     return true;
+}
+
+void colloc_contract_tables(int L, int Q, CollocContract& t)
+{
+    t.L = L;
+    t.Q = Q;
+    composite_gl(1, Q, t.z, t.w);
+    t.basis.assign((size_t)5 * L * Q, 0.0);
+    t.proj.assign((size_t)5 * Q * L, 0.0);
+    for (int kind = 0; kind < 5; ++kind)
+        for (int i = 0; i < L; ++i)
+            for (int q = 0; q < Q; ++q) {
+                const double v = basis(kind, i, t.z[q]);
+                t.basis[((size_t)kind * L + i) * Q + q] = v;
+                t.proj[((size_t)kind * Q + q) * L + i] = t.w[q] * v;
+            }
 }
 
 bool colloc_tables(int L, int nq, CollocTables& t)

@@ -18,7 +18,12 @@ struct Tables {
     double ibbb(int i, int j, int k) const { return -t3(Iabc, i, j, k) - t3(Iabc, i, k, j); }
 };
 
-void build_tables(int L, Tables& T);
+// colloc_nq > 0: the 3-index tensors (the nonlinear term's) are the colloc_nq-point
+// Gauss-Legendre sums sum_q w_q a_i(z_q) b_j(z_q) c_k(z_q) instead of the exact integrals,
+// i.e. the tensors of a step that forms its products on colloc_nq collocation levels and
+// projects them back with the same rule; the 2-index tables (linear operators,
+// diagnostics) stay exact.
+void build_tables(int L, Tables& T, int colloc_nq = 0);
 
 // Value of the contraction matrix T'(i,j) of family f at output mode k.
 double family_value(const Tables& T, int family, int i, int j, int k);
@@ -71,6 +76,14 @@ struct CollocTables {
     std::vector<double> z, C, Cp, S, Ps, Pc;
 };
 bool colloc_tables(int L, int nq, CollocTables& t);
+// The collocation form's contraction (colloc_prog.h) on Q Gauss-Legendre levels of
+// (-1/2, 1/2): z[q], w[q], basis[(kind * L + i) * Q + q] = kind's function i at z_q (kinds
+// C, C', C'', S, S') and proj[(kind * Q + q) * L + k] = w_q times kind's function k at z_q.
+struct CollocContract {
+    int L = 0, Q = 0;
+    std::vector<double> z, w, basis, proj;
+};
+void colloc_contract_tables(int L, int Q, CollocContract& t);
 // Tracer start patterns of particle_tracer::init_positions (rbc_tracer_init types).
 void tracer_pattern(int type, uint64_t seed, int n, double lx, double ly, double cx, double cy, double cz,
                     double sigma, double* xyz);

@@ -15,7 +15,7 @@
 //   -init_giantspiral | -init_test   pattern initial conditions (main.cu:88-98, 326-352)
 //   -init_mode m  -init_noise a      their mode (default Lx/2) and the noise of the other
 //                                    modes (default 1e-6, init_random's amplitude)
-//   -form fp64|mixed     precision form
+//   -form fp64|mixed|colloc   precision form (-colloc_nq Q: collocation levels of colloc)
 //   -diag n              print Nu_wall, Nu_vol, KE every n steps
 //   -real_bytes 4|8      element size of the written dumps (4 = the reference's default)
 //   -freeze_circle N     from iteration N on, hold the field inside the circle of radius 0.8
@@ -119,7 +119,10 @@ int main(int argc, char** argv)
     p.device = (int)a.num("-device", 0);
     p.n_tracers = (int)a.num("-particles", 0);
     const char* form = a.str("-form");
-    p.form = (form && !std::strcmp(form, "mixed")) ? RBC_FORM_MIXED : RBC_FORM_FP64;
+    p.form = (form && !std::strcmp(form, "mixed"))    ? RBC_FORM_MIXED
+             : (form && !std::strcmp(form, "colloc")) ? RBC_FORM_COLLOC
+                                                      : RBC_FORM_FP64;
+    p.colloc_nq = (int)a.num("-colloc_nq", 0);
     const int nfiles = (int)a.num("-nfiles", 1);
     const unsigned long long seed = (unsigned long long)a.num("-seed", 1);
     const int diag_every = (int)a.num("-diag", 0);
