@@ -658,7 +658,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed", "colloc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", type=int, default=1, help="1: autotune the FFT launch tiling at creation")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-form and surrogate legs")
@@ -836,7 +836,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "steps_per_s": 1000.0 * args.steps / ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD if args.form == "fp64" else WORKLOAD.replace("FP64", "MIXED"),
+                "config": {"workload": WORKLOAD if args.form == "fp64" else WORKLOAD.replace("FP64", args.form.upper()),
                            "form": args.form, "parallelism": f"replicas x{world}",
                            "launch": {"autotuned": bool(args.tune), "column_block": W, "row_pairs": NP},
                            "l2": "working set > 126 MB L2 (state, history, scratch ~300 MB); no flush",
