@@ -98,3 +98,25 @@ def test_collocation_levels_are_validated():
     for q in (4, 12, 40):   # below nz, not a multiple of 8, above the tile
         with pytest.raises(sdc_b200.RBCError):
             sdc_b200.Solver(*case, form="colloc", colloc_nq=q)
+
+
+@pytest.mark.parametrize("kind", ["rectangle", "circle"])
+def test_collocation_form_with_penalization_matches_oracle(kind):
+    """The penalized operator of the PENALIZED builds adds its terms to the contracted
+    groups the collocation kernel writes; steps against the oracle with the same level rule
+    and the same penalization."""
+    case = (64, 48, 6, 16.0, 12.0, 4500.0, 1.0, 5e-4)
+    q = 16
+    s = sdc_b200.Solver(*case, form="colloc", colloc_nq=q, penalization=(0.02, kind))
+    o = oracle.Oracle(*case, threads=8)
+    o.set_colloc(q)
+    o.set_penalization(0.02, kind)
+    st = random_state(64, 48, 6, seed=44, amp=0.05)
+    s.set_state(*st)
+    o.set_state(*st)
+    s.step(10)
+    o.step(10)
+    got, ref = s.get_state(), o.get_state()
+    scale = max(np.abs(b).max() for b in ref[:3])
+    for name, a, b in zip(("theta", "f", "g", "F", "G"), got, ref):
+        assert np.abs(a - b).max() / scale < 3e-6, (name, np.abs(a - b).max() / scale)
