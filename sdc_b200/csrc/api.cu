@@ -1341,8 +1341,24 @@ rbc_status rbc_set_stream(rbc_handle* h, void* stream)
 
 static void upload_field(rbc_handle* h, const double* src, double2* dst, int nmat)
 {
-    const size_t n = (size_t)h->G.ny * h->G.mox * nmat;
-    RBC_CUDA(cudaMemcpyAsync(h->stage, src, n * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    // only the kept band crosses to the device: the kept prefix and suffix of rows of every
+    // matrix, columns c < ckeep (k_ref_to_cm reads nothing else of the staging copy), as two
+    // strided copies
+    const Geom& G = h->G;
+    const size_t rowb = (size_t)G.mox * sizeof(double2);
+    const int nlow = h->upd_nlow, nkr = h->upd_nkr;
+    for (int part = 0; part < 2; ++part) {
+        const int r0 = part == 0 ? 0 : nlow + (G.ny - nkr), nr = part == 0 ? nlow : nkr - nlow;
+        if (nr <= 0) continue;
+        cudaMemcpy3DParms cp = {};
+        cp.srcPtr = make_cudaPitchedPtr(const_cast<double*>(src), rowb, rowb, G.ny);
+        cp.dstPtr = make_cudaPitchedPtr(h->stage, rowb, rowb, G.ny);
+        cp.srcPos = make_cudaPos(0, r0, 0);
+        cp.dstPos = make_cudaPos(0, r0, 0);
+        cp.extent = make_cudaExtent((size_t)G.ckeep * sizeof(double2), nr, nmat);
+        cp.kind = cudaMemcpyHostToDevice;
+        RBC_CUDA(cudaMemcpy3DAsync(&cp, h->stream));
+    }
     k_ref_to_cm<<<512, 256, 0, h->stream>>>(h->stage, dst, h->G, nmat);
     RBC_CUDA(cudaGetLastError());
 }
