@@ -318,6 +318,10 @@ rbc_handle* rbc_ensemble_member(rbc_ensemble* e, int i);
 rbc_status rbc_ensemble_step(rbc_ensemble* e, int nsteps);
 /* Text of the last error of rbc_ensemble_step ("" when none). */
 const char* rbc_ensemble_last_error(const rbc_ensemble* e);
+/* Device time in ms (CUDA events on the ensemble's root stream) of the graph-replayed steps
+ * of the last rbc_ensemble_step call; 0 when that call replayed none (its first steps, and
+ * steps of members with tracers, are enqueued eagerly and not timed here). */
+rbc_status rbc_ensemble_elapsed(const rbc_ensemble* e, float* ms);
 /* Column-block width W and row pairs per CTA NP chosen for a handle (after tuning). */
 rbc_status rbc_launch_config(const rbc_handle* h, int* W, int* NP);
 

@@ -73,7 +73,8 @@ EXPORTS = ["rbc_create", "rbc_destroy", "rbc_last_error", "rbc_status_string", "
            "rbc_tracers_advance", "rbc_diagnostics", "rbc_diag_history", "rbc_spectrum", "rbc_synthesis",
            "rbc_table", "rbc_galerkin_table", "rbc_stage_times", "rbc_measure_fp64_peak", "rbc_nonlinear_noalloc", "rbc_dump_read", "rbc_dump_write",
            "rbc_save_state", "rbc_load_state", "rbc_save_history", "rbc_load_history", "rbc_ensemble_create",
-           "rbc_ensemble_destroy", "rbc_ensemble_member", "rbc_ensemble_step", "rbc_ensemble_last_error", "rbc_launch_config",
+           "rbc_ensemble_destroy", "rbc_ensemble_member", "rbc_ensemble_step", "rbc_ensemble_last_error",
+           "rbc_ensemble_elapsed", "rbc_launch_config",
            "rbc_kernel_launches", "rbc_tracers_init", "rbc_tracer_moments", "rbc_tracks_read", "rbc_track_write",
            "rbc_init_pattern", "rbc_fno_create", "rbc_gemm_bf16", "rbc_fno_destroy", "rbc_fno_last_error", "rbc_fno_num_params",
            "rbc_fno_get_params", "rbc_fno_set_params", "rbc_fno_get_norm", "rbc_fno_set_norm", "rbc_fno_forward",
@@ -151,6 +152,7 @@ def lib():
     L.rbc_ensemble_member.argtypes = [vp, ctypes.c_int]
     L.rbc_ensemble_member.restype = vp
     L.rbc_ensemble_step.argtypes = [vp, ctypes.c_int]
+    L.rbc_ensemble_elapsed.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.rbc_ensemble_last_error.argtypes = [vp]
     L.rbc_ensemble_last_error.restype = ctypes.c_char_p
     L.rbc_launch_config.argtypes = [vp, ip, ip]
@@ -284,6 +286,16 @@ class Ensemble:
         st = lib().rbc_ensemble_step(self.e, n)
         if st != RBC_OK:
             raise RBCError(st, "rbc_ensemble_step: " + lib().rbc_ensemble_last_error(self.e).decode())
+
+    def timed_step(self, n):
+        """step(n) and the device time in ms of its graph-replayed steps (CUDA events on the
+        ensemble's root stream)."""
+        self.step(n)
+        ms = ctypes.c_float()
+        st = lib().rbc_ensemble_elapsed(self.e, ctypes.byref(ms))
+        if st != RBC_OK:
+            raise RBCError(st, "rbc_ensemble_elapsed")
+        return ms.value
 
     def close(self):
         if getattr(self, "e", None):

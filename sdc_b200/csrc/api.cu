@@ -2183,6 +2183,8 @@ struct rbc_ensemble {
     cudaStream_t root = nullptr;
     std::vector<cudaEvent_t> ev;            // fork + one join event per worker
     cudaGraphExec_t graph = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr; // around the graph-replayed steps of a call
+    float last_ms = 0.0f;
     int device = 0;
     std::string last_error;
 };
@@ -2233,6 +2235,7 @@ rbc_status rbc_ensemble_create(const rbc_params* members, int n, int nstreams, r
     for (int s = 0; s < nstreams && ok; ++s) ok = cudaStreamCreateWithFlags(&e->streams[s], cudaStreamNonBlocking) == cudaSuccess;
     e->ev.resize(nstreams + 1);
     for (auto& x : e->ev) ok = ok && cudaEventCreateWithFlags(&x, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreate(&e->t0) == cudaSuccess && cudaEventCreate(&e->t1) == cudaSuccess;
     if (!ok) {
         rbc_ensemble_destroy(e);
         return RBC_ERR_CUDA;
@@ -2250,7 +2253,16 @@ void rbc_ensemble_destroy(rbc_ensemble* e)
     for (auto s : e->streams) if (s) cudaStreamDestroy(s);
     if (e->root) cudaStreamDestroy(e->root);
     for (auto x : e->ev) if (x) cudaEventDestroy(x);
+    if (e->t0) cudaEventDestroy(e->t0);
+    if (e->t1) cudaEventDestroy(e->t1);
     delete e;
+}
+
+rbc_status rbc_ensemble_elapsed(const rbc_ensemble* e, float* ms)
+{
+    if (!e || !ms) return RBC_ERR_INVALID_ARG;
+    *ms = e->last_ms;
+    return RBC_OK;
 }
 
 const char* rbc_ensemble_last_error(const rbc_ensemble* e)
@@ -2322,11 +2334,16 @@ rbc_status rbc_ensemble_step(rbc_ensemble* e, int nsteps)
             cudaGraphDestroy(g);
             RBC_CUDA(ce);
         }
+        const int replayed = nsteps - s;
+        if (replayed > 0) RBC_CUDA(cudaEventRecord(e->t0, e->root));
         for (; s < nsteps; ++s) {
             RBC_CUDA(cudaGraphLaunch(e->graph, e->root));
             for (auto* h : e->members) ++h->host_steps;
         }
+        if (replayed > 0) RBC_CUDA(cudaEventRecord(e->t1, e->root));
         RBC_CUDA(cudaStreamSynchronize(e->root));
+        e->last_ms = 0.0f;
+        if (replayed > 0) RBC_CUDA(cudaEventElapsedTime(&e->last_ms, e->t0, e->t1));
         for (auto st : e->streams) RBC_CUDA(cudaStreamSynchronize(st));
         for (auto* h : e->members) {
             rbc_status st = check_err(h);

@@ -28,7 +28,8 @@ def test_ensemble_members_match_independent_runs():
         r.set_state(*st)
         refs.append(r)
     ens.step(3)      # first step is an Euler step, then graph replays
-    ens.step(17)
+    ms = ens.timed_step(17)
+    assert ms > 0.0  # device time of the 17 replayed steps (CUDA events on the root stream)
     for m, r in zip(ens.members, refs):
         r.step(20)
         for a, b in zip(m.get_state(), r.get_state()):
