@@ -596,6 +596,18 @@ def profile_diagnostics(local, iters=3):
                       "nu_wall": s.diagnostics()["nu_wall"]}))
 
 
+def profile_sdc(local, form="mixed", steps=6):
+    """Small workload for kernel profiling on the spiral-defect-chaos grid (512 x 512 x 12,
+    Lx = Ly = 64, Ra 6000, Pr 1, dt 2.5e-4): `steps` steps of the given form from the seeded
+    state (its transforms run on the Stockham kernels: 512 has no two-pass form)."""
+    import sdc_b200
+    s = sdc_b200.Solver(**SDC, form=form, device=local, tune=True)
+    s.init_fields(3, 1e-3, 8.0)
+    s.step(steps)
+    print(json.dumps({"profile_sdc": form, "nu_wall": s.diagnostics()["nu_wall"],
+                      "stages_us": {k: round(v[0] * 1000, 1) for k, v in s.stage_times(10).items()}}))
+
+
 def ensemble_configs(n=64, seed=4):
     """The uneven ensemble: per member a grid from {64, 128, 192, 256}^2, Nz from {4, 6, 8},
     Ra ~ U[2000, 8000], Pr from {0.7, 1, 7}, Lx = Ly = grid / 8, dt = 5e-4 (drawn by seed)."""
@@ -675,6 +687,8 @@ def main():
                     help="run only a small freeze/heating/penalization workload (for kernel profiling) and exit")
     ap.add_argument("--profile-diagnostics", action="store_true",
                     help="run only a small spectrum/structure-function/mean-forcing workload (for kernel profiling) and exit")
+    ap.add_argument("--profile-sdc", default=None, choices=["fp64", "mixed", "colloc"],
+                    help="run only a few steps of the given form on the 512x512x12 grid (for kernel profiling) and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_surrogate:
@@ -685,6 +699,9 @@ def main():
         return
     if args.profile_diagnostics:
         profile_diagnostics(int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.profile_sdc:
+        profile_sdc(int(os.environ.get("LOCAL_RANK", "0")), form=args.profile_sdc)
         return
 
     world, rank, local = dist_env()

@@ -501,9 +501,15 @@ static bool L_supported(int L, bool mixed)
     return L == 2 || L == 3 || L == 4 || L == 5 || L == 6 || L == 8 || L == 12;
 }
 
-// Radix of the two-pass register FFT for the x and y lengths (0: Stockham passes).
-static int rx_x(const rbc_handle* h) { return rbcfft::two_pass_radix(h->G.nx); }
-static int rx_y(const rbc_handle* h) { return rbcfft::two_pass_radix(h->G.ny); }
+// Lanes per transform of the register FFT for the x and y lengths (0: Stockham passes).
+// The combine kernel runs its 13 transforms in one CTA of at most kThreads threads, so
+// it takes the register FFT only up to 16 lanes (N = 256).
+static int rx_x(const rbc_handle* h) { return rbcfft::reg_fft_lanes(h->G.nx); }
+static int rx_y(const rbc_handle* h) { return rbcfft::reg_fft_lanes(h->G.ny); }
+static int rx_comb(const rbc_handle* h) { return 13 * rx_y(h) <= kThreads ? rx_y(h) : 0; }
+// Row pairs (transforms) a row-kernel CTA can hold: one per TL lanes of kThreads threads,
+// or one Stockham chunk.
+static int max_row_pairs(const rbc_handle* h) { return rx_x(h) ? kThreads / rx_x(h) : h->px.chunk; }
 
 template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
 {
@@ -515,7 +521,7 @@ template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
 }
 template <typename R> static size_t smem_combine(const rbc_handle* h)
 {
-    const int rx = rx_y(h);
+    const int rx = rx_comb(h);
     return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + 13 * (size_t)(rx ? tp_stride(h->G.ny, rx) : h->py.stride));
 }
 template <typename R> static size_t smem_rows(const rbc_handle* h)
@@ -537,6 +543,10 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     StageScope sc(h, ST_SYNTH);
     const size_t sm = smem_cols<R>(h, 8);
     switch (rx_y(h)) {
+    case 32:
+        if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, 32>, g1, dim3(8 * h->W * 32), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
+        else k_synth_columns_tp<R, 32><<<g1, 8 * h->W * 32, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H);
+        break;
     case 16:
         if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, 16>, g1, dim3(8 * h->W * 16), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
         else k_synth_columns_tp<R, 16><<<g1, 8 * h->W * 16, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H);
@@ -556,6 +566,7 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     const int nb = rows / (2 * h->NP);
     const size_t sm = smem_rows<R>(h);
     switch (rx_x(h)) {
+    case 32: launch_dep(h, k_rows_c2r_tp<R, 32>, dim3(nb), dim3(h->NP * 32), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     case 16: launch_dep(h, k_rows_c2r_tp<R, 16>, dim3(nb), dim3(h->NP * 16), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     case 8: launch_dep(h, k_rows_c2r_tp<R, 8>, dim3(nb), dim3(h->NP * 8), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     default: launch_dep(h, k_rows_c2r<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const C*)h->H, (R*)h->phys);
@@ -614,6 +625,7 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     const int nb = rows / (2 * h->NP);
     const size_t sm = smem_rows<R>(h);
     switch (rx_x(h)) {
+    case 32: launch_dep(h, k_rows_r2c_tp<R, 32>, dim3(nb), dim3(h->NP * 32), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     case 16: launch_dep(h, k_rows_r2c_tp<R, 16>, dim3(nb), dim3(h->NP * 16), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     case 8: launch_dep(h, k_rows_r2c_tp<R, 8>, dim3(nb), dim3(h->NP * 8), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     default: launch_dep(h, k_rows_r2c<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh);
@@ -624,7 +636,7 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     {
     StageScope sc(h, ST_COMBINE);
     const size_t sm = smem_combine<R>(h);
-    switch (rx_y(h)) {
+    switch (rx_comb(h)) {
     case 16: launch_dep(h, k_columns_combine_tp<R, 16>, g5, dim3(13 * 16), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     case 8: launch_dep(h, k_columns_combine_tp<R, 8>, g5, dim3(13 * 8), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     default: launch_dep(h, k_columns_combine<R>, g5, dim3(kThreads), sm, G, h->py, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
@@ -841,10 +853,13 @@ template <typename R> static void set_attributes(rbc_handle* h)
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
@@ -873,7 +888,7 @@ static void autotune(rbc_handle* h)
     for (int W = 1; W <= 4; W *= 2) {
         if (8 * W > h->py.chunk && W > 1) continue;
         if (rx_y(h) && 8 * W * rx_y(h) > kThreads) continue;
-        for (int NP = 1; NP <= 32 && NP <= h->px.chunk; ++NP) {
+        for (int NP = 1; NP <= 32 && NP <= max_row_pairs(h); ++NP) {
             if ((G.ny / 2) % NP) continue;
             if (rx_x(h) && NP * rx_x(h) > kThreads) continue;
             const int W0 = h->W, NP0 = h->NP;
@@ -1177,9 +1192,10 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         int W = 1;
         while (W < 4 && 8 * (2 * W) <= h->py.chunk) W *= 2;
         h->W = W;
-        // row kernels: NP row pairs per CTA, a divisor of Ny/2 that fits one FFT chunk
+        // row kernels: NP row pairs per CTA, a divisor of Ny/2 that fits one CTA's transforms
         int NP = 1;
-        for (int c = 1; c <= 32 && c <= h->px.chunk; ++c)
+        const int tlx = rbcfft::reg_fft_lanes(p->nx);
+        for (int c = 1; c <= 32 && c <= (tlx ? kThreads / tlx : h->px.chunk); ++c)
             if ((p->ny / 2) % c == 0) NP = c;
         h->NP = NP;
         Geom& G = h->G;

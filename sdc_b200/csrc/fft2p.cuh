@@ -1,4 +1,5 @@
-// fft2p.cuh -- register-resident two-pass FFTs of length N = R * R (R = 8 or 16).
+// fft2p.cuh -- register-resident FFTs: two passes for N = R * R (R = 8 or 16), three for
+// N = 512 (16 x 16 x 2, one warp per transform; three_pass_512 below).
 //
 // One transform is done by R consecutive lanes of a warp (a quarter or half warp).
 // With x[n], n = t + R a, the lane t holds v[a] = x[t + R a] on entry and
@@ -50,7 +51,63 @@ RBC_D void two_pass(typename cplx_t<Rt>::type (&v)[R], int t, typename cplx_t<Rt
     __syncwarp(m); // the tile may be reused by the caller after this
 }
 
-// R for a length handled by two_pass (0: use the Stockham passes).
-RBC_HD constexpr int two_pass_radix(int n) { return n == 256 ? 16 : n == 64 ? 8 : 0; }
+// Length 512 = 16 x 32 on a full warp. Lane t (< 32) holds v[a] = x[t + 32 a] (a < 16) on
+// entry and v[m] = X[t + 32 m] on exit, the layout two_pass gives with R = 16 values per lane
+// and 32 lanes. With t = t1 + 16 t0 (t1 < 16) and k = k1 + 16 (j2 + 2 m):
+//   pass 1: Y[k1] = sum_a x[t + 32 a] W_16^(a k1), times W_512^(t k1)       (registers)
+//   pass 2: the 2-point DFT over t0 between lanes t and t ^ 16; lane t0 = j2 keeps
+//           P[k1] = (Y_t1[k1] + (-1)^j2 Y_(t1+16)[k1]) W_32^(t1 j2)        (shuffles)
+//   pass 3: transpose through S[j2 272 + k1 17 + t1], so that lane k1 + 16 j2 holds P over
+//           t1, and the 16-point DFT over t1 gives X[k1 + 16 j2 + 32 m] in v[m].
+// S has 544 elements (tile_len_512); odd row pitch 17 keeps the transposed reads free of
+// bank conflicts.
+RBC_HD constexpr int tile_len_512() { return 2 * 16 * 17; }
+
+template <typename Rt>
+RBC_D void three_pass_512(typename cplx_t<Rt>::type (&v)[16], int t, typename cplx_t<Rt>::type* S,
+                          const typename cplx_t<Rt>::type* tw, int sign)
+{
+    typedef typename cplx_t<Rt>::type C;
+    dft_small<16, Rt>(v, sign);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) {
+        C w = tw[t * k1];                 // W_512^(t k1), t k1 <= 465
+        if (sign > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    const int t1 = t & 15, j2 = t >> 4;
+    C w = tw[16 * t1];                    // W_32^t1, applied by the j2 = 1 lanes
+    if (sign > 0) w.y = -w.y;
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) {
+        C o;
+        o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, 16);
+        o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, 16);
+        const C p = j2 ? cmul(o - v[k1], w) : v[k1] + o;
+        S[j2 * 272 + k1 * 17 + t1] = p;
+    }
+    __syncwarp();
+    const int k1 = t & 15;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = S[j2 * 272 + k1 * 17 + i];
+    dft_small<16, Rt>(v, sign);
+    __syncwarp(); // the tile may be reused by the caller after this
+}
+
+// Lanes per transform of the register FFT for length n (0: use the Stockham passes),
+// the length for a lane count, and the shared tile one transform needs.
+RBC_HD constexpr int reg_fft_lanes(int n) { return n == 512 ? 32 : n == 256 ? 16 : n == 64 ? 8 : 0; }
+RBC_HD constexpr int reg_fft_len(int lanes) { return lanes == 32 ? 512 : lanes * lanes; }
+RBC_HD constexpr int reg_tile_len(int lanes) { return lanes == 32 ? tile_len_512() : lanes * (lanes + 1); }
+
+// The register FFT of length reg_fft_len(TL) done by TL lanes, each holding VL = N / TL
+// values: v[a] = x[t + TL a] on entry, v[k] = X[t + TL k] on exit.
+template <int TL, typename Rt>
+RBC_D void reg_fft(typename cplx_t<Rt>::type (&v)[reg_fft_len(TL) / TL], int t, typename cplx_t<Rt>::type* S,
+                   const typename cplx_t<Rt>::type* tw, int sign)
+{
+    if constexpr (TL == 32) three_pass_512<Rt>(v, t, S, tw, sign);
+    else two_pass<TL, Rt>(v, t, S, tw, sign);
+}
 
 } // namespace rbcfft

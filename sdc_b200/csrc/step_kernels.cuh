@@ -321,12 +321,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
 }
 
 // =================================================================================
-// Two-pass forms of K1, K2, K4 and K5 for transform lengths N = RX * RX (64, 256), see
-// fft2p.cuh. The CTA holds the same transforms as the Stockham forms; each transform
-// is done by RX consecutive lanes, so the block has (transforms x RX) threads. A
-// transform's shared region has tp_stride(N) elements (the padded row of the Stockham
-// forms, or the RX (RX + 1) transpose tile if that is longer).
-RBC_HD int tp_stride(int n, int rx) { return rbcfft::padded_len(n) > rx * (rx + 1) ? rbcfft::padded_len(n) : rx * (rx + 1); }
+// Register-FFT forms of K1, K2, K4 and K5 for the transform lengths N = 64, 256 and 512
+// (fft2p.cuh): the CTA holds the same transforms as the Stockham forms; each transform is
+// done by TL consecutive lanes (8, 16, 32) holding VL = N / TL values each, so the block
+// has (transforms x TL) threads. A transform's shared region has tp_stride(N, TL) elements
+// (the padded row of the Stockham forms, or the register FFT's tile if that is longer).
+RBC_HD int tp_stride(int n, int tl)
+{
+    return rbcfft::padded_len(n) > rbcfft::reg_tile_len(tl) ? rbcfft::padded_len(n) : rbcfft::reg_tile_len(tl);
+}
 
 // Synthesis field fld (order of k_synth_columns) at (c, r) from theta, f, g.
 RBC_D double2 synth_value(int fld, double2 vt, double2 vf, double2 vg, const Mult& m)
@@ -343,18 +346,18 @@ RBC_D double2 synth_value(int fld, double2 vt, double2 vf, double2 vg, const Mul
     }
 }
 
-// K1, two-pass: grid (ckw / W, L), block 8 W RX threads (transform q = fld W + cc).
-template <typename R, int RX>
+// K1, register FFT: grid (ckw / W, L), block 8 W TL threads (transform q = fld W + cc).
+template <typename R, int TL>
 __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
     Geom G, int W, const double2* __restrict__ twy, const double2* __restrict__ th,
     const double2* __restrict__ f, const double2* __restrict__ g, const double2* __restrict__ FG,
     typename cplx_t<R>::type* __restrict__ H)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = RX * RX;
+    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
-    const int st = tp_stride(N, RX);
+    const int st = tp_stride(N, TL);
     C* buf = tw + N;
     double2* stg = reinterpret_cast<double2*>(buf + 8 * W * st); // [3][W][N]: theta, f, g
     const int k = blockIdx.y;
@@ -373,17 +376,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
     }
     cp_async_wait_all();
     __syncthreads();
-    const int q = threadIdx.x / RX, t = threadIdx.x - q * RX;
+    const int q = threadIdx.x / TL, t = threadIdx.x - q * TL;
     const int fld = q / W, cc = q - fld * W, c = c0 + cc;
     // the multipliers of Mult, evaluated with the same expressions, only where a field
     // needs them (fx per column; fy and the Laplacian per row)
     const double fx = c * (2 * kPi / G.lx), ac = c / G.lx;
     const bool ckept = c < G.ckeep;
     const double2* in = stg + (fld < 3 ? W * N : fld < 5 ? 2 * W * N : 0) + cc * N; // f, g or theta
-    C v[RX];
+    C v[VL];
 #pragma unroll
-    for (int a = 0; a < RX; ++a) {
-        const int r = t + RX * a;
+    for (int a = 0; a < VL; ++a) {
+        const int r = t + TL * a;
         const double2 u = (ckept && row_kept(r, N)) ? in[r] : make_double2(0, 0);
         const int ry = wrap_row(r, N);
         double2 val;
@@ -403,24 +406,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
         }
         v[a] = cmk<C>(val.x, val.y);
     }
-    rbcfft::two_pass<RX, R>(v, t, buf + q * st, tw, +1);
+    rbcfft::reg_fft<TL, R>(v, t, buf + q * st, tw, +1);
     C* dst = H + (((size_t)fld * G.L + k) * G.ckp + c) * N;
 #pragma unroll
-    for (int k2 = 0; k2 < RX; ++k2) dst[t + RX * k2] = v[k2];
+    for (int k2 = 0; k2 < VL; ++k2) dst[t + TL * k2] = v[k2];
 }
 
-// K2, two-pass: block NP RX threads, transform pp = row pair.
-template <typename R, int RX>
+// K2, register FFT: block NP TL threads, transform pp = row pair.
+template <typename R, int TL>
 __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
     Geom G, int NP, const double2* __restrict__ twx, const typename cplx_t<R>::type* __restrict__ H,
     R* __restrict__ phys)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = RX * RX;
+    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + N;
-    const int st = tp_stride(N, RX);
+    const int st = tp_stride(N, TL);
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     pdl_trigger();
@@ -454,52 +457,52 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
         }
     }
     __syncthreads();
-    const int pp = threadIdx.x / RX, t = threadIdx.x - pp * RX;
+    const int pp = threadIdx.x / TL, t = threadIdx.x - pp * TL;
     C* S = buf + pp * st;
-    C v[RX];
+    C v[VL];
 #pragma unroll
-    for (int a = 0; a < RX; ++a) v[a] = S[rbcfft::pad(t + RX * a)];
-    __syncwarp(rbcfft::team_mask<RX>()); // every lane has read before the tile is overwritten
-    rbcfft::two_pass<RX, R>(v, t, S, tw, +1);
+    for (int a = 0; a < VL; ++a) v[a] = S[rbcfft::pad(t + TL * a)];
+    __syncwarp(rbcfft::team_mask<TL>()); // every lane has read before the tile is overwritten
+    rbcfft::reg_fft<TL, R>(v, t, S, tw, +1);
     R* dst = phys + (size_t)(row0 + 2 * pp) * N;
 #pragma unroll
-    for (int k2 = 0; k2 < RX; ++k2) {
-        dst[t + RX * k2] = v[k2].x;
-        dst[N + t + RX * k2] = v[k2].y;
+    for (int k2 = 0; k2 < VL; ++k2) {
+        dst[t + TL * k2] = v[k2].x;
+        dst[N + t + TL * k2] = v[k2].y;
     }
 }
 
-// K4, two-pass: block NP RX threads.
-template <typename R, int RX>
+// K4, register FFT: block NP TL threads.
+template <typename R, int TL>
 __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     Geom G, int NP, const double2* __restrict__ twx, const R* __restrict__ grp,
     typename cplx_t<R>::type* __restrict__ gh)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = RX * RX;
+    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + N;
-    const int st = tp_stride(N, RX);
+    const int st = tp_stride(N, TL);
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
-    const int pp = threadIdx.x / RX, t = threadIdx.x - pp * RX;
+    const int pp = threadIdx.x / TL, t = threadIdx.x - pp * TL;
     const R* src = grp + (size_t)(row0 + 2 * pp) * N;
     pdl_trigger();
     load_twiddles_async<R>(tw, twx, N);
     pdl_wait();
-    C v[RX];
+    C v[VL];
 #pragma unroll
-    for (int a = 0; a < RX; ++a) {
-        v[a].x = ld_cg(src + t + RX * a);
-        v[a].y = ld_cg(src + N + t + RX * a);
+    for (int a = 0; a < VL; ++a) {
+        v[a].x = ld_cg(src + t + TL * a);
+        v[a].y = ld_cg(src + N + t + TL * a);
     }
     cp_async_wait_all();
     __syncthreads();
     C* S = buf + pp * st;
-    rbcfft::two_pass<RX, R>(v, t, S, tw, -1);
+    rbcfft::reg_fft<TL, R>(v, t, S, tw, -1);
 #pragma unroll
-    for (int k2 = 0; k2 < RX; ++k2) S[rbcfft::pad(t + RX * k2)] = v[k2];
+    for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
     __syncthreads();
     const R half = (R)0.5;
     C* dst = gh + (size_t)plane * G.ckp * G.ny + y0;
@@ -519,34 +522,34 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     }
 }
 
-// K5, two-pass: grid (ckw, L), block 13 RX threads (transform = group).
-template <typename R, int RX>
+// K5, register FFT: grid (ckw, L), block 13 TL threads (transform = group).
+template <typename R, int TL>
 __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     Geom G, const double2* __restrict__ twy, const typename cplx_t<R>::type* __restrict__ gh,
     typename cplx_t<R>::type* __restrict__ N_out, double* __restrict__ NFG)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = RX * RX;
+    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + N;
-    const int st = tp_stride(N, RX);
+    const int st = tp_stride(N, TL);
     const int c = blockIdx.x, k = blockIdx.y;
     const size_t cstride = (size_t)G.L * G.ckp * N; // between groups
-    const int gq = threadIdx.x / RX, t = threadIdx.x - gq * RX;
+    const int gq = threadIdx.x / TL, t = threadIdx.x - gq * TL;
     const C* src = gh + ((size_t)k * G.ckp + c) * N + gq * cstride;
     pdl_trigger();
     load_twiddles_async<R>(tw, twy, N);
     pdl_wait();
-    C v[RX];
+    C v[VL];
 #pragma unroll
-    for (int a = 0; a < RX; ++a) v[a] = ld_cg(src + t + RX * a);
+    for (int a = 0; a < VL; ++a) v[a] = ld_cg(src + t + TL * a);
     cp_async_wait_all();
     __syncthreads();
     C* S = buf + gq * st;
-    rbcfft::two_pass<RX, R>(v, t, S, tw, -1);
+    rbcfft::reg_fft<TL, R>(v, t, S, tw, -1);
 #pragma unroll
-    for (int k2 = 0; k2 < RX; ++k2) S[rbcfft::pad(t + RX * k2)] = v[k2];
+    for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
     __syncthreads();
     const double invP = 1.0 / ((double)G.nx * N);
     for (int r = threadIdx.x; r < N; r += blockDim.x) {
