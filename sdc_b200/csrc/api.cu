@@ -502,11 +502,8 @@ static bool L_supported(int L, bool mixed)
 }
 
 // Lanes per transform of the register FFT for the x and y lengths (0: Stockham passes).
-// The combine kernel runs its 13 transforms in one CTA of at most kThreads threads, so
-// it takes the register FFT only up to 16 lanes (N = 256).
 static int rx_x(const rbc_handle* h) { return rbcfft::reg_fft_lanes(h->G.nx); }
 static int rx_y(const rbc_handle* h) { return rbcfft::reg_fft_lanes(h->G.ny); }
-static int rx_comb(const rbc_handle* h) { return 13 * rx_y(h) <= kThreads ? rx_y(h) : 0; }
 // Row pairs (transforms) a row-kernel CTA can hold: one per TL lanes of kThreads threads,
 // or one Stockham chunk.
 static int max_row_pairs(const rbc_handle* h) { return rx_x(h) ? kThreads / rx_x(h) : h->px.chunk; }
@@ -521,7 +518,7 @@ template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
 }
 template <typename R> static size_t smem_combine(const rbc_handle* h)
 {
-    const int rx = rx_comb(h);
+    const int rx = rx_y(h);
     return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + 13 * (size_t)(rx ? tp_stride(h->G.ny, rx) : h->py.stride));
 }
 template <typename R> static size_t smem_rows(const rbc_handle* h)
@@ -636,7 +633,8 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     {
     StageScope sc(h, ST_COMBINE);
     const size_t sm = smem_combine<R>(h);
-    switch (rx_comb(h)) {
+    switch (rx_y(h)) {
+    case 32: launch_dep(h, k_columns_combine_tp<R, 32>, g5, dim3(kThreads), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     case 16: launch_dep(h, k_columns_combine_tp<R, 16>, g5, dim3(13 * 16), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     case 8: launch_dep(h, k_columns_combine_tp<R, 8>, g5, dim3(13 * 8), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     default: launch_dep(h, k_columns_combine<R>, g5, dim3(kThreads), sm, G, h->py, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
@@ -862,6 +860,7 @@ template <typename R> static void set_attributes(rbc_handle* h)
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     if (h->prm.n_tracers > 0) RBC_DISPATCH_L(set_tracer_attribute, R, h->G.L, h);

@@ -522,7 +522,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     }
 }
 
-// K5, register FFT: grid (ckw, L), block 13 TL threads (transform = group).
+// K5, register FFT: grid (ckw, L), block min(13 TL, kThreads) threads; team q (TL lanes)
+// transforms groups q, q + teams, ... (one group each for TL <= 16, up to two for TL = 32).
 template <typename R, int TL>
 __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     Geom G, const double2* __restrict__ twy, const typename cplx_t<R>::type* __restrict__ gh,
@@ -536,20 +537,27 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     const int st = tp_stride(N, TL);
     const int c = blockIdx.x, k = blockIdx.y;
     const size_t cstride = (size_t)G.L * G.ckp * N; // between groups
-    const int gq = threadIdx.x / TL, t = threadIdx.x - gq * TL;
-    const C* src = gh + ((size_t)k * G.ckp + c) * N + gq * cstride;
+    const int teams = blockDim.x / TL, team = threadIdx.x / TL, t = threadIdx.x - team * TL;
+    const C* src = gh + ((size_t)k * G.ckp + c) * N + t;
     pdl_trigger();
     load_twiddles_async<R>(tw, twy, N);
     pdl_wait();
+    int gq = team;
     C v[VL];
 #pragma unroll
-    for (int a = 0; a < VL; ++a) v[a] = ld_cg(src + t + TL * a);
+    for (int a = 0; a < VL; ++a) v[a] = ld_cg(src + gq * cstride + TL * a);
     cp_async_wait_all();
     __syncthreads();
-    C* S = buf + gq * st;
-    rbcfft::reg_fft<TL, R>(v, t, S, tw, -1);
+    for (;;) {
+        C* S = buf + gq * st;
+        rbcfft::reg_fft<TL, R>(v, t, S, tw, -1);
 #pragma unroll
-    for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
+        for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
+        gq += teams;
+        if (gq >= 13) break;
+#pragma unroll
+        for (int a = 0; a < VL; ++a) v[a] = ld_cg(src + gq * cstride + TL * a);
+    }
     __syncthreads();
     const double invP = 1.0 / ((double)G.nx * N);
     for (int r = threadIdx.x; r < N; r += blockDim.x) {
