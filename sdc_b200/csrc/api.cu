@@ -88,7 +88,7 @@ struct rbc_handle {
     bool have_hist = false;
     // operators
     int* cls = nullptr;
-    double *binv = nullptr, *imp = nullptr, *diag_tab = nullptr;
+    double *optab = nullptr, *diag_tab = nullptr;
     void* coef = nullptr; // R
     double2 *twx = nullptr, *twy = nullptr;
     rbcfft::Plan px{}, py{};
@@ -456,8 +456,7 @@ template <typename R, int L> static void launch_update(rbc_handle* h)
     UpdateArgs A;
     A.G = h->G;
     A.cls = h->cls;
-    A.binv = h->binv;
-    A.imp = h->imp;
+    A.optab = h->optab;
     A.diag_tab = h->diag_tab;
     A.N = h->N;
     A.NFG = h->NFG;
@@ -1227,15 +1226,36 @@ rbc_status rbc_create(const rbc_params* p, rbc_handle** out)
         for (int c = 0; c < G.ckeep; ++c)
             for (int r = 0; r < G.ny; ++r) cls_cm[(size_t)c * G.ny + r] = op.cls[(size_t)r * G.mox + c];
         h->cls = dalloc<int>(plane, h->owned);
-        h->binv = dalloc<double>(op.binv.size(), h->owned);
-        h->imp = dalloc<double>(op.imp.size(), h->owned);
         RBC_CUDA(cudaMemcpy(h->cls, cls_cm.data(), plane * sizeof(int), cudaMemcpyHostToDevice));
-        RBC_CUDA(cudaMemcpy(h->binv, op.binv.data(), op.binv.size() * sizeof(double), cudaMemcpyHostToDevice));
-        RBC_CUDA(cudaMemcpy(h->imp, op.imp.data(), op.imp.size() * sizeof(double), cudaMemcpyHostToDevice));
+        // parity-packed rows of B_ff^-1 and the implicit blocks (update_kernel.cuh)
+        {
+            const int H = op_half(L), RW = op_row(L);
+            std::vector<double> pk((size_t)op.nclass * L * RW, 0.0);
+            for (int c = 0; c < op.nclass; ++c)
+                for (int b = 0; b < 5; ++b) {
+                    const double* m = b == 0 ? &op.binv[(size_t)c * L * L] : &op.imp[((size_t)c * 4 + b - 1) * L * L];
+                    for (int k = 0; k < L; ++k)
+                        for (int j = 0; j < L; ++j) {
+                            const double v = m[(size_t)k * L + j];
+                            if ((j - k) & 1) {
+                                if (v != 0.0) throw ArgError{"operator tables couple modes of opposite parity"};
+                            } else {
+                                pk[((size_t)c * L + k) * RW + (size_t)b * H + j / 2] = v;
+                            }
+                        }
+                }
+            h->optab = dalloc<double>(pk.size(), h->owned);
+            RBC_CUDA(cudaMemcpy(h->optab, pk.data(), pk.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
         std::vector<double> dtab;
         dtab.insert(dtab.end(), h->tab.CpCp.begin(), h->tab.CpCp.end());
         dtab.insert(dtab.end(), h->tab.CC.begin(), h->tab.CC.end());
         dtab.insert(dtab.end(), h->tab.CS.begin(), h->tab.CS.end());
+        for (int t = 0; t < 3; ++t) // the diagnostics skip the opposite-parity entries too
+            for (int k = 0; k < L; ++k)
+                for (int j = 0; j < L; ++j)
+                    if (((j - k) & 1) && dtab[(size_t)t * L * L + k + (size_t)j * L] != 0.0)
+                        throw ArgError{"diagnostic integrals couple modes of opposite parity"};
         h->diag_tab = dalloc<double>(dtab.size(), h->owned);
         RBC_CUDA(cudaMemcpy(h->diag_tab, dtab.data(), dtab.size() * sizeof(double), cudaMemcpyHostToDevice));
         std::vector<double> coef;

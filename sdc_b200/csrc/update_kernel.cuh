@@ -18,11 +18,20 @@
 
 namespace rbck {
 
+// The operators couple only vertical modes of equal parity: the Chandrasekhar functions
+// and sines of odd index m + 1 are even in z, those of even index odd, and every matrix
+// here (B_ff^-1, the four blocks of the implicit operator, the diagnostics' integrals) has
+// exact zeros where the row and column parities differ. Row k of each is therefore kept
+// as its OP_H(L) entries in columns m = (k & 1) + 2 i (0 past column L - 1), and the
+// products skip the zeros, which leaves every sum bit for bit unchanged.
+RBC_HD constexpr int op_half(int L) { return (L + 1) / 2; }
+// Doubles per packed row: B_ff^-1, then the (tt, tf, ft, ff) blocks, padded to even.
+RBC_HD constexpr int op_row(int L) { return (5 * op_half(L) + 1) & ~1; }
+
 struct UpdateArgs {
     Geom G;
     const int* cls;            // CM [ckp][Ny] q^2 class (-1: not kept)
-    const double* binv;        // [nclass][L*L]
-    const double* imp;         // [nclass][4][L*L]
+    const double* optab;       // [nclass][L][op_row(L)] parity-packed rows (see above)
     const double* diag_tab;    // [3][L*L]: int C'_i C'_j, int C_i C_j, int C_i S_j
     const void* N;             // CM [3][L][ckp][Ny] complex (R)
     const double* NFG;         // [2][L]
@@ -51,7 +60,7 @@ RBC_D double2 shfl2(double2 v, int src, int width)
 }
 
 template <typename R, int L>
-__global__ void __launch_bounds__(kThreads, L <= 8 ? 2 : 1) k_update(UpdateArgs A)
+__global__ void __launch_bounds__(kThreads, 2) k_update(UpdateArgs A)
 {
     typedef typename cplx_t<R>::type C;
     constexpr int T = TeamSize<L>::value;
@@ -109,39 +118,21 @@ __global__ void __launch_bounds__(kThreads, L <= 8 ? 2 : 1) k_update(UpdateArgs 
         }
         const bool act = cl >= 0;
         const bool kact = act && k < L;
-        double bi[L], M[4][L];
+        constexpr int H = op_half(L), RW = op_row(L);
+        const int par = k & 1;                      // columns m = par + 2 i of row k
+        double tv[RW];                              // bi = tv[0, H), block b at tv[(b + 1) H ...]
         if (kact) {
-            const double* brow = A.binv + (size_t)cl * L * L + (size_t)k * L;
-            const double* mrow = A.imp + (size_t)cl * 4 * L * L + (size_t)k * L;
-            if constexpr (L % 2 == 0) {
-                // rows start on even doubles: 16-byte loads
+            // rows start on even doubles: 16-byte loads
+            const double2* row = reinterpret_cast<const double2*>(A.optab + ((size_t)cl * L + k) * RW);
 #pragma unroll
-                for (int m = 0; m < L; m += 2) {
-                    const double2 v = __ldg(reinterpret_cast<const double2*>(brow + m));
-                    bi[m] = v.x;
-                    bi[m + 1] = v.y;
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const double2 w = __ldg(reinterpret_cast<const double2*>(mrow + b * L * L + m));
-                        M[b][m] = w.x;
-                        M[b][m + 1] = w.y;
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int m = 0; m < L; ++m) {
-                    bi[m] = __ldg(brow + m);
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) M[b][m] = __ldg(mrow + b * L * L + m);
-                }
+            for (int i = 0; i < RW / 2; ++i) {
+                const double2 v = __ldg(row + i);
+                tv[2 * i] = v.x;
+                tv[2 * i + 1] = v.y;
             }
         } else {
 #pragma unroll
-            for (int m = 0; m < L; ++m) {
-                bi[m] = 0;
-#pragma unroll
-                for (int b = 0; b < 4; ++b) M[b][m] = 0;
-            }
+            for (int i = 0; i < RW; ++i) tv[i] = 0;
         }
         // ---------------- inverse B (f needs the team's N_f)
         stg[wid][0][tm][k] = nf;
@@ -149,9 +140,9 @@ __global__ void __launch_bounds__(kThreads, L <= 8 ? 2 : 1) k_update(UpdateArgs 
         const double2 bt = nt * 2.0;
         double2 bf = make_double2(0, 0);
 #pragma unroll
-        for (int m = 0; m < L; ++m) {
-            const double2 v = stg[wid][0][tm][m];
-            bf = make_double2(bf.x + bi[m] * v.x, bf.y + bi[m] * v.y);
+        for (int i = 0; i < H; ++i) {
+            const double2 v = stg[wid][0][tm][par + 2 * i]; // past L - 1: a zero slot and a zero entry
+            bf = make_double2(bf.x + tv[i] * v.x, bf.y + tv[i] * v.y);
         }
         const double2 bg = (q2d != 0.0) ? ng * ((-2.0) * pr / q2d) : make_double2(0, 0);
         // ---------------- AB2 and history
@@ -177,10 +168,12 @@ __global__ void __launch_bounds__(kThreads, L <= 8 ? 2 : 1) k_update(UpdateArgs 
         __syncwarp();
         double2 to = make_double2(0, 0), fo = to;
 #pragma unroll
-        for (int m = 0; m < L; ++m) {
+        for (int i = 0; i < H; ++i) {
+            const int m = par + 2 * i;
             const double2 vt = stg[wid][0][tm][m], vf = stg[wid][1][tm][m];
-            to = make_double2(to.x + (M[0][m] * vt.x + M[1][m] * vf.x), to.y + (M[0][m] * vt.y + M[1][m] * vf.y));
-            fo = make_double2(fo.x + (M[2][m] * vt.x + M[3][m] * vf.x), fo.y + (M[2][m] * vt.y + M[3][m] * vf.y));
+            const double m0 = tv[H + i], m1 = tv[2 * H + i], m2 = tv[3 * H + i], m3 = tv[4 * H + i];
+            to = make_double2(to.x + (m0 * vt.x + m1 * vf.x), to.y + (m0 * vt.y + m1 * vf.y));
+            fo = make_double2(fo.x + (m2 * vt.x + m3 * vf.x), fo.y + (m2 * vt.y + m3 * vf.y));
         }
         double2 go = (q2d != 0.0) ? ug * (1.0 / (1.0 + dt * pr * (q2d + mpi * mpi))) : make_double2(0, 0);
         if (c == 0 && r == 0) { to.y = 0; fo.y = 0; go.y = 0; }
@@ -207,7 +200,9 @@ __global__ void __launch_bounds__(kThreads, L <= 8 ? 2 : 1) k_update(UpdateArgs 
             const double qx = 2 * kPi * c / G.lx, qy = 2 * kPi * ry / G.ly, q2 = qx * qx + qy * qy;
             double eff = 0, ecc = 0, wt = 0;
 #pragma unroll
-            for (int j = 0; j < L; ++j) {
+            for (int i = 0; i < H; ++i) {
+                const int j = par + 2 * i;
+                if (j >= L) break;
                 const double2 tj = stg[wid][0][tm][j], fj = stg[wid][1][tm][j];
                 const double ff = fo.x * fj.x + fo.y * fj.y;
                 eff += __ldg(dtab + k + j * L) * ff;
