@@ -500,9 +500,12 @@ static bool L_supported(int L, bool mixed)
     return L == 2 || L == 3 || L == 4 || L == 5 || L == 6 || L == 8 || L == 12;
 }
 
-// Lanes per transform of the register FFT for the x and y lengths (0: Stockham passes).
+// Lanes per transform of the register FFT for the x and y lengths (0: Stockham passes),
+// and the length that selects the register-FFT kernels (0: the Stockham kernels).
 static int rx_x(const rbc_handle* h) { return rbcfft::reg_fft_lanes(h->G.nx); }
 static int rx_y(const rbc_handle* h) { return rbcfft::reg_fft_lanes(h->G.ny); }
+static int reg_nx(const rbc_handle* h) { return rx_x(h) ? h->G.nx : 0; }
+static int reg_ny(const rbc_handle* h) { return rx_y(h) ? h->G.ny : 0; }
 // Row pairs (transforms) a row-kernel CTA can hold: one per TL lanes of kThreads threads,
 // or one Stockham chunk.
 static int max_row_pairs(const rbc_handle* h) { return rx_x(h) ? kThreads / rx_x(h) : h->px.chunk; }
@@ -511,19 +514,19 @@ template <typename R> static size_t smem_cols(const rbc_handle* h, int nfield)
 {
     const size_t c = sizeof(typename cplx_t<R>::type);
     if (const int rx = rx_y(h))
-        return c * ((size_t)h->G.ny + (size_t)nfield * h->W * tp_stride(h->G.ny, rx)) +
+        return c * ((size_t)h->G.ny + (size_t)nfield * h->W * tp_stride(h->G.ny)) +
                sizeof(double2) * 3 * (size_t)h->W * h->G.ny;
     return c * ((size_t)h->G.ny + (size_t)nfield * h->W * h->py.stride);
 }
 template <typename R> static size_t smem_combine(const rbc_handle* h)
 {
     const int rx = rx_y(h);
-    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + 13 * (size_t)(rx ? tp_stride(h->G.ny, rx) : h->py.stride));
+    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.ny + 13 * (size_t)(rx ? tp_stride(h->G.ny) : h->py.stride));
 }
 template <typename R> static size_t smem_rows(const rbc_handle* h)
 {
     const int rx = rx_x(h);
-    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.nx + (size_t)h->NP * (rx ? tp_stride(h->G.nx, rx) : h->px.stride));
+    return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.nx + (size_t)h->NP * (rx ? tp_stride(h->G.nx) : h->px.stride));
 }
 
 template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h);
@@ -538,19 +541,17 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     {
     StageScope sc(h, ST_SYNTH);
     const size_t sm = smem_cols<R>(h, 8);
-    switch (rx_y(h)) {
-    case 32:
-        if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, 32>, g1, dim3(8 * h->W * 32), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
-        else k_synth_columns_tp<R, 32><<<g1, 8 * h->W * 32, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H);
+    switch (reg_ny(h)) {
+#define RBC_SYNTH_TP(NN)                                                                                                          \
+    case NN:                                                                                                                      \
+        if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, NN>, g1, dim3(8 * h->W * rx_y(h)), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H); \
+        else k_synth_columns_tp<R, NN><<<g1, 8 * h->W * rx_y(h), sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H); \
         break;
-    case 16:
-        if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, 16>, g1, dim3(8 * h->W * 16), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
-        else k_synth_columns_tp<R, 16><<<g1, 8 * h->W * 16, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H);
-        break;
-    case 8:
-        if (h->k1_dep) launch_dep(h, k_synth_columns_tp<R, 8>, g1, dim3(8 * h->W * 8), sm, G, h->W, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
-        else k_synth_columns_tp<R, 8><<<g1, 8 * h->W * 8, sm, h->stream>>>(G, h->W, h->twy, th, f, g, FG, (C*)h->H);
-        break;
+    RBC_SYNTH_TP(512)
+    RBC_SYNTH_TP(256)
+    RBC_SYNTH_TP(128)
+    RBC_SYNTH_TP(64)
+#undef RBC_SYNTH_TP
     default:
         if (h->k1_dep) launch_dep(h, k_synth_columns<R>, g1, dim3(kThreads), sm, G, h->W, h->py, (const double2*)h->twy, th, f, g, FG, (C*)h->H);
         else k_synth_columns<R><<<g1, kThreads, sm, h->stream>>>(G, h->W, h->py, h->twy, th, f, g, FG, (C*)h->H);
@@ -561,10 +562,12 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     StageScope sc(h, ST_C2R);
     const int nb = rows / (2 * h->NP);
     const size_t sm = smem_rows<R>(h);
-    switch (rx_x(h)) {
-    case 32: launch_dep(h, k_rows_c2r_tp<R, 32>, dim3(nb), dim3(h->NP * 32), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
-    case 16: launch_dep(h, k_rows_c2r_tp<R, 16>, dim3(nb), dim3(h->NP * 16), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
-    case 8: launch_dep(h, k_rows_c2r_tp<R, 8>, dim3(nb), dim3(h->NP * 8), sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
+    const dim3 tb(h->NP * rx_x(h));
+    switch (reg_nx(h)) {
+    case 512: launch_dep(h, k_rows_c2r_tp<R, 512>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
+    case 256: launch_dep(h, k_rows_c2r_tp<R, 256>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
+    case 128: launch_dep(h, k_rows_c2r_tp<R, 128>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
+    case 64: launch_dep(h, k_rows_c2r_tp<R, 64>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     default: launch_dep(h, k_rows_c2r<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const C*)h->H, (R*)h->phys);
     }
     RBC_CUDA(cudaGetLastError());
@@ -620,10 +623,12 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     StageScope sc(h, ST_R2C);
     const int nb = rows / (2 * h->NP);
     const size_t sm = smem_rows<R>(h);
-    switch (rx_x(h)) {
-    case 32: launch_dep(h, k_rows_r2c_tp<R, 32>, dim3(nb), dim3(h->NP * 32), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
-    case 16: launch_dep(h, k_rows_r2c_tp<R, 16>, dim3(nb), dim3(h->NP * 16), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
-    case 8: launch_dep(h, k_rows_r2c_tp<R, 8>, dim3(nb), dim3(h->NP * 8), sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    const dim3 tb(h->NP * rx_x(h));
+    switch (reg_nx(h)) {
+    case 512: launch_dep(h, k_rows_r2c_tp<R, 512>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 256: launch_dep(h, k_rows_r2c_tp<R, 256>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 128: launch_dep(h, k_rows_r2c_tp<R, 128>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 64: launch_dep(h, k_rows_r2c_tp<R, 64>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     default: launch_dep(h, k_rows_r2c<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh);
     }
     RBC_CUDA(cudaGetLastError());
@@ -632,10 +637,12 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     {
     StageScope sc(h, ST_COMBINE);
     const size_t sm = smem_combine<R>(h);
-    switch (rx_y(h)) {
-    case 32: launch_dep(h, k_columns_combine_tp<R, 32>, g5, dim3(kThreads), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
-    case 16: launch_dep(h, k_columns_combine_tp<R, 16>, g5, dim3(13 * 16), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
-    case 8: launch_dep(h, k_columns_combine_tp<R, 8>, g5, dim3(13 * 8), sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    const dim3 tb(std::min(13 * rx_y(h), kThreads));
+    switch (reg_ny(h)) {
+    case 512: launch_dep(h, k_columns_combine_tp<R, 512>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    case 256: launch_dep(h, k_columns_combine_tp<R, 256>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    case 128: launch_dep(h, k_columns_combine_tp<R, 128>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    case 64: launch_dep(h, k_columns_combine_tp<R, 64>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     default: launch_dep(h, k_columns_combine<R>, g5, dim3(kThreads), sm, G, h->py, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
     }
     RBC_CUDA(cudaGetLastError());
@@ -850,18 +857,22 @@ template <typename R> static void set_attributes(rbc_handle* h)
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     if (h->prm.n_tracers > 0) RBC_DISPATCH_L(set_tracer_attribute, R, h->G.L, h);
 }
 

@@ -1,5 +1,6 @@
-// fft2p.cuh -- register-resident FFTs: two passes for N = R * R (R = 8 or 16), three for
-// N = 512 (16 x 16 x 2, one warp per transform; three_pass_512 below).
+// fft2p.cuh -- register-resident FFTs: two passes for N = R * R (R = 8 or 16) and for
+// N = 128 = 8 x 16 (two_pass_wide), three for N = 512 (16 x 16 x 2, one warp per
+// transform; three_pass_512 below).
 //
 // One transform is done by R consecutive lanes of a warp (a quarter or half warp).
 // With x[n], n = t + R a, the lane t holds v[a] = x[t + R a] on entry and
@@ -94,19 +95,59 @@ RBC_D void three_pass_512(typename cplx_t<Rt>::type (&v)[16], int t, typename cp
     __syncwarp(); // the tile may be reused by the caller after this
 }
 
-// Lanes per transform of the register FFT for length n (0: use the Stockham passes),
-// the length for a lane count, and the shared tile one transform needs.
-RBC_HD constexpr int reg_fft_lanes(int n) { return n == 512 ? 32 : n == 256 ? 16 : n == 64 ? 8 : 0; }
-RBC_HD constexpr int reg_fft_len(int lanes) { return lanes == 32 ? 512 : lanes * lanes; }
-RBC_HD constexpr int reg_tile_len(int lanes) { return lanes == 32 ? tile_len_512() : lanes * (lanes + 1); }
-
-// The register FFT of length reg_fft_len(TL) done by TL lanes, each holding VL = N / TL
-// values: v[a] = x[t + TL a] on entry, v[k] = X[t + TL k] on exit.
+// N = TL * VL with VL = 2 TL (128 = 8 x 16) on TL lanes: lane t holds v[a] = x[t + TL a]
+// (a < VL) on entry and v[m] = X[t + TL m] on exit.
+//   pass 1: v[k1] = sum_a x[t + TL a] W_VL^(a k1), times W_N^(t k1)          (registers)
+//   transpose through S[k1 (TL + 1) + t]
+//   pass 2: lane t does the TL-point DFTs of k1 = t and t + TL over t':
+//           X[k1 + VL k2] = sum_t' S[k1 (TL + 1) + t'] W_TL^(t' k2), i.e. v[j + 2 k2] for
+//           k1 = t + TL j.
 template <int TL, typename Rt>
-RBC_D void reg_fft(typename cplx_t<Rt>::type (&v)[reg_fft_len(TL) / TL], int t, typename cplx_t<Rt>::type* S,
+RBC_D void two_pass_wide(typename cplx_t<Rt>::type (&v)[2 * TL], int t, typename cplx_t<Rt>::type* S,
+                         const typename cplx_t<Rt>::type* tw, int sign)
+{
+    typedef typename cplx_t<Rt>::type C;
+    constexpr int VL = 2 * TL;
+    dft_small<VL, Rt>(v, sign);
+#pragma unroll
+    for (int k1 = 1; k1 < VL; ++k1) {
+        C w = tw[t * k1];                 // W_N^(t k1), t k1 < N
+        if (sign > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    const unsigned m = team_mask<TL>();
+#pragma unroll
+    for (int k1 = 0; k1 < VL; ++k1) S[k1 * (TL + 1) + t] = v[k1];
+    __syncwarp(m);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        C u[TL];
+#pragma unroll
+        for (int i = 0; i < TL; ++i) u[i] = S[(t + TL * j) * (TL + 1) + i];
+        dft_small<TL, Rt>(u, sign);
+#pragma unroll
+        for (int k2 = 0; k2 < TL; ++k2) v[j + 2 * k2] = u[k2];
+    }
+    __syncwarp(m); // the tile may be reused by the caller after this
+}
+
+// Lanes per transform of the register FFT for length n (0: use the Stockham passes),
+// and the shared tile one transform needs.
+RBC_HD constexpr int reg_fft_lanes(int n) { return n == 512 ? 32 : n == 256 ? 16 : n == 128 ? 8 : n == 64 ? 8 : 0; }
+RBC_HD constexpr int reg_tile_len(int n)
+{
+    return n == 512 ? tile_len_512() : (n / reg_fft_lanes(n)) * (reg_fft_lanes(n) + 1);
+}
+
+// The register FFT of length N done by TL = reg_fft_lanes(N) lanes, each holding
+// VL = N / TL values: v[a] = x[t + TL a] on entry, v[k] = X[t + TL k] on exit.
+template <int N, typename Rt>
+RBC_D void reg_fft(typename cplx_t<Rt>::type (&v)[N / reg_fft_lanes(N)], int t, typename cplx_t<Rt>::type* S,
                    const typename cplx_t<Rt>::type* tw, int sign)
 {
-    if constexpr (TL == 32) three_pass_512<Rt>(v, t, S, tw, sign);
+    constexpr int TL = reg_fft_lanes(N);
+    if constexpr (N == 512) three_pass_512<Rt>(v, t, S, tw, sign);
+    else if constexpr (N == 2 * TL * TL) two_pass_wide<TL, Rt>(v, t, S, tw, sign);
     else two_pass<TL, Rt>(v, t, S, tw, sign);
 }
 

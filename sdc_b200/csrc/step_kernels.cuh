@@ -321,14 +321,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
 }
 
 // =================================================================================
-// Register-FFT forms of K1, K2, K4 and K5 for the transform lengths N = 64, 256 and 512
-// (fft2p.cuh): the CTA holds the same transforms as the Stockham forms; each transform is
-// done by TL consecutive lanes (8, 16, 32) holding VL = N / TL values each, so the block
-// has (transforms x TL) threads. A transform's shared region has tp_stride(N, TL) elements
-// (the padded row of the Stockham forms, or the register FFT's tile if that is longer).
-RBC_HD int tp_stride(int n, int tl)
+// Register-FFT forms of K1, K2, K4 and K5 for the transform lengths N = 64, 128, 256 and
+// 512 (fft2p.cuh): the CTA holds the same transforms as the Stockham forms; each transform
+// is done by TL = reg_fft_lanes(N) consecutive lanes (8, 8, 16, 32) holding VL = N / TL
+// values each, so the block has (transforms x TL) threads. A transform's shared region has
+// tp_stride(N) elements (the padded row of the Stockham forms, or the register FFT's tile
+// if that is longer).
+RBC_HD int tp_stride(int n)
 {
-    return rbcfft::padded_len(n) > rbcfft::reg_tile_len(tl) ? rbcfft::padded_len(n) : rbcfft::reg_tile_len(tl);
+    return rbcfft::padded_len(n) > rbcfft::reg_tile_len(n) ? rbcfft::padded_len(n) : rbcfft::reg_tile_len(n);
 }
 
 // Synthesis field fld (order of k_synth_columns) at (c, r) from theta, f, g.
@@ -347,17 +348,17 @@ RBC_D double2 synth_value(int fld, double2 vt, double2 vf, double2 vg, const Mul
 }
 
 // K1, register FFT: grid (ckw / W, L), block 8 W TL threads (transform q = fld W + cc).
-template <typename R, int TL>
+template <typename R, int N>
 __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
     Geom G, int W, const double2* __restrict__ twy, const double2* __restrict__ th,
     const double2* __restrict__ f, const double2* __restrict__ g, const double2* __restrict__ FG,
     typename cplx_t<R>::type* __restrict__ H)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
+    constexpr int TL = rbcfft::reg_fft_lanes(N), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
-    const int st = tp_stride(N, TL);
+    const int st = tp_stride(N);
     C* buf = tw + N;
     double2* stg = reinterpret_cast<double2*>(buf + 8 * W * st); // [3][W][N]: theta, f, g
     const int k = blockIdx.y;
@@ -406,24 +407,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_synth_columns_tp(
         }
         v[a] = cmk<C>(val.x, val.y);
     }
-    rbcfft::reg_fft<TL, R>(v, t, buf + q * st, tw, +1);
+    rbcfft::reg_fft<N, R>(v, t, buf + q * st, tw, +1);
     C* dst = H + (((size_t)fld * G.L + k) * G.ckp + c) * N;
 #pragma unroll
     for (int k2 = 0; k2 < VL; ++k2) dst[t + TL * k2] = v[k2];
 }
 
 // K2, register FFT: block NP TL threads, transform pp = row pair.
-template <typename R, int TL>
+template <typename R, int N>
 __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
     Geom G, int NP, const double2* __restrict__ twx, const typename cplx_t<R>::type* __restrict__ H,
     R* __restrict__ phys)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
+    constexpr int TL = rbcfft::reg_fft_lanes(N), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + N;
-    const int st = tp_stride(N, TL);
+    const int st = tp_stride(N);
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     pdl_trigger();
@@ -463,7 +464,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
 #pragma unroll
     for (int a = 0; a < VL; ++a) v[a] = S[rbcfft::pad(t + TL * a)];
     __syncwarp(rbcfft::team_mask<TL>()); // every lane has read before the tile is overwritten
-    rbcfft::reg_fft<TL, R>(v, t, S, tw, +1);
+    rbcfft::reg_fft<N, R>(v, t, S, tw, +1);
     R* dst = phys + (size_t)(row0 + 2 * pp) * N;
 #pragma unroll
     for (int k2 = 0; k2 < VL; ++k2) {
@@ -473,17 +474,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
 }
 
 // K4, register FFT: block NP TL threads.
-template <typename R, int TL>
+template <typename R, int N>
 __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     Geom G, int NP, const double2* __restrict__ twx, const R* __restrict__ grp,
     typename cplx_t<R>::type* __restrict__ gh)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
+    constexpr int TL = rbcfft::reg_fft_lanes(N), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + N;
-    const int st = tp_stride(N, TL);
+    const int st = tp_stride(N);
     const int row0 = 2 * NP * blockIdx.x;
     const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     const int pp = threadIdx.x / TL, t = threadIdx.x - pp * TL;
@@ -500,7 +501,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     cp_async_wait_all();
     __syncthreads();
     C* S = buf + pp * st;
-    rbcfft::reg_fft<TL, R>(v, t, S, tw, -1);
+    rbcfft::reg_fft<N, R>(v, t, S, tw, -1);
 #pragma unroll
     for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
     __syncthreads();
@@ -524,17 +525,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
 
 // K5, register FFT: grid (ckw, L), block min(13 TL, kThreads) threads; team q (TL lanes)
 // transforms groups q, q + teams, ... (one group each for TL <= 16, up to two for TL = 32).
-template <typename R, int TL>
+template <typename R, int N>
 __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     Geom G, const double2* __restrict__ twy, const typename cplx_t<R>::type* __restrict__ gh,
     typename cplx_t<R>::type* __restrict__ N_out, double* __restrict__ NFG)
 {
     typedef typename cplx_t<R>::type C;
-    constexpr int N = rbcfft::reg_fft_len(TL), VL = N / TL;
+    constexpr int TL = rbcfft::reg_fft_lanes(N), VL = N / TL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + N;
-    const int st = tp_stride(N, TL);
+    const int st = tp_stride(N);
     const int c = blockIdx.x, k = blockIdx.y;
     const size_t cstride = (size_t)G.L * G.ckp * N; // between groups
     const int teams = blockDim.x / TL, team = threadIdx.x / TL, t = threadIdx.x - team * TL;
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine_tp(
     __syncthreads();
     for (;;) {
         C* S = buf + gq * st;
-        rbcfft::reg_fft<TL, R>(v, t, S, tw, -1);
+        rbcfft::reg_fft<N, R>(v, t, S, tw, -1);
 #pragma unroll
         for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
         gq += teams;
