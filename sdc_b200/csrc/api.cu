@@ -529,6 +529,19 @@ template <typename R> static size_t smem_rows(const rbc_handle* h)
     return sizeof(typename cplx_t<R>::type) * ((size_t)h->G.nx + (size_t)h->NP * (rx ? tp_stride(h->G.nx) : h->px.stride));
 }
 
+// Grid of the analysis row kernel: at most the CTAs that are resident at once (each CTA
+// then loops over its items and prefetches the next one), never more than the items.
+template <typename K> static int resident_grid(const rbc_handle* h, K kernel, int threads, size_t smem, int items)
+{
+    (void)h;
+    int dev = 0, nsm = 148, per = 0;
+    RBC_CUDA(cudaGetDevice(&dev));
+    RBC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    RBC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+    const long long res = (long long)nsm * (per > 0 ? per : 1);
+    return (int)std::min<long long>(items, res);
+}
+
 template <typename R> static void launch_tracer_from_synthesis(rbc_handle* h);
 
 // Synthesis: K1 (columns) + K2 (rows) into h->phys from the state in (th, f, g, FG).
@@ -625,10 +638,10 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     const size_t sm = smem_rows<R>(h);
     const dim3 tb(h->NP * rx_x(h));
     switch (reg_nx(h)) {
-    case 512: launch_dep(h, k_rows_r2c_tp<R, 512>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
-    case 256: launch_dep(h, k_rows_r2c_tp<R, 256>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
-    case 128: launch_dep(h, k_rows_r2c_tp<R, 128>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
-    case 64: launch_dep(h, k_rows_r2c_tp<R, 64>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 512: launch_dep(h, k_rows_r2c_tp<R, 512>, dim3(resident_grid(h, k_rows_r2c_tp<R, 512>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 256: launch_dep(h, k_rows_r2c_tp<R, 256>, dim3(resident_grid(h, k_rows_r2c_tp<R, 256>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 128: launch_dep(h, k_rows_r2c_tp<R, 128>, dim3(resident_grid(h, k_rows_r2c_tp<R, 128>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 64: launch_dep(h, k_rows_r2c_tp<R, 64>, dim3(resident_grid(h, k_rows_r2c_tp<R, 64>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     default: launch_dep(h, k_rows_r2c<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh);
     }
     RBC_CUDA(cudaGetLastError());

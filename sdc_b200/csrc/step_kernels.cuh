@@ -473,10 +473,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_c2r_tp(
     }
 }
 
-// K4, register FFT: block NP TL threads.
+// K4, register FFT: block NP TL threads; item i = row pairs [NP i, NP (i + 1)) of the 13 L
+// group planes. A CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ... and loads the next
+// item's rows into registers as soon as the current item's spectra are in shared memory, so
+// the loads are in flight during the current item's output stage.
 template <typename R, int N>
 __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
-    Geom G, int NP, const double2* __restrict__ twx, const R* __restrict__ grp,
+    Geom G, int NP, int nitems, const double2* __restrict__ twx, const R* __restrict__ grp,
     typename cplx_t<R>::type* __restrict__ gh)
 {
     typedef typename cplx_t<R>::type C;
@@ -485,41 +488,52 @@ __global__ void __launch_bounds__(kThreads, 2) k_rows_r2c_tp(
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + N;
     const int st = tp_stride(N);
-    const int row0 = 2 * NP * blockIdx.x;
-    const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
     const int pp = threadIdx.x / TL, t = threadIdx.x - pp * TL;
-    const R* src = grp + (size_t)(row0 + 2 * pp) * N;
+    C* S = buf + pp * st;
+    C v[VL];
+    auto load = [&](int item) {
+        const R* src = grp + (size_t)(2 * NP * item + 2 * pp) * N;
+#pragma unroll
+        for (int a = 0; a < VL; ++a) {
+            v[a].x = ld_cg(src + t + TL * a);
+            v[a].y = ld_cg(src + N + t + TL * a);
+        }
+    };
     pdl_trigger();
     load_twiddles_async<R>(tw, twx, N);
     pdl_wait();
-    C v[VL];
-#pragma unroll
-    for (int a = 0; a < VL; ++a) {
-        v[a].x = ld_cg(src + t + TL * a);
-        v[a].y = ld_cg(src + N + t + TL * a);
-    }
+    int it = blockIdx.x; // < nitems: the grid is never larger than the item count
+    load(it);
     cp_async_wait_all();
     __syncthreads();
-    C* S = buf + pp * st;
-    rbcfft::reg_fft<N, R>(v, t, S, tw, -1);
-#pragma unroll
-    for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
-    __syncthreads();
     const R half = (R)0.5;
-    C* dst = gh + (size_t)plane * G.ckp * G.ny + y0;
-    for (int e = threadIdx.x; e < NP * G.ckw; e += blockDim.x) {
-        const int n = e / NP, q = e - n * NP;
-        C A = cmk<C>(0, 0), B = A;
-        if (n < G.ckeep) {
-            const C z = buf[q * st + rbcfft::pad(n)];
-            const C zm = buf[q * st + rbcfft::pad(n == 0 ? 0 : N - n)];
-            A.x = half * (z.x + zm.x);
-            A.y = half * (z.y - zm.y);
-            B.x = half * (z.y + zm.y);
-            B.y = half * (zm.x - z.x);
+    for (;;) {
+        rbcfft::reg_fft<N, R>(v, t, S, tw, -1);
+#pragma unroll
+        for (int k2 = 0; k2 < VL; ++k2) S[rbcfft::pad(t + TL * k2)] = v[k2];
+        const int nxt = it + gridDim.x;
+        if (nxt < nitems) load(nxt);
+        __syncthreads();
+        const int row0 = 2 * NP * it;
+        const int plane = row0 / G.ny, y0 = row0 - plane * G.ny;
+        C* dst = gh + (size_t)plane * G.ckp * G.ny + y0;
+        for (int e = threadIdx.x; e < NP * G.ckw; e += blockDim.x) {
+            const int n = e / NP, q = e - n * NP;
+            C A = cmk<C>(0, 0), B = A;
+            if (n < G.ckeep) {
+                const C z = buf[q * st + rbcfft::pad(n)];
+                const C zm = buf[q * st + rbcfft::pad(n == 0 ? 0 : N - n)];
+                A.x = half * (z.x + zm.x);
+                A.y = half * (z.y - zm.y);
+                B.x = half * (z.y + zm.y);
+                B.y = half * (zm.x - z.x);
+            }
+            dst[(size_t)n * G.ny + 2 * q] = A;
+            dst[(size_t)n * G.ny + 2 * q + 1] = B;
         }
-        dst[(size_t)n * G.ny + 2 * q] = A;
-        dst[(size_t)n * G.ny + 2 * q + 1] = B;
+        it = nxt;
+        if (it >= nitems) break;
+        __syncthreads(); // the spectra are read before the next transform reuses the tiles
     }
 }
 
