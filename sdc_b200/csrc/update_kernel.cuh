@@ -252,11 +252,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_update(UpdateArgs A)
     if (!last) return;
     __threadfence();
     // fixed partition (lane l sums blocks l, l + 32, ...) and a fixed shuffle tree:
-    // the result does not depend on the order in which blocks finished
+    // the result does not depend on the order in which blocks finished. The partials are
+    // read through L2 (the fence above orders them after the other blocks' writes), eight
+    // loads in flight per lane before they are added in that order.
     double a = 0, b = 0;
-    for (int i = lane; i < (int)gridDim.x; i += 32) {
-        a += ((volatile double*)A.partial)[2 * i];
-        b += ((volatile double*)A.partial)[2 * i + 1];
+    const int nb = (int)gridDim.x;
+    for (int i0 = lane; i0 < nb; i0 += 32 * 8) {
+        double pa[8], pb[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int i = i0 + 32 * j;
+            pa[j] = i < nb ? ld_cg(A.partial + 2 * i) : 0.0;
+            pb[j] = i < nb ? ld_cg(A.partial + 2 * i + 1) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (i0 + 32 * j < nb) {
+                a += pa[j];
+                b += pb[j];
+            }
     }
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
@@ -264,8 +278,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_update(UpdateArgs A)
         b += __shfl_down_sync(0xffffffffu, b, s);
     }
     if (lane == 0) {
+        double t00[L];
+#pragma unroll
+        for (int kk = 0; kk < L; ++kk) t00[kk] = ld_cg(A.th00 + kk);
         double nuw = 1.0;
-        for (int kk = 0; kk < L; ++kk) nuw -= (kk + 1) * kPi * ((volatile double*)A.th00)[kk];
+#pragma unroll
+        for (int kk = 0; kk < L; ++kk) nuw -= (kk + 1) * kPi * t00[kk];
         const long long s = *A.step_counter + 1;
         *A.step_counter = s;
         double* slot = A.ring + 4 * (size_t)((s - 1) % A.ring_cap);
