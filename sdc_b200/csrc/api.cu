@@ -425,6 +425,8 @@ template <typename R, int L> static void launch_contract(rbc_handle* h)
             A.phys = (const float*)h->phys;
             A.grp = (float*)h->grp;
             A.nv = h->tracer_pending ? (float*)h->nv : nullptr;
+            A.step_counter = h->step_counter;
+            A.step_copy = h->tr_step;
             A.bimg = h->col_bimg;
             A.proj = h->col_proj;
             A.P = h->G.P;
@@ -438,7 +440,7 @@ template <typename R, int L> static void launch_contract(rbc_handle* h)
     }
     R* nv = h->tracer_pending ? (R*)h->nv : nullptr; // node records for the tracer advance
     launch_dep(h, k_contract<R, L>, dim3(h->contract_grid), dim3(128), (size_t)h->contract_smem, (const R*)h->phys,
-               (R*)h->grp, (const R*)h->coef, h->G.P, nv);
+               (R*)h->grp, (const R*)h->coef, h->G.P, nv, (const long long*)h->step_counter, h->tr_step);
     RBC_CUDA(cudaGetLastError());
     ++h->launches;
 }
@@ -597,7 +599,9 @@ static void join_tracer(rbc_handle* h)
 
 // The tracer advance of step m reads m (diffusion noise, track frame) while, on the side
 // stream, the update kernel of the step it overlaps increments the step counter: the
-// advance reads a copy taken on the main stream before the fork.
+// advance reads a copy taken on the main stream before the fork (inside the step, by the
+// contraction kernel that writes the node records; here, for an advance from a synthesis
+// that no step starts from).
 static void snapshot_step(rbc_handle* h)
 {
     RBC_CUDA(cudaMemcpyAsync(h->tr_step, h->step_counter, sizeof(long long), cudaMemcpyDeviceToDevice, h->stream));
@@ -614,9 +618,8 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
 {
     typedef typename cplx_t<R>::type C;
     join_tracer(h); // an advance still reading the node records ends before they are rewritten
-    RBC_DISPATCH_L(launch_contract, R, G.L, h);
+    RBC_DISPATCH_L(launch_contract, R, G.L, h); // with a pending advance it also copies the step counter
     if (h->tracer_pending) {
-        snapshot_step(h);
         if (h->side && !h->profiling) {
             RBC_CUDA(cudaEventRecord(h->ev_fork, h->stream));
             RBC_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));

@@ -160,6 +160,8 @@ struct CollocArgs {
     const float* phys;      // [8][L][P] synthesised fields (FP32)
     float* grp;             // [13][L][P] contracted groups (FP32)
     float* nv;              // node records of the tracers, or null
+    const long long* step_counter; // copied to step_copy when nv is not null (the tracer
+    long long* step_copy;          // advance reads the copy; the update increments the counter)
     const float* bimg;      // basis operands, hi then lo, in the shared-memory image layout
     const float* proj;      // [NKIND][Q][Lp] w_q chi_{c,k}(z_q)
     int P, ntiles;
@@ -307,7 +309,8 @@ __global__ void __launch_bounds__(kColThreads, 1) k_colloc_contract(CollocArgs A
                      : "memory");
     }
     ok = !__syncthreads_or(!col_wait(bar_b, 0)); // every thread takes the same branch
-    pdl_wait(); // the synthesis is complete
+    pdl_wait(); // the synthesis is complete (and with it the previous step's update)
+    if (A.nv && blockIdx.x == 0 && threadIdx.x == 0) *A.step_copy = ld_cg(A.step_counter);
     unsigned tile_no = 0;
     for (int t = blockIdx.x; t < A.ntiles && ok; t += gridDim.x, ++tile_no) {
         const long long x = (long long)t * kColM + r;

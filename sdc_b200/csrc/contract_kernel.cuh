@@ -101,17 +101,21 @@ __global__ void __launch_bounds__(256) k_node_records(const R* __restrict__ phys
 
 // Grid-stride over points; coef (global) is the packed array of pack_contraction,
 // copied once per CTA into shared memory. When nv is not null the kernel also writes
-// every point's node record nv[x * NodeRec] (the tracers gather those records).
+// every point's node record nv[x * NodeRec] (the tracers gather those records), and
+// copies the step counter to step_copy: the tracer advance that reads the records runs
+// beside the update that increments the counter, and reads the copy.
 template <typename R, int L>
 __global__ void __launch_bounds__(128) k_contract(const R* __restrict__ phys, R* __restrict__ grp,
-                                                  const R* __restrict__ coef_g, int P, R* __restrict__ nv)
+                                                  const R* __restrict__ coef_g, int P, R* __restrict__ nv,
+                                                  const long long* __restrict__ step_counter, long long* step_copy)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* coef = reinterpret_cast<R*>(smem_raw);
     constexpr int NC = rbcprog::NUNIT * L * L * rbcprog::half_len(L);
     pdl_trigger();
     for (int e = threadIdx.x; e < NC; e += blockDim.x) coef[e] = coef_g[e];
-    pdl_wait(); // the synthesis is complete
+    pdl_wait(); // the synthesis is complete (and with it the previous step's update)
+    if (nv && blockIdx.x == 0 && threadIdx.x == 0) *step_copy = ld_cg(step_counter);
     __syncthreads();
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < P; x += gridDim.x * blockDim.x) {
         R in[rbcprog::NFIELD][L];

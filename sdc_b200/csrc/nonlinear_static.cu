@@ -145,7 +145,7 @@ void say(char* buf, int len, const char* msg)
 template <int L> void launch_contract_na(const Geom& G, double* phys, double* grp, const double* coef, cudaStream_t s)
 {
     const int smem = (int)(rbcprog::NUNIT * L * L * rbcprog::half_len(L) * sizeof(double));
-    k_contract<double, L><<<(G.P + 127) / 128, 128, smem, s>>>(phys, grp, coef, G.P, nullptr);
+    k_contract<double, L><<<(G.P + 127) / 128, 128, smem, s>>>(phys, grp, coef, G.P, nullptr, nullptr, nullptr);
 }
 
 } // namespace
