@@ -564,6 +564,7 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
         break;
     RBC_SYNTH_TP(512)
     RBC_SYNTH_TP(256)
+    RBC_SYNTH_TP(192)
     RBC_SYNTH_TP(128)
     RBC_SYNTH_TP(64)
 #undef RBC_SYNTH_TP
@@ -581,6 +582,7 @@ static void run_synthesis(rbc_handle* h, const double2* th, const double2* f, co
     switch (reg_nx(h)) {
     case 512: launch_dep(h, k_rows_c2r_tp<R, 512>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     case 256: launch_dep(h, k_rows_c2r_tp<R, 256>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
+    case 192: launch_dep(h, k_rows_c2r_tp<R, 192>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     case 128: launch_dep(h, k_rows_c2r_tp<R, 128>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     case 64: launch_dep(h, k_rows_c2r_tp<R, 64>, dim3(nb), tb, sm, G, h->NP, (const double2*)h->twx, (const C*)h->H, (R*)h->phys); break;
     default: launch_dep(h, k_rows_c2r<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const C*)h->H, (R*)h->phys);
@@ -643,6 +645,7 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     switch (reg_nx(h)) {
     case 512: launch_dep(h, k_rows_r2c_tp<R, 512>, dim3(resident_grid(h, k_rows_r2c_tp<R, 512>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     case 256: launch_dep(h, k_rows_r2c_tp<R, 256>, dim3(resident_grid(h, k_rows_r2c_tp<R, 256>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
+    case 192: launch_dep(h, k_rows_r2c_tp<R, 192>, dim3(resident_grid(h, k_rows_r2c_tp<R, 192>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     case 128: launch_dep(h, k_rows_r2c_tp<R, 128>, dim3(resident_grid(h, k_rows_r2c_tp<R, 128>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     case 64: launch_dep(h, k_rows_r2c_tp<R, 64>, dim3(resident_grid(h, k_rows_r2c_tp<R, 64>, tb.x, sm, nb)), tb, sm, G, h->NP, nb, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh); break;
     default: launch_dep(h, k_rows_r2c<R>, dim3(nb), dim3(kThreads), sm, G, h->NP, h->px, (const double2*)h->twx, (const R*)h->grp, (C*)h->gh);
@@ -657,6 +660,7 @@ template <typename R> static void run_analysis(rbc_handle* h, const Geom& G, boo
     switch (reg_ny(h)) {
     case 512: launch_dep(h, k_columns_combine_tp<R, 512>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     case 256: launch_dep(h, k_columns_combine_tp<R, 256>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
+    case 192: launch_dep(h, k_columns_combine_tp<R, 192>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     case 128: launch_dep(h, k_columns_combine_tp<R, 128>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     case 64: launch_dep(h, k_columns_combine_tp<R, 64>, g5, tb, sm, G, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG); break;
     default: launch_dep(h, k_columns_combine<R>, g5, dim3(kThreads), sm, G, h->py, (const double2*)h->twy, (const C*)h->gh, (C*)h->N, h->NFG);
@@ -875,18 +879,22 @@ template <typename R> static void set_attributes(rbc_handle* h)
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_synth_columns_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_c2r_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_rows_r2c_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     RBC_CUDA(cudaFuncSetAttribute(k_columns_combine_tp<R, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     if (h->prm.n_tracers > 0) RBC_DISPATCH_L(set_tracer_attribute, R, h->G.L, h);

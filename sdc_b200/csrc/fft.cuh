@@ -132,6 +132,30 @@ RBC_D void dft_small(typename cplx_t<R>::type* v, int sign)
         v[1] = e1 + o1; v[5] = e1 - o1;
         v[2] = e2 + o2; v[6] = e2 - o2;
         v[3] = e3 + o3; v[7] = e3 - o3;
+    } else if constexpr (RAD == 12) {
+        // n = 3 n1 + n2: 4-point DFTs over n1 for each n2, twiddles W12^(n2 k1), 3-point
+        // DFTs over n2; X[k1 + 4 k2] is the k2-th output of the k1-th 3-point DFT
+        C y[3][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 3; ++n2) {
+            y[n2][0] = v[n2]; y[n2][1] = v[3 + n2]; y[n2][2] = v[6 + n2]; y[n2][3] = v[9 + n2];
+            dft4<R>(y[n2][0], y[n2][1], y[n2][2], y[n2][3], sign);
+        }
+        const R c1 = (R)0.86602540378443864676, h = (R)0.5;
+        y[1][1] = rot<C, R>(y[1][1], c1, s * h);    // W12^1
+        y[1][2] = rot<C, R>(y[1][2], h, s * c1);    // W12^2
+        y[1][3] = cmul_is<C, R>(y[1][3], s);        // W12^3
+        y[2][1] = rot<C, R>(y[2][1], h, s * c1);    // W12^2
+        y[2][2] = rot<C, R>(y[2][2], -h, s * c1);   // W12^4
+        y[2][3] = y[2][3] * (R)-1;                  // W12^6
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            C t3[3] = {y[0][k1], y[1][k1], y[2][k1]};
+            dft_small<3, R>(t3, sign);
+            v[k1] = t3[0];
+            v[k1 + 4] = t3[1];
+            v[k1 + 8] = t3[2];
+        }
     } else if constexpr (RAD == 16) {
         // n = 4 m + q: 4-point DFTs over m in place (v[q], v[q+4], v[q+8], v[q+12] then
         // hold Y_q[k1 = 0..3]), twiddles W16^(q k1), 4-point DFTs over q for each k1;

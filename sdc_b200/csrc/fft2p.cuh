@@ -1,6 +1,6 @@
-// fft2p.cuh -- register-resident FFTs: two passes for N = R * R (R = 8 or 16) and for
-// N = 128 = 8 x 16 (two_pass_wide), three for N = 512 (16 x 16 x 2, one warp per
-// transform; three_pass_512 below).
+// fft2p.cuh -- register-resident FFTs: two passes for N = R * R (R = 8 or 16), for
+// N = 128 = 8 x 16 (two_pass_wide) and for N = 192 = 12 x 16 (fft192), three for N = 512
+// (16 x 16 x 2, one warp per transform; three_pass_512 below).
 //
 // One transform is done by R consecutive lanes of a warp (a quarter or half warp).
 // With x[n], n = t + R a, the lane t holds v[a] = x[t + R a] on entry and
@@ -131,12 +131,57 @@ RBC_D void two_pass_wide(typename cplx_t<Rt>::type (&v)[2 * TL], int t, typename
     __syncwarp(m); // the tile may be reused by the caller after this
 }
 
+// Length 192 = 12 x 16 on 16 lanes: lane t holds v[a] = x[t + 16 a] (a < 12) on entry and
+// v[m] = X[t + 16 m] on exit.
+//   pass 1: v[k1] = sum_a x[t + 16 a] W_12^(a k1), times W_192^(t k1)        (registers)
+//   transpose through S[k1 17 + t]
+//   pass 2: lanes t < 12 do the 16-point DFT of column k1 = t over t':
+//           X[k1 + 12 k2] = sum_t' S[k1 17 + t'] W_16^(t' k2)
+//   the results go back through the tile in natural order (S[pad(k)]), from which every
+//   lane reads its X[t + 16 m].
+// S has 204 elements (12 x 17; pad(191) = 202).
+template <typename Rt>
+RBC_D void fft192(typename cplx_t<Rt>::type (&v)[12], int t, typename cplx_t<Rt>::type* S,
+                  const typename cplx_t<Rt>::type* tw, int sign)
+{
+    typedef typename cplx_t<Rt>::type C;
+    dft_small<12, Rt>(v, sign);
+#pragma unroll
+    for (int k1 = 1; k1 < 12; ++k1) {
+        C w = tw[t * k1];                 // W_192^(t k1), t k1 <= 165
+        if (sign > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    const unsigned m = team_mask<16>();
+#pragma unroll
+    for (int k1 = 0; k1 < 12; ++k1) S[k1 * 17 + t] = v[k1];
+    __syncwarp(m);
+    C u[16];
+    if (t < 12) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) u[i] = S[t * 17 + i];
+        dft_small<16, Rt>(u, sign);
+    }
+    __syncwarp(m); // every column is read before the tile takes the results
+    if (t < 12) {
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) S[pad(t + 12 * k2)] = u[k2];
+    }
+    __syncwarp(m);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) v[i] = S[pad(t + 16 * i)];
+    __syncwarp(m); // the tile may be reused by the caller after this
+}
+
 // Lanes per transform of the register FFT for length n (0: use the Stockham passes),
 // and the shared tile one transform needs.
-RBC_HD constexpr int reg_fft_lanes(int n) { return n == 512 ? 32 : n == 256 ? 16 : n == 128 ? 8 : n == 64 ? 8 : 0; }
+RBC_HD constexpr int reg_fft_lanes(int n)
+{
+    return n == 512 ? 32 : n == 256 ? 16 : n == 192 ? 16 : n == 128 ? 8 : n == 64 ? 8 : 0;
+}
 RBC_HD constexpr int reg_tile_len(int n)
 {
-    return n == 512 ? tile_len_512() : (n / reg_fft_lanes(n)) * (reg_fft_lanes(n) + 1);
+    return n == 512 ? tile_len_512() : n == 192 ? 12 * 17 : (n / reg_fft_lanes(n)) * (reg_fft_lanes(n) + 1);
 }
 
 // The register FFT of length N done by TL = reg_fft_lanes(N) lanes, each holding
@@ -147,6 +192,7 @@ RBC_D void reg_fft(typename cplx_t<Rt>::type (&v)[N / reg_fft_lanes(N)], int t, 
 {
     constexpr int TL = reg_fft_lanes(N);
     if constexpr (N == 512) three_pass_512<Rt>(v, t, S, tw, sign);
+    else if constexpr (N == 192) fft192<Rt>(v, t, S, tw, sign);
     else if constexpr (N == 2 * TL * TL) two_pass_wide<TL, Rt>(v, t, S, tw, sign);
     else two_pass<TL, Rt>(v, t, S, tw, sign);
 }

@@ -41,9 +41,12 @@ def test_nonlinear_operator_matches_oracle(case):
         assert rel_err(a, b) < 1e-12, (name, rel_err(a, b))
 
 
-# longer FFT lengths: 128 = 16*8, 192 = 16*4*3, 256 = 16*16, 512 = 16*16*2, 96 = 16*2*3
+# longer FFT lengths, each in x (row kernels) and in y (column kernels): register forms
+# 128 = 8 lanes x 16, 192 = 16 lanes x 12, 256 = 16 x 16, 512 = 32 lanes x 16; Stockham
+# passes for 96 = 16*2*3
 FFT_CASES = [
     (128, 192, 2, 16.0, 24.0, 3000.0, 1.0, 1e-3),
+    (192, 128, 3, 24.0, 16.0, 3000.0, 1.0, 1e-3),
     (256, 96, 2, 32.0, 12.0, 3000.0, 1.0, 1e-3),
     (512, 64, 2, 64.0, 8.0, 3000.0, 1.0, 1e-3),
     (64, 512, 3, 8.0, 64.0, 3000.0, 1.0, 1e-3),
