@@ -321,9 +321,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_columns_combine(
 }
 
 // =================================================================================
-// Register-FFT forms of K1, K2, K4 and K5 for the transform lengths N = 64, 128, 256 and
-// 512 (fft2p.cuh): the CTA holds the same transforms as the Stockham forms; each transform
-// is done by TL = reg_fft_lanes(N) consecutive lanes (8, 8, 16, 32) holding VL = N / TL
+// Register-FFT forms of K1, K2, K4 and K5 for the transform lengths N = 64, 128, 192, 256
+// and 512 (fft2p.cuh): the CTA holds the same transforms as the Stockham forms; each transform
+// is done by TL = reg_fft_lanes(N) consecutive lanes (8, 8, 16, 16, 32) holding VL = N / TL
 // values each, so the block has (transforms x TL) threads. A transform's shared region has
 // tp_stride(N) elements (the padded row of the Stockham forms, or the register FFT's tile
 // if that is longer).
