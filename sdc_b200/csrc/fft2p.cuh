@@ -5,7 +5,8 @@
 // One transform is done by R consecutive lanes of a warp (a quarter or half warp).
 // With x[n], n = t + R a, the lane t holds v[a] = x[t + R a] on entry and
 //   pass 1: v[k1] = sum_a x[t + R a] W_R^(a k1), times W_N^(t k1)  (registers)
-//   transpose through the transform's own padded shared tile S[k1 (R + 1) + t]
+//   transpose through the transform's own padded shared tile S[k1 (R + 1) + t] (R (R + 1)
+//   elements; the odd row pitch keeps the column reads of pass 2 free of bank conflicts)
 //   pass 2: v[k2] = sum_t' S[t (R + 1) + t'] W_R^(t' k2)             (registers)
 // so that on exit lane t holds X[t + R k2] in v[k2] (X[k] = sum_n x[n] W_N^(n k),
 // W_N = exp(sign 2 pi i / N)). The tile is private to the transform, so the lanes only
@@ -17,10 +18,6 @@
 #include "fft.cuh"
 
 namespace rbcfft {
-
-// Shared tile of one transform: R * (R + 1) elements. Odd row pitch R + 1 keeps the
-// column reads of pass 2 free of bank conflicts.
-template <int R> RBC_HD constexpr int tile_len() { return R * (R + 1); }
 
 // Lane mask of the R lanes that share a transform with this lane.
 template <int R> RBC_D unsigned team_mask()
