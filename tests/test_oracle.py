@@ -24,6 +24,20 @@ def test_oracle_tables_match_reference_golden(L, name):
     assert np.abs(got - ref).max() <= 1e-13 * scale, name
 
 
+@pytest.mark.parametrize("L", [4, 8, 12])
+def test_linear_tables_couple_equal_parities_only(L):
+    """The update kernel keeps only the same-parity half of each row of B_ff^-1 and of the
+    implicit operator (built from Iac and Ia1): in the reference's own tables every entry
+    whose row and column parities differ is an exact zero."""
+    ref = np.load(os.path.join(GOLD, f"coeff_L{L}.npz"))
+    i, j = np.meshgrid(np.arange(L), np.arange(L), indexing="ij")
+    odd = ((i + j) % 2).ravel() == 1
+    for name in ("Iac", "Ia1"):
+        t = ref[name].ravel()
+        assert np.all(t[odd] == 0.0), name
+        assert np.all(np.diag(t.reshape(L, L)) != 0.0), name  # the diagonal is not
+
+
 def test_known_answer_comments():
     # gpu_flow/code/operator/linear_implicit_operator.cu:3-9
     ia1 = oracle.table(2, "Ia1")
