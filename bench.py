@@ -608,6 +608,18 @@ def profile_sdc(local, form="mixed", steps=6):
                       "stages_us": {k: round(v[0] * 1000, 1) for k, v in s.stage_times(10).items()}}))
 
 
+def profile_stockham(local, steps=6):
+    """Small workload for kernel profiling of the shared-memory Stockham FFT kernels (the
+    lengths without a register form): `steps` FP64 steps of a 384 x 384 x 8 grid (Lx = Ly = 48,
+    Ra 5000, Pr 0.9, dt 5e-4) from a seeded state, launch tiling not autotuned."""
+    import sdc_b200
+    s = sdc_b200.Solver(384, 384, 8, 48.0, 48.0, 5000.0, 0.9, 5e-4, device=local, tune=False)
+    s.init_fields(3, 1e-3, 8.0)
+    s.step(steps)
+    print(json.dumps({"profile_stockham": "384x384x8", "nu_wall": s.diagnostics()["nu_wall"],
+                      "stages_us": {k: round(v[0] * 1000, 1) for k, v in s.stage_times(10).items()}}))
+
+
 def ensemble_configs(n=64, seed=4):
     """The uneven ensemble: per member a grid from {64, 128, 192, 256}^2, Nz from {4, 6, 8},
     Ra ~ U[2000, 8000], Pr from {0.7, 1, 7}, Lx = Ly = grid / 8, dt = 5e-4 (drawn by seed)."""
@@ -687,6 +699,8 @@ def main():
                     help="run only a small freeze/heating/penalization workload (for kernel profiling) and exit")
     ap.add_argument("--profile-diagnostics", action="store_true",
                     help="run only a small spectrum/structure-function/mean-forcing workload (for kernel profiling) and exit")
+    ap.add_argument("--profile-stockham", action="store_true",
+                    help="run only a few FP64 steps on a 384x384x8 grid (Stockham FFT kernels, for kernel profiling) and exit")
     ap.add_argument("--profile-sdc", default=None, choices=["fp64", "mixed", "colloc"],
                     help="run only a few steps of the given form on the 512x512x12 grid (for kernel profiling) and exit")
     args = ap.parse_args()
@@ -699,6 +713,9 @@ def main():
         return
     if args.profile_diagnostics:
         profile_diagnostics(int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.profile_stockham:
+        profile_stockham(int(os.environ.get("LOCAL_RANK", "0")))
         return
     if args.profile_sdc:
         profile_sdc(int(os.environ.get("LOCAL_RANK", "0")), form=args.profile_sdc)
