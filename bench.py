@@ -59,8 +59,9 @@ def stage_bytes(nx, ny, L, ckeep, nkept, ntr):
         "contract": 8 * L * P * 8 + 13 * L * P * 8,
         "rows_r2c": 13 * L * P * 8 + 13 * L * col * C,
         "columns_combine": 13 * L * col * C + 3 * L * col * C,
-        # N, state and history read, state and history written, operator tables
-        "update": kept * L * C * (3 + 3 + 3 + 3 + 3) + kept * 5 * L * L * 8,
+        # N, state and history read, state and history written, operator table rows (the
+        # same-parity half of each row of the five L x L matrices)
+        "update": kept * L * C * (3 + 3 + 3 + 3 + 3) + kept * 5 * L * ((L + 1) // 2) * 8,
     }
 
 
